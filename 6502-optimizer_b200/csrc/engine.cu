@@ -1,0 +1,1354 @@
+// engine.cu -- B200 kernels and the C ABI of libm6502gpu.so.
+//
+// Pipeline of one device pass over a block of targets (all on one stream,
+// one host synchronisation per pass):
+//
+//   k_fingerprint   warp per target, lane v runs the target on test vector v:
+//                   32 packed 64-bit output states per target (256 B).
+//   k_qc1           tile of 64 targets x all 2,863 candidates per CTA; the
+//                   candidates' vector-0 outputs stay in registers, the
+//                   targets' in shared memory; one masked 64-bit compare per
+//                   pair rejects almost everything; hits run the byte
+//                   filter, pruner, the other 7 QC vectors and the 24 mid
+//                   vectors, and survivors are appended with one atomic per
+//                   warp (ballot + popc).
+//   k_exhaustive    persistent; a warp takes one surviving pair from a
+//                   device ticket, derives the pair's swept input space
+//                   (reference rule) and the input cone of every output
+//                   location, and sweeps each maximal cone; large cones are
+//                   probed in-warp and the rest is split into work items.
+//   k_exh_items     persistent; warps drain the work-item queue; a failing
+//                   item raises the pair's fail flag, which the others poll.
+//   k_emit_*        passing pairs -> rules (CUDA semantics: all of them; Go
+//                   semantics: first candidate in Go order per target).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "isa.cuh"
+#include "m6502.h"
+
+using namespace m6502;
+
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+constexpr int kMaxSeq = 16;          // longest sequence the pairwise API takes
+constexpr int kWarpsPerBlock = 8;    // 256-thread CTAs
+constexpr uint64_t kSmallSweep = 1ull << 17;  // sweep in-warp up to this many states
+constexpr uint64_t kProbe = 1ull << 12;       // in-warp probe of a large cone
+constexpr uint64_t kChunk = 1ull << 16;       // states per work item
+
+// Test vectors: TestVectors + MidCheckVectors of pkg/search/verifier.go:18-67
+// (A, X, Y, P, S, M, S0, S1).  Vectors 0..7 are QuickCheck's.
+const uint8_t kVectors[32][8] = {
+    {0x00, 0x00, 0x00, 0x00, 0xFD, 0x42, 0x00, 0x00}, {0xFF, 0xFF, 0xFF, 0xFF, 0xFF, 0xBD, 0xFF, 0xFF},
+    {0x01, 0x02, 0x03, 0x00, 0xFD, 0x13, 0x10, 0x20}, {0x80, 0x40, 0x20, 0x01, 0xFC, 0x7E, 0x30, 0x40},
+    {0x55, 0xAA, 0x55, 0x00, 0xFE, 0xA5, 0x55, 0xAA}, {0xAA, 0x55, 0xAA, 0x01, 0xFD, 0x5A, 0xAA, 0x55},
+    {0x0F, 0xF0, 0x0F, 0x00, 0xFB, 0xE1, 0x0F, 0xF0}, {0x7F, 0x80, 0x7F, 0x01, 0xFD, 0x33, 0x80, 0x7F},
+    {0x02, 0x01, 0x04, 0x00, 0xFD, 0x91, 0x11, 0x22}, {0x04, 0x08, 0x10, 0x01, 0xFD, 0x48, 0x33, 0x44},
+    {0x08, 0x10, 0x20, 0x00, 0xFD, 0x24, 0x55, 0x66}, {0x10, 0x20, 0x40, 0x01, 0xFD, 0xD7, 0x77, 0x88},
+    {0x20, 0x40, 0x80, 0x00, 0xFD, 0x6B, 0x99, 0xBB}, {0x40, 0x80, 0x01, 0x01, 0xFD, 0xB2, 0xCC, 0xDD},
+    {0x03, 0x05, 0x09, 0x00, 0xFD, 0x0F, 0xEE, 0x11}, {0x05, 0x0A, 0x14, 0x01, 0xFD, 0xF0, 0x22, 0x33},
+    {0xFE, 0x7F, 0x80, 0x00, 0xFD, 0x01, 0x44, 0x55}, {0x81, 0xFE, 0x01, 0x01, 0xFD, 0xFE, 0x66, 0x77},
+    {0x7E, 0x81, 0x42, 0x00, 0xFD, 0x80, 0x88, 0x99}, {0xBF, 0x40, 0xBF, 0x01, 0xFD, 0x40, 0xAA, 0xBB},
+    {0xC0, 0x3F, 0xC0, 0x00, 0xFD, 0x1F, 0xCC, 0xDD}, {0xE0, 0x1F, 0xE0, 0x01, 0xFD, 0xEF, 0xEE, 0x00},
+    {0xF0, 0x0F, 0xF0, 0x00, 0xFD, 0x55, 0x11, 0x22}, {0x0E, 0xE0, 0x0E, 0x01, 0xFD, 0xAA, 0x33, 0x44},
+    {0x11, 0x22, 0x33, 0x00, 0xFE, 0xC3, 0x00, 0x00}, {0x22, 0x33, 0x44, 0x01, 0xFF, 0x3C, 0x55, 0x66},
+    {0x44, 0x55, 0x66, 0x00, 0xFC, 0x87, 0x77, 0x88}, {0x88, 0x99, 0xAA, 0x01, 0xFB, 0x69, 0x99, 0xAA},
+    {0x33, 0x44, 0x55, 0x00, 0xFD, 0xAE, 0xBB, 0xCC}, {0xCC, 0xDD, 0xEE, 0x01, 0xFD, 0x51, 0xDD, 0xEE},
+    {0x66, 0x77, 0x88, 0x00, 0xFD, 0xDA, 0x12, 0x34}, {0x99, 0xAA, 0xBB, 0x01, 0xFD, 0x25, 0x56, 0x78},
+};
+
+// Representative values of the reduced sweep (pkg/search/verifier.go:378-383).
+const uint8_t kRepValues[32] = {
+    0x00, 0x01, 0x02, 0x0F, 0x10, 0x1F, 0x20, 0x3F, 0x40, 0x55, 0x7E, 0x7F, 0x80, 0x81, 0xAA, 0xBF,
+    0xC0, 0xD5, 0xE0, 0xEF, 0xF0, 0xF7, 0xFE, 0xFF, 0x03, 0x07, 0x11, 0x33, 0x77, 0xBB, 0xDD, 0xEE,
+};
+
+__constant__ uint64_t c_vec[32];             // packed test vectors
+__constant__ uint16_t c_dep[NUM_OPS][NUM_LOCS];
+__constant__ uint16_t c_wr[NUM_OPS];          // written locations per opcode
+__constant__ uint16_t c_sweep[NUM_OPS];       // swept locations implied by opReads
+__constant__ uint16_t c_tab[kNumInsns];       // instructions, CUDA order
+__constant__ uint16_t c_gotab[kNumInsns];     // instructions, Go order
+__constant__ uint32_t c_gorank[kNumInsns];    // Go-order rank of CUDA index i
+__constant__ uint32_t c_rep[32];
+
+// ---------------------------------------------------------------------------
+// Host tables
+// ---------------------------------------------------------------------------
+void host_tables(uint16_t* cuda_tab, uint16_t* go_tab, uint32_t* gorank) {
+    int k = 0;
+    for (uint32_t op = 0; op < NUM_OPS; op++) {
+        if (has_imm(op)) for (uint32_t v = 0; v < 256; v++) cuda_tab[k++] = (uint16_t)(op | (v << 8));
+        else cuda_tab[k++] = (uint16_t)op;
+    }
+    k = 0;
+    for (uint32_t op = 0; op < NUM_OPS; op++) if (!has_imm(op)) go_tab[k++] = (uint16_t)op;
+    for (uint32_t op = 0; op < NUM_OPS; op++)
+        if (has_imm(op)) for (uint32_t v = 0; v < 256; v++) go_tab[k++] = (uint16_t)(op | (v << 8));
+    // rank of each CUDA-order instruction in Go order
+    for (int i = 0; i < kNumInsns; i++) {
+        uint32_t op = cuda_tab[i] & 0xFF, imm = cuda_tab[i] >> 8;
+        uint32_t r;
+        if (!has_imm(op)) {
+            r = 0;
+            for (uint32_t o = 0; o < op; o++) r += has_imm(o) ? 0 : 1;
+        } else {
+            r = 47;
+            for (uint32_t o = 0; o < op; o++) r += has_imm(o) ? 256 : 0;
+            r += imm;
+        }
+        gorank[i] = r;
+    }
+}
+
+uint32_t sweep_locs_of_reads(uint32_t reads) {
+    uint32_t l = 0;
+    if (reads & R_X) l |= LB(L_X);
+    if (reads & R_Y) l |= LB(L_Y);
+    if (reads & R_M) l |= LB(L_M);
+    if (reads & R_S) l |= LB(L_S);
+    if (reads & R_S0) l |= LB(L_S0);
+    if (reads & R_S1) l |= LB(L_S1);
+    return l;
+}
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t fp_of(const St& s) {
+    return pack(s) & ~((uint64_t)(~kPMask & 0xFFu) << 24);   // P & PMask
+}
+
+// Survivor record: target (index within the pass) and candidate code:
+// bits 0..22 candidate index, bit 23 length-2 candidate, bit 24 Go masked
+// pass, bits 25..30 FlagDiff (P bits 0-3, 6-7 compressed to 6 bits).
+struct Surv {
+    uint32_t t;
+    uint32_t c;
+};
+constexpr uint32_t kSurvLen2 = 1u << 23, kSurvMasked = 1u << 24;
+__host__ __device__ __forceinline__ uint32_t fd_pack(uint32_t fd) { return (fd & 0x0Fu) | ((fd >> 2) & 0x30u); }
+
+struct Counters {
+    unsigned long long qc, mid, surv, exh_ticket, items, item_ticket, rules, exh_pass, states, algo;
+};
+
+struct Item {   // one chunk of a large cone sweep
+    uint32_t pair;
+    uint16_t cone;
+    uint8_t rep;
+    uint8_t pad;
+    uint64_t outmask;
+    uint64_t start;
+    uint64_t count;
+};
+
+// A pair as the exhaustive kernels see it, staged in shared memory.
+struct PairView {
+    const uint16_t* t;
+    const uint16_t* c;
+    int tn, cn;
+    uint32_t dead;
+};
+
+// Pair sources: survivors of the enumeration pipeline, or explicit CSR pairs.
+struct SurvSource {
+    const Surv* surv;
+    const uint16_t* targets;
+    uint32_t tlen;
+    uint32_t run_dead;
+    int go;
+    __device__ void load(uint64_t p, uint16_t* st, uint16_t* sc, int& tn, int& cn, uint32_t& dead,
+                         int lane) const {
+        Surv s = surv[p];
+        tn = (int)tlen;
+        if (lane < (int)tlen) st[lane] = targets[(uint64_t)s.t * tlen + lane];
+        uint32_t idx = s.c & 0x7FFFFFu;
+        if (s.c & kSurvLen2) {
+            cn = 2;
+            if (lane == 0) { sc[0] = c_tab[idx / kNumInsns]; sc[1] = c_tab[idx % kNumInsns]; }
+        } else {
+            cn = 1;
+            if (lane == 0) sc[0] = c_tab[idx];
+        }
+        dead = go ? ((s.c & kSurvMasked) ? run_dead : 0u) : run_dead;
+    }
+};
+
+struct CsrSource {
+    const uint16_t* t_ins;
+    const uint32_t* t_off;
+    const uint16_t* c_ins;
+    const uint32_t* c_off;
+    uint32_t dead_;
+    __device__ void load(uint64_t p, uint16_t* st, uint16_t* sc, int& tn, int& cn, uint32_t& dead,
+                         int lane) const {
+        uint32_t t0 = t_off[p], c0 = c_off[p];
+        tn = (int)(t_off[p + 1] - t0);
+        cn = (int)(c_off[p + 1] - c0);
+        if (lane < tn) st[lane] = t_ins[t0 + lane];
+        if (lane < cn) sc[lane] = c_ins[c0 + lane];
+        dead = dead_;
+    }
+};
+
+// Decode parameters of one cone sweep.  State index bits: A (8, if in the
+// cone), carry (1), then each swept extra register in the cone (8 bits, or 5
+// bits indexing the representative values).
+struct Fields {
+    uint32_t sh[8], mk[8], base[8];   // order: A, X, Y, S, M, S0, S1, carry
+    uint32_t rep_mask;                // fields translated through c_rep
+    uint32_t bits;
+};
+
+__device__ __forceinline__ Fields make_fields(uint32_t cone, uint32_t swept, bool rep) {
+    Fields f;
+    uint32_t bit = 0;
+    const uint32_t locs[8] = {L_A, L_X, L_Y, L_S, L_M, L_S0, L_S1, L_C};
+    f.rep_mask = 0;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+        uint32_t l = locs[i];
+        f.sh[i] = 0; f.mk[i] = 0;
+        f.base[i] = (l == L_S && !(swept & LB(L_S))) ? 0xFDu : 0u;
+        if (cone & LB(l)) {
+            uint32_t w = (l == L_C) ? 1u : ((rep && l != L_A) ? 5u : 8u);
+            f.sh[i] = bit; f.mk[i] = (1u << w) - 1u; f.base[i] = 0;
+            if (rep && l != L_A && l != L_C) f.rep_mask |= 1u << i;
+            bit += w;
+        }
+    }
+    f.bits = bit;
+    return f;
+}
+
+__device__ __forceinline__ uint32_t fld(const Fields& f, int i, uint64_t s) {
+    uint32_t v = (uint32_t)(s >> f.sh[i]) & f.mk[i];
+    if (f.rep_mask & (1u << i)) v = c_rep[v];
+    return v | f.base[i];
+}
+
+// Sweeps states [s0, s1) of one cone; true when target and candidate agree
+// on the compared outputs in every state.  Warp-collective.  When `stop`
+// becomes nonzero (another item of the same pair failed) the sweep ends
+// early; its result is then irrelevant.
+__device__ __forceinline__ bool sweep_states(const PairView& pv, const Fields& f, uint64_t om, uint64_t s0,
+                             uint64_t s1, const volatile uint32_t* stop, unsigned long long* nstates,
+                             int lane) {
+    const uint32_t ma = (uint32_t)om & 0xFFu, mx = (uint32_t)(om >> 8) & 0xFFu,
+                   my = (uint32_t)(om >> 16) & 0xFFu, mp = (uint32_t)(om >> 24) & 0xFFu,
+                   ms = (uint32_t)(om >> 32) & 0xFFu, mm = (uint32_t)(om >> 40) & 0xFFu,
+                   m0 = (uint32_t)(om >> 48) & 0xFFu, m1 = (uint32_t)(om >> 56) & 0xFFu;
+    uint64_t iter = 0;
+    for (uint64_t b = s0; b < s1; b += 32, iter++) {
+        uint64_t s = b + (uint64_t)lane;
+        uint32_t d = 0;
+        if (s < s1) {
+            St in;
+            in.a = fld(f, 0, s); in.x = fld(f, 1, s); in.y = fld(f, 2, s); in.s = fld(f, 3, s);
+            in.m = fld(f, 4, s); in.s0 = fld(f, 5, s); in.s1 = fld(f, 6, s); in.p = fld(f, 7, s);
+            St t = in, c = in;
+            for (int i = 0; i < pv.tn; i++) exec(t, pv.t[i]);
+            for (int i = 0; i < pv.cn; i++) exec(c, pv.c[i]);
+            d = ((t.a ^ c.a) & ma) | ((t.x ^ c.x) & mx) | ((t.y ^ c.y) & my) | ((t.p ^ c.p) & mp) |
+                ((t.s ^ c.s) & ms) | ((t.m ^ c.m) & mm) | ((t.s0 ^ c.s0) & m0) | ((t.s1 ^ c.s1) & m1);
+        }
+        if (__any_sync(kFull, d != 0)) {
+            if (lane == 0) *nstates += (b - s0) + 32;
+            return false;
+        }
+        if ((iter & 255) == 255 && stop) {
+            uint32_t sv = lane == 0 ? *stop : 0u;   // one read, broadcast: keeps the warp uniform
+            if (__shfl_sync(kFull, sv, 0)) break;
+        }
+    }
+    if (lane == 0) *nstates += s1 - s0;
+    return true;
+}
+
+// Swept locations, written locations and input cones of a pair.  Lane l
+// (l < 13) ends with the cone of output location l.
+struct Flow {
+    uint32_t swept;      // A, carry and the extra registers opReads implies
+    uint32_t written;    // locations either sequence writes
+    uint32_t cone;       // this lane's output cone (within `swept`)
+    int k;               // extra registers swept
+};
+
+__device__ __forceinline__ uint32_t compose(uint32_t D, const uint16_t* seq, int n, int lane,
+                                            uint32_t& written, uint32_t& sweep) {
+    for (int i = 0; i < n; i++) {
+        uint32_t op = seq[i] & 0xFFu;
+        uint32_t dep = (lane < NUM_LOCS) ? c_dep[op][lane] : 0u;
+        uint32_t nd = 0;
+#pragma unroll
+        for (int l = 0; l < NUM_LOCS; l++) {
+            uint32_t x = __shfl_sync(kFull, D, l);
+            if (dep & (1u << l)) nd |= x;
+        }
+        D = nd;
+        written |= c_wr[op];
+        sweep |= c_sweep[op];
+    }
+    return D;
+}
+
+__device__ __forceinline__ Flow dataflow(const PairView& pv, int lane) {
+    Flow fl;
+    uint32_t wt = 0, wc = 0, sw = 0;
+    uint32_t id = (lane < NUM_LOCS) ? (1u << lane) : 0u;
+    uint32_t dt = compose(id, pv.t, pv.tn, lane, wt, sw);
+    uint32_t dc = compose(id, pv.c, pv.cn, lane, wc, sw);
+    fl.k = __popc(sw);
+    fl.swept = sw | LB(L_A) | LB(L_C);
+    fl.written = wt | wc;
+    fl.cone = (dt | dc) & fl.swept;
+    return fl;
+}
+
+// Groups of a pair: maximal cones among the compared outputs; each group
+// compares every output whose cone it contains.
+struct Groups {
+    int n;
+    uint16_t cone[NUM_LOCS];
+    uint64_t mask[NUM_LOCS];
+    uint32_t bits[NUM_LOCS];
+};
+
+__device__ __forceinline__ uint32_t cone_bits(uint32_t cone, bool rep) {
+    uint32_t b = 0;
+    if (cone & LB(L_A)) b += 8;
+    if (cone & LB(L_C)) b += 1;
+    uint32_t extra = cone & ~(LB(L_A) | LB(L_C));
+    b += (uint32_t)__popc(extra) * (rep ? 5u : 8u);
+    return b;
+}
+
+__device__ Groups make_groups(const Flow& fl, uint32_t dead, bool rep, bool brute, int lane) {
+    Groups g;
+    g.n = 0;
+    if (brute) {
+        g.n = 1;
+        g.cone[0] = (uint16_t)fl.swept;
+        g.mask[0] = cmp_mask(dead);
+        g.bits[0] = cone_bits(fl.swept, rep);
+        return g;
+    }
+    uint32_t deadlocs = 0;
+    for (uint32_t l = L_C; l <= L_N; l++) if (dead & flag_bit(l)) deadlocs |= LB(l);
+    uint32_t active = fl.written & ~deadlocs;
+    uint32_t cones[NUM_LOCS];
+#pragma unroll
+    for (int l = 0; l < NUM_LOCS; l++) cones[l] = __shfl_sync(kFull, fl.cone, l);
+    for (int o = 0; o < NUM_LOCS; o++) {
+        if (!(active & (1u << o))) continue;
+        bool maximal = true;
+        for (int q = 0; q < NUM_LOCS && maximal; q++) {
+            if (q == o || !(active & (1u << q))) continue;
+            bool sup = (cones[q] & cones[o]) == cones[o];
+            if (sup && (cones[q] != cones[o] || q < o)) maximal = false;
+        }
+        if (!maximal) continue;
+        uint64_t m = 0;
+        for (int q = 0; q < NUM_LOCS; q++)
+            if ((active & (1u << q)) && (cones[q] & cones[o]) == cones[q]) m |= loc_mask64((uint32_t)q);
+        g.cone[g.n] = (uint16_t)cones[o];
+        g.mask[g.n] = m;
+        g.bits[g.n] = cone_bits(cones[o], rep);
+        g.n++;
+    }
+    // smallest sweeps first: cheap groups reject failing pairs early
+    for (int i = 1; i < g.n; i++)
+        for (int j = i; j > 0 && g.bits[j] < g.bits[j - 1]; j--) {
+            uint16_t tc = g.cone[j]; g.cone[j] = g.cone[j - 1]; g.cone[j - 1] = tc;
+            uint64_t tm = g.mask[j]; g.mask[j] = g.mask[j - 1]; g.mask[j - 1] = tm;
+            uint32_t tb = g.bits[j]; g.bits[j] = g.bits[j - 1]; g.bits[j - 1] = tb;
+        }
+    (void)lane;
+    return g;
+}
+
+struct ExhArgs {
+    uint32_t* fail;              // per pair: 1 = not equivalent
+    Item* items;
+    uint64_t item_cap;
+    Counters* cnt;
+    uint32_t sweep;              // M6502_SWEEP_*
+    uint32_t brute;
+};
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+
+// Fingerprints: warp per sequence, lane v = test vector v.  out: 32 packed
+// states per sequence (P & PMask); meta (optional): CUDA bytes | Go bytes << 4.
+struct FixedSeqs {
+    const uint16_t* p;
+    uint32_t len;
+    __device__ int load(uint64_t i, uint16_t* dst, int lane) const {
+        if (lane < (int)len) dst[lane] = p[i * len + lane];
+        return (int)len;
+    }
+};
+struct CsrSeqs {
+    const uint16_t* ins;
+    const uint32_t* off;
+    __device__ int load(uint64_t i, uint16_t* dst, int lane) const {
+        uint32_t a = off[i], n = off[i + 1] - a;
+        if (lane < (int)n) dst[lane] = ins[a + lane];
+        return (int)n;
+    }
+};
+struct CandSeqs {
+    uint32_t len;
+    __device__ int load(uint64_t i, uint16_t* dst, int lane) const {
+        if (lane == 0) {
+            if (len == 1) dst[0] = c_tab[i];
+            else { dst[0] = c_tab[i / kNumInsns]; dst[1] = c_tab[i % kNumInsns]; }
+        }
+        return (int)len;
+    }
+};
+
+template <class Src>
+__global__ void __launch_bounds__(256) k_fingerprint(Src src, uint64_t n, uint64_t* __restrict__ out,
+                                                      uint8_t* __restrict__ meta) {
+    __shared__ uint16_t s_seq[kWarpsPerBlock][kMaxSeq];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint64_t nw = (uint64_t)gridDim.x * kWarpsPerBlock;
+    for (uint64_t i = (uint64_t)blockIdx.x * kWarpsPerBlock + w; i < n; i += nw) {
+        int len = src.load(i, s_seq[w], lane);
+        __syncwarp();
+        St s = unpack(c_vec[lane]);
+        for (int k = 0; k < len; k++) exec(s, s_seq[w][k]);
+        out[i * 32 + lane] = fp_of(s);
+        if (meta && lane == 0) {
+            uint32_t bc = 0, bg = 0;
+            for (int k = 0; k < len; k++) { bc += bytes_cuda(s_seq[w][k] & 0xFFu); bg += bytes_go(s_seq[w][k] & 0xFFu); }
+            meta[i] = (uint8_t)(min(bc, 15u) | (min(bg, 15u) << 4));
+        }
+        __syncwarp();
+    }
+}
+
+// Warp-aggregated append of one record per passing lane (all 32 lanes call).
+__device__ __forceinline__ void append_surv(bool pass, Surv rec, Surv* out, uint64_t cap,
+                                            unsigned long long* counter, int lane) {
+    unsigned vote = __ballot_sync(kFull, pass);
+    if (!vote) return;
+    int leader = __ffs(vote) - 1;
+    unsigned long long base = 0;
+    if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(vote));
+    base = __shfl_sync(kFull, base, leader);
+    if (pass) {
+        unsigned long long idx = base + (unsigned long long)__popc(vote & ((1u << lane) - 1u));
+        if (idx < cap) out[idx] = rec;
+    }
+}
+
+// QC (+ MidCheck) of targets x all length-1 candidates.
+constexpr int kQcTile = 64;
+constexpr int kQcPerThread = 12;   // 256 x 12 = 3072 >= 2863 candidates
+
+template <bool GO>
+__global__ void __launch_bounds__(256) k_qc1(const uint64_t* __restrict__ tfp, const uint8_t* __restrict__ tmeta,
+                                              uint32_t nt, const uint64_t* __restrict__ cfp,
+                                              const uint8_t* __restrict__ cmeta, uint32_t dead,
+                                              uint32_t stages, Surv* __restrict__ surv, uint64_t cap,
+                                              Counters* __restrict__ cnt) {
+    __shared__ uint64_t s_t0[kQcTile];
+    __shared__ uint8_t s_tb[kQcTile];
+    const int lane = threadIdx.x & 31;
+    const uint64_t loose = cmp_mask(dead), exact = cmp_mask(0);
+    uint64_t c0[kQcPerThread];
+    uint32_t cm[kQcPerThread];
+#pragma unroll
+    for (int j = 0; j < kQcPerThread; j++) {
+        uint32_t c = threadIdx.x + 256u * (uint32_t)j;
+        if (c < (uint32_t)kNumInsns) { c0[j] = cfp[c]; cm[j] = cmeta[c]; }
+        else { c0[j] = 0; cm[j] = 0x80u; }   // padding lane: always filtered
+    }
+    unsigned long long nqc = 0, nmid = 0;
+    const uint32_t ntiles = (nt + kQcTile - 1) / kQcTile;
+    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        __syncthreads();
+        if (threadIdx.x < kQcTile) {
+            uint32_t t = tile * kQcTile + threadIdx.x;
+            s_t0[threadIdx.x] = t < nt ? tfp[(uint64_t)t * 32] : 0;
+            s_tb[threadIdx.x] = t < nt ? tmeta[t] : 0;
+        }
+        __syncthreads();
+        const int tcount = (int)min((uint32_t)kQcTile, nt - tile * kQcTile);
+        for (int k = 0; k < tcount; k++) {
+            const uint64_t t0 = s_t0[k];
+            uint32_t hm = 0;
+#pragma unroll
+            for (int j = 0; j < kQcPerThread; j++) hm |= (((t0 ^ c0[j]) & loose) == 0 ? 1u : 0u) << j;
+            if (!__any_sync(kFull, hm != 0)) continue;
+            const uint32_t t = tile * kQcTile + (uint32_t)k;
+            const uint32_t tb = GO ? (s_tb[k] >> 4) : (s_tb[k] & 15u);
+            const uint64_t* trow = tfp + (uint64_t)t * 32;
+#pragma unroll
+            for (int j = 0; j < kQcPerThread; j++) {
+                bool pass = false;
+                uint32_t code = 0;
+                const uint32_t c = threadIdx.x + 256u * (uint32_t)j;
+                if (hm & (1u << j)) {
+                    const uint32_t cb = GO ? ((cm[j] >> 2) & 3u) : (cm[j] & 3u);
+                    if (!(cm[j] & 0x90u) && cb < tb) {   // not pruned, not padding, shorter
+                        bool qc = true, ex = ((t0 ^ c0[j]) & exact) == 0;
+                        for (int v = 1; v < 8 && qc; v++) {
+                            uint64_t x = trow[v] ^ cfp[(uint64_t)v * kNumInsns + c];
+                            qc = (x & loose) == 0;
+                            ex = ex && (x & exact) == 0;
+                        }
+                        if (qc) {
+                            if (!GO) {
+                                nqc++;
+                                bool mid = true;
+                                if (stages & M6502_CHECK_MID)
+                                    for (int v = 8; v < 32 && mid; v++)
+                                        mid = ((trow[v] ^ cfp[(uint64_t)v * kNumInsns + c]) & loose) == 0;
+                                if (mid) { nmid++; pass = true; code = c; }
+                            } else if (ex) {           // processTask: unmasked QC passes
+                                nqc++; nmid++; pass = true; code = c;
+                            } else if (dead) {         // processTaskMasked
+                                uint32_t fd = 0;
+                                for (int v = 0; v < 8; v++)
+                                    fd |= (uint32_t)((trow[v] ^ cfp[(uint64_t)v * kNumInsns + c]) >> 24) & kPMask;
+                                if (fd) { nqc++; nmid++; pass = true; code = c | kSurvMasked | (fd_pack(fd) << 25); }
+                            }
+                        }
+                    }
+                }
+                append_surv(pass, Surv{t, code}, surv, cap, &cnt->surv, lane);
+            }
+        }
+    }
+    // one atomic per warp for the stage counters
+    for (int o = 16; o; o >>= 1) {
+        nqc += __shfl_down_sync(kFull, nqc, o);
+        nmid += __shfl_down_sync(kFull, nmid, o);
+    }
+    if (lane == 0) {
+        if (nqc) atomicAdd(&cnt->qc, nqc);
+        if (nmid) atomicAdd(&cnt->mid, nmid);
+    }
+}
+
+// Exhaustive check, one pair per warp (persistent, device ticket).
+template <class Src>
+__global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long long* n_pairs_ptr,
+                                                     uint64_t n_cap, ExhArgs a) {
+    __shared__ uint16_t s_t[kWarpsPerBlock][kMaxSeq], s_c[kWarpsPerBlock][kMaxSeq];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint64_t n = min((uint64_t)*n_pairs_ptr, n_cap);
+    unsigned long long nstates = 0;
+    for (;;) {
+        unsigned long long p = 0;
+        if (lane == 0) p = atomicAdd(&a.cnt->exh_ticket, 1ull);
+        p = __shfl_sync(kFull, p, 0);
+        if (p >= n) break;
+        PairView pv;
+        pv.t = s_t[w]; pv.c = s_c[w];
+        src.load(p, s_t[w], s_c[w], pv.tn, pv.cn, pv.dead, lane);
+        __syncwarp();
+        Flow fl = dataflow(pv, lane);
+        const bool rep = a.sweep == M6502_SWEEP_REFERENCE && fl.k >= 3;
+        Groups g = make_groups(fl, pv.dead, rep, a.brute != 0, lane);
+        bool ok = true;
+        uint32_t big = 0;   // groups left for the work queue
+        for (int i = 0; i < g.n && ok; i++) {
+            Fields f = make_fields(g.cone[i], fl.swept, rep);
+            uint64_t total = 1ull << g.bits[i];
+            uint64_t end = total <= kSmallSweep ? total : kProbe;
+            ok = sweep_states(pv, f, g.mask[i], 0, end, nullptr, &nstates, lane);
+            if (ok && end < total) big |= 1u << i;
+        }
+        if (ok && big) {
+            for (int i = 0; i < g.n; i++) {
+                if (!(big & (1u << i))) continue;
+                uint64_t total = 1ull << g.bits[i];
+                uint64_t nitems = (total - kProbe + kChunk - 1) / kChunk;
+                unsigned long long base = 0;
+                if (lane == 0) base = atomicAdd(&a.cnt->items, (unsigned long long)nitems);
+                base = __shfl_sync(kFull, base, 0);
+                for (uint64_t j = lane; j < nitems; j += 32) {
+                    if (base + j >= a.item_cap) break;
+                    Item it;
+                    it.pair = (uint32_t)p; it.cone = g.cone[i]; it.rep = rep ? 1 : 0; it.pad = 0;
+                    it.outmask = g.mask[i];
+                    it.start = kProbe + j * kChunk;
+                    it.count = min(kChunk, total - it.start);
+                    a.items[base + j] = it;
+                }
+            }
+        }
+        if (lane == 0) a.fail[p] = ok ? 0u : 1u;
+        __syncwarp();
+    }
+    if (lane == 0 && nstates) atomicAdd(&a.cnt->states, nstates);
+}
+
+template <class Src>
+__global__ void __launch_bounds__(256) k_exh_items(Src src, ExhArgs a) {
+    __shared__ uint16_t s_t[kWarpsPerBlock][kMaxSeq], s_c[kWarpsPerBlock][kMaxSeq];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint64_t n = min((uint64_t)a.cnt->items, a.item_cap);
+    unsigned long long nstates = 0;
+    for (;;) {
+        unsigned long long q = 0;
+        if (lane == 0) q = atomicAdd(&a.cnt->item_ticket, 1ull);
+        q = __shfl_sync(kFull, q, 0);
+        if (q >= n) break;
+        const Item it = a.items[q];
+        volatile uint32_t* flag = a.fail + it.pair;
+        uint32_t fv = lane == 0 ? *flag : 0u;
+        if (__shfl_sync(kFull, fv, 0)) continue;
+        PairView pv;
+        pv.t = s_t[w]; pv.c = s_c[w];
+        src.load(it.pair, s_t[w], s_c[w], pv.tn, pv.cn, pv.dead, lane);
+        __syncwarp();
+        Flow fl = dataflow(pv, lane);
+        Fields f = make_fields(it.cone, fl.swept, it.rep != 0);
+        bool ok = sweep_states(pv, f, it.outmask, it.start, it.start + it.count, flag, &nstates, lane);
+        if (!ok && lane == 0) *flag = 1u;
+        __syncwarp();
+    }
+    if (lane == 0 && nstates) atomicAdd(&a.cnt->states, nstates);
+}
+
+// Algorithmic work of one passing pair under the fixed measurement
+// convention: every state of the product sweep (2^(9+8k), or 512 x 32^k for
+// the reduced sweep) costs 10 ops per executed instruction + 3 per compare.
+__device__ __forceinline__ unsigned long long algo_ops(const uint16_t* t, uint32_t tn, const uint16_t* c,
+                                                       uint32_t cn, uint32_t sweep_mode) {
+    uint32_t sw = 0;
+    for (uint32_t i = 0; i < tn; i++) sw |= c_sweep[t[i] & 0xFFu];
+    for (uint32_t i = 0; i < cn; i++) sw |= c_sweep[c[i] & 0xFFu];
+    uint32_t k = (uint32_t)__popc(sw);
+    uint32_t bits = 9 + k * ((sweep_mode == M6502_SWEEP_REFERENCE && k >= 3) ? 5u : 8u);
+    return (1ull << bits) * (unsigned long long)(10 * (tn + cn) + 3);
+}
+
+// CUDA semantics: every passing survivor is a rule.
+__global__ void k_emit_all(const Surv* __restrict__ surv, const unsigned long long* n_ptr, uint64_t n_cap,
+                           const uint32_t* __restrict__ fail, const uint64_t* __restrict__ ids,
+                           uint32_t run_dead, m6502_rule* __restrict__ rules, uint64_t rcap,
+                           Counters* cnt, int check_exh, const uint16_t* __restrict__ targets,
+                           uint32_t tlen, uint32_t sweep_mode) {
+    const uint64_t n = min((uint64_t)*n_ptr, n_cap);
+    const int lane = threadIdx.x & 31;
+    unsigned long long npass = 0, algo = 0;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t p = base + threadIdx.x;
+        bool pass = p < n && (!check_exh || fail[p] == 0);
+        m6502_rule r;
+        memset(&r, 0, sizeof r);
+        if (pass) {
+            Surv s = surv[p];
+            uint32_t idx = s.c & 0x7FFFFFu;
+            r.target = ids ? ids[s.t] : s.t;
+            r.dead_flags = (uint8_t)run_dead;
+            if (s.c & kSurvLen2) { r.cand_len = 2; r.cand[0] = c_tab[idx / kNumInsns]; r.cand[1] = c_tab[idx % kNumInsns]; }
+            else { r.cand_len = 1; r.cand[0] = c_tab[idx]; }
+            npass++;
+            if (check_exh) algo += algo_ops(targets + (uint64_t)s.t * tlen, tlen, r.cand, r.cand_len, sweep_mode);
+        }
+        unsigned vote = __ballot_sync(kFull, pass);
+        if (vote) {
+            int leader = __ffs(vote) - 1;
+            unsigned long long b = 0;
+            if (lane == leader) b = atomicAdd(&cnt->rules, (unsigned long long)__popc(vote));
+            b = __shfl_sync(kFull, b, leader);
+            if (pass) {
+                unsigned long long idx = b + __popc(vote & ((1u << lane) - 1u));
+                if (idx < rcap) rules[idx] = r;
+            }
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        npass += __shfl_down_sync(kFull, npass, o);
+        algo += __shfl_down_sync(kFull, algo, o);
+    }
+    if (lane == 0 && npass) atomicAdd(&cnt->exh_pass, npass);
+    if (lane == 0 && algo) atomicAdd(&cnt->algo, algo);
+}
+
+// Go semantics: first passing candidate per target and pass, in Go order
+// (shorter candidates first, then Go enumeration order).
+__global__ void k_go_select(const Surv* __restrict__ surv, const unsigned long long* n_ptr, uint64_t n_cap,
+                            const uint32_t* __restrict__ fail, uint32_t nt, uint32_t* __restrict__ best,
+                            Counters* cnt, const uint16_t* __restrict__ targets, uint32_t tlen,
+                            uint32_t sweep_mode) {
+    const uint64_t n = min((uint64_t)*n_ptr, n_cap);
+    unsigned long long npass = 0, algo = 0;
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+        if (fail[p]) continue;
+        npass++;
+        Surv s = surv[p];
+        uint32_t idx = s.c & 0x7FFFFFu, key;
+        if (s.c & kSurvLen2) key = (1u << 28) | (c_gorank[idx / kNumInsns] * kNumInsns + c_gorank[idx % kNumInsns]);
+        else key = c_gorank[idx];
+        // keep FlagDiff beside the rank so the winner carries its own
+        uint64_t pass = (s.c & kSurvMasked) ? 1 : 0;
+        atomicMin(&best[pass * nt + s.t], key);
+        uint16_t cand[2];
+        uint32_t cn = (s.c & kSurvLen2) ? 2u : 1u;
+        if (cn == 2) { cand[0] = c_tab[idx / kNumInsns]; cand[1] = c_tab[idx % kNumInsns]; }
+        else cand[0] = c_tab[idx];
+        algo += algo_ops(targets + (uint64_t)s.t * tlen, tlen, cand, cn, sweep_mode);
+    }
+    if (npass) atomicAdd(&cnt->exh_pass, npass);
+    if (algo) atomicAdd(&cnt->algo, algo);
+}
+
+__global__ void k_go_emit(const uint32_t* __restrict__ best, uint32_t nt, const uint16_t* __restrict__ targets,
+                          uint32_t tlen, const uint64_t* __restrict__ ids, m6502_rule* __restrict__ rules,
+                          uint64_t rcap, Counters* cnt) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nt; t += gridDim.x * blockDim.x) {
+        for (int pass = 0; pass < 2; pass++) {
+            uint32_t key = best[(uint64_t)pass * nt + t];
+            if (key == 0xFFFFFFFFu) continue;
+            m6502_rule r;
+            memset(&r, 0, sizeof r);
+            r.target = ids ? ids[t] : t;
+            if (key >> 28) {
+                uint32_t rk = key & 0x0FFFFFFFu;
+                r.cand_len = 2; r.cand[0] = c_gotab[rk / kNumInsns]; r.cand[1] = c_gotab[rk % kNumInsns];
+            } else {
+                r.cand_len = 1; r.cand[0] = c_gotab[key];
+            }
+            if (pass == 1) {   // FlagDiff over the QC vectors (verifier.go:591-604)
+                uint32_t fd = 0;
+                for (int v = 0; v < 8; v++) {
+                    St a = unpack(c_vec[v]), b = a;
+                    for (uint32_t i = 0; i < tlen; i++) exec(a, targets[(uint64_t)t * tlen + i]);
+                    for (int i = 0; i < r.cand_len; i++) exec(b, r.cand[i]);
+                    fd |= (a.p ^ b.p) & kPMask;
+                }
+                r.dead_flags = (uint8_t)fd;
+            }
+            unsigned long long idx = atomicAdd(&cnt->rules, 1ull);
+            if (idx < rcap) rules[idx] = r;
+        }
+    }
+}
+
+// Pairwise QC / MidCheck / FlagDiff: warp per pair, lane = vector.
+__global__ void __launch_bounds__(256) k_pair_vectors(CsrSource src, uint64_t n, uint8_t* __restrict__ out,
+                                                       uint8_t* __restrict__ fdiff) {
+    __shared__ uint16_t s_t[kWarpsPerBlock][kMaxSeq], s_c[kWarpsPerBlock][kMaxSeq];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (uint64_t p = (uint64_t)blockIdx.x * kWarpsPerBlock + w; p < n; p += (uint64_t)gridDim.x * kWarpsPerBlock) {
+        int tn, cn;
+        uint32_t dead;
+        src.load(p, s_t[w], s_c[w], tn, cn, dead, lane);
+        __syncwarp();
+        St a = unpack(c_vec[lane]), b = a;
+        for (int i = 0; i < tn; i++) exec(a, s_t[w][i]);
+        for (int i = 0; i < cn; i++) exec(b, s_c[w][i]);
+        uint64_t x = pack(a) ^ pack(b);
+        bool eq = (x & cmp_mask(dead)) == 0;
+        unsigned ev = __ballot_sync(kFull, eq);
+        bool nonp = (x & 0xFFFFFFFF00FFFFFFull) == 0;
+        unsigned nv = __ballot_sync(kFull, nonp);
+        uint32_t pd = (lane < 8) ? ((uint32_t)(x >> 24) & kPMask) : 0u;
+        for (int o = 16; o; o >>= 1) pd |= __shfl_xor_sync(kFull, pd, o);
+        if (lane == 0) {
+            uint8_t r = 0;
+            if ((ev & 0xFFu) == 0xFFu) r |= 1;
+            if (ev == kFull) r |= 2;
+            out[p] = r;
+            if (fdiff) fdiff[p] = (uint8_t)(((nv & 0xFFu) == 0xFFu) ? pd : 0u);
+        }
+        __syncwarp();
+    }
+}
+
+// Runs sequence i on packed input state in[i] (thread per sequence).
+__global__ void k_exec_batch(CsrSeqs src, uint64_t n, const uint64_t* __restrict__ in, uint64_t* __restrict__ out) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        St s = unpack(in[i]);
+        for (uint32_t k = src.off[i]; k < src.off[i + 1]; k++) exec(s, src.ins[k]);
+        out[i] = pack(s);
+    }
+}
+
+// Pruned target enumeration: ids in [id0, id1) of the length-L space,
+// compacted into targets/ids (order unspecified).
+__global__ void k_enum_targets(uint64_t id0, uint64_t id1, uint32_t len, uint16_t* __restrict__ targets,
+                               uint64_t* __restrict__ ids, uint64_t cap, unsigned long long* count) {
+    const int lane = threadIdx.x & 31;
+    for (uint64_t base = id0 + (uint64_t)blockIdx.x * blockDim.x; base < id1; base += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t id = base + threadIdx.x;
+        uint16_t s[3] = {0, 0, 0};
+        bool keep = false;
+        if (id < id1) {
+            uint64_t r = id;
+            for (int k = (int)len - 1; k >= 0; k--) { s[k] = c_tab[r % kNumInsns]; r /= kNumInsns; }
+            keep = !should_prune(s, (int)len);
+        }
+        unsigned vote = __ballot_sync(kFull, keep);
+        if (!vote) continue;
+        int leader = __ffs(vote) - 1;
+        unsigned long long b = 0;
+        if (lane == leader) b = atomicAdd(count, (unsigned long long)__popc(vote));
+        b = __shfl_sync(kFull, b, leader);
+        if (keep) {
+            unsigned long long idx = b + __popc(vote & ((1u << lane) - 1u));
+            if (idx < cap) {
+                for (uint32_t k = 0; k < len; k++) targets[idx * len + k] = s[k];
+                ids[idx] = id;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct m6502_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t sev[6] = {};   // stage boundaries of one pass
+    std::string err;
+    std::mutex mu;
+    int sms = 148;
+    int exh_blocks = 0, exh_item_blocks = 0, qc_blocks = 0, fp_blocks = 0;
+    uint64_t pass_targets = 1ull << 21;
+    bool ready = false;
+    DevBuf cfp1, cmeta1, targets, ids, tfp, tmeta, surv, fail, items, rules, cnt, best, pins, poffs,
+        cins, coffs, pout, pfd, enum_count;
+    std::vector<m6502_rule> staging;
+};
+
+namespace {
+
+int set_err(m6502_ctx* ctx, int code, const std::string& msg) {
+    ctx->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                            \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return set_err(ctx, e_ == cudaErrorMemoryAllocation ? M6502_E_NOMEM : M6502_E_CUDA, \
+                           std::string(#call) + ": " + cudaGetErrorString(e_));             \
+    } while (0)
+
+#define CKL(what)                                                                           \
+    do {                                                                                    \
+        cudaError_t e_ = cudaGetLastError();                                                \
+        if (e_ != cudaSuccess)                                                              \
+            return set_err(ctx, M6502_E_CUDA, std::string("launch ") + what + ": " +        \
+                                                  cudaGetErrorString(e_));                  \
+    } while (0)
+
+int ensure(m6502_ctx* ctx, DevBuf& b, size_t bytes) {
+    if (b.bytes >= bytes && b.p) return M6502_OK;
+    if (b.p) { cudaFree(b.p); b.p = nullptr; b.bytes = 0; }
+    size_t want = std::max<size_t>(bytes, 256);
+    CK(cudaMalloc(&b.p, want));
+    b.bytes = want;
+    return M6502_OK;
+}
+
+#define TRY(x)                      \
+    do {                            \
+        int rc_ = (x);              \
+        if (rc_ != M6502_OK) return rc_; \
+    } while (0)
+
+int init_ctx(m6502_ctx* ctx) {
+    if (ctx->ready) return M6502_OK;
+    CK(cudaSetDevice(ctx->device));
+    uint64_t vec[32];
+    for (int v = 0; v < 32; v++) {
+        uint64_t x = 0;
+        for (int b = 0; b < 8; b++) x |= (uint64_t)kVectors[v][b] << (8 * b);
+        vec[v] = x;
+    }
+    uint16_t dep[NUM_OPS][NUM_LOCS], wr[NUM_OPS], sw[NUM_OPS];
+    for (uint32_t op = 0; op < NUM_OPS; op++) {
+        wr[op] = (uint16_t)op_deps(op, dep[op]);
+        sw[op] = (uint16_t)sweep_locs_of_reads(op_reads(op));
+    }
+    static uint16_t tab[kNumInsns], gotab[kNumInsns];
+    static uint32_t gorank[kNumInsns];
+    host_tables(tab, gotab, gorank);
+    uint32_t rep[32];
+    for (int i = 0; i < 32; i++) rep[i] = kRepValues[i];
+    CK(cudaMemcpyToSymbol(c_vec, vec, sizeof vec));
+    CK(cudaMemcpyToSymbol(c_dep, dep, sizeof dep));
+    CK(cudaMemcpyToSymbol(c_wr, wr, sizeof wr));
+    CK(cudaMemcpyToSymbol(c_sweep, sw, sizeof sw));
+    CK(cudaMemcpyToSymbol(c_tab, tab, sizeof tab));
+    CK(cudaMemcpyToSymbol(c_gotab, gotab, sizeof gotab));
+    CK(cudaMemcpyToSymbol(c_gorank, gorank, sizeof gorank));
+    CK(cudaMemcpyToSymbol(c_rep, rep, sizeof rep));
+
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_exhaustive<SurvSource>, 256, 0));
+    ctx->exh_blocks = ctx->sms * std::max(occ, 1);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_exh_items<SurvSource>, 256, 0));
+    ctx->exh_item_blocks = ctx->sms * std::max(occ, 1);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_qc1<false>, 256, 0));
+    ctx->qc_blocks = ctx->sms * std::max(occ, 1);
+    ctx->fp_blocks = ctx->sms * 8;
+
+    // length-1 candidate fingerprints and metadata
+    TRY(ensure(ctx, ctx->cfp1, sizeof(uint64_t) * 32 * kNumInsns));
+    TRY(ensure(ctx, ctx->cmeta1, kNumInsns));
+    DevBuf tmp;
+    TRY(ensure(ctx, tmp, sizeof(uint64_t) * 32 * kNumInsns));
+    k_fingerprint<CandSeqs><<<ctx->fp_blocks, 256, 0, ctx->stream>>>(CandSeqs{1}, kNumInsns,
+                                                                     (uint64_t*)tmp.p, nullptr);
+    CKL("k_fingerprint(candidates)");
+    std::vector<uint64_t> h(32 * (size_t)kNumInsns), tr(32 * (size_t)kNumInsns);
+    CK(cudaMemcpyAsync(h.data(), tmp.p, h.size() * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(tmp.p);
+    for (int c = 0; c < kNumInsns; c++)
+        for (int v = 0; v < 32; v++) tr[(size_t)v * kNumInsns + c] = h[(size_t)c * 32 + v];
+    std::vector<uint8_t> meta(kNumInsns);
+    for (int c = 0; c < kNumInsns; c++) {
+        uint32_t op = tab[c] & 0xFF;
+        uint16_t one = tab[c];
+        meta[c] = (uint8_t)(bytes_cuda(op) | (bytes_go(op) << 2) | (should_prune(&one, 1) ? 0x10 : 0));
+    }
+    CK(cudaMemcpyAsync(ctx->cfp1.p, tr.data(), tr.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->cmeta1.p, meta.data(), meta.size(), cudaMemcpyHostToDevice, ctx->stream));
+    TRY(ensure(ctx, ctx->cnt, sizeof(Counters)));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->ready = true;
+    return M6502_OK;
+}
+
+struct PassOut {
+    Counters c;
+};
+
+// One device pass: nt targets (device pointer) of length tlen.  Appends the
+// rules to ctx->staging (target index = base + local, or ids[local]).
+int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targets, uint64_t nt,
+             uint32_t tlen, const uint64_t* d_ids, uint64_t base, m6502_stats* st) {
+    const bool go = cfg.semantics == M6502_SEM_GO;
+    const uint32_t stages = cfg.stages ? cfg.stages : M6502_CHECK_ALL;
+    const uint32_t dead = cfg.dead_flags;
+    TRY(ensure(ctx, ctx->tfp, nt * 32 * sizeof(uint64_t)));
+    TRY(ensure(ctx, ctx->tmeta, nt));
+    uint64_t scap = std::max<uint64_t>(ctx->surv.bytes / sizeof(Surv), nt * 4 + 4096);
+    uint64_t icap = std::max<uint64_t>(ctx->items.bytes / sizeof(Item), 1u << 16);
+    uint64_t rcap = std::max<uint64_t>(ctx->rules.bytes / sizeof(m6502_rule), nt / 2 + 4096);
+    for (int attempt = 0; attempt < 6; attempt++) {
+        TRY(ensure(ctx, ctx->surv, scap * sizeof(Surv)));
+        TRY(ensure(ctx, ctx->fail, scap * sizeof(uint32_t)));
+        TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
+        TRY(ensure(ctx, ctx->rules, rcap * sizeof(m6502_rule)));
+        if (go) TRY(ensure(ctx, ctx->best, 2 * nt * sizeof(uint32_t)));
+        Counters* cnt = (Counters*)ctx->cnt.p;
+        CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), ctx->stream));
+        CK(cudaEventRecord(ctx->sev[0], ctx->stream));
+        k_fingerprint<FixedSeqs><<<ctx->fp_blocks, 256, 0, ctx->stream>>>(
+            FixedSeqs{d_targets, tlen}, nt, (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p);
+        CKL("k_fingerprint(targets)");
+        CK(cudaEventRecord(ctx->sev[1], ctx->stream));
+        uint32_t qgrid = (uint32_t)std::min<uint64_t>(ctx->qc_blocks, (nt + kQcTile - 1) / kQcTile);
+        if (go)
+            k_qc1<true><<<qgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
+                                                        (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
+                                                        (uint8_t*)ctx->cmeta1.p, dead, stages,
+                                                        (Surv*)ctx->surv.p, scap, cnt);
+        else
+            k_qc1<false><<<qgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
+                                                         (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
+                                                         (uint8_t*)ctx->cmeta1.p, dead, stages,
+                                                         (Surv*)ctx->surv.p, scap, cnt);
+        CKL("k_qc1");
+        CK(cudaEventRecord(ctx->sev[2], ctx->stream));
+        const bool exh = (stages & M6502_CHECK_EXH) != 0;
+        SurvSource src{(const Surv*)ctx->surv.p, d_targets, tlen, dead, go ? 1 : 0};
+        ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep, cfg.exh_mode == M6502_EXH_BRUTE};
+        if (exh) {
+            k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &cnt->surv, scap, ea);
+            CKL("k_exhaustive");
+        }
+        CK(cudaEventRecord(ctx->sev[3], ctx->stream));
+        if (exh) {
+            k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
+            CKL("k_exh_items");
+        }
+        CK(cudaEventRecord(ctx->sev[4], ctx->stream));
+        if (go) {
+            CK(cudaMemsetAsync(ctx->best.p, 0xFF, 2 * nt * sizeof(uint32_t), ctx->stream));
+            if (!exh) CK(cudaMemsetAsync(ctx->fail.p, 0, scap * sizeof(uint32_t), ctx->stream));
+            k_go_select<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
+                                                               (const uint32_t*)ctx->fail.p, (uint32_t)nt,
+                                                               (uint32_t*)ctx->best.p, cnt, d_targets, tlen, cfg.sweep);
+            CKL("k_go_select");
+            k_go_emit<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const uint32_t*)ctx->best.p, (uint32_t)nt,
+                                                             d_targets, tlen, d_ids,
+                                                             (m6502_rule*)ctx->rules.p, rcap, cnt);
+            CKL("k_go_emit");
+        } else {
+            k_emit_all<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
+                                                              (const uint32_t*)ctx->fail.p, d_ids, dead,
+                                                              (m6502_rule*)ctx->rules.p, rcap, cnt, exh ? 1 : 0,
+                                                              d_targets, tlen, cfg.sweep);
+            CKL("k_emit_all");
+        }
+        CK(cudaEventRecord(ctx->sev[5], ctx->stream));
+        Counters hc;
+        CK(cudaMemcpyAsync(&hc, cnt, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        bool redo = false;
+        if (hc.surv > scap) { scap = hc.surv + hc.surv / 4 + 1024; redo = true; }
+        if (hc.items > icap) { icap = hc.items + hc.items / 4 + 1024; redo = true; }
+        if (hc.rules > rcap) { rcap = hc.rules + hc.rules / 4 + 1024; redo = true; }
+        if (redo) continue;
+        size_t old = ctx->staging.size();
+        ctx->staging.resize(old + hc.rules);
+        if (hc.rules)
+            CK(cudaMemcpyAsync(ctx->staging.data() + old, ctx->rules.p, hc.rules * sizeof(m6502_rule),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (!d_ids)
+            for (size_t i = old; i < ctx->staging.size(); i++) ctx->staging[i].target += base;
+        if (st) {
+            st->targets += nt;
+            st->pairs += nt * (uint64_t)kNumInsns;
+            st->qc_hits += hc.qc;
+            st->mid_hits += hc.mid;
+            st->exh_checked += exh ? hc.surv : 0;
+            st->exh_passed += hc.exh_pass;
+            st->rules += hc.rules;
+            st->exh_states += hc.states;
+            st->exh_items += hc.items;
+            st->exh_algo_ops += hc.algo;
+            float ms[5];
+            for (int i = 0; i < 5; i++) cudaEventElapsedTime(&ms[i], ctx->sev[i], ctx->sev[i + 1]);
+            st->ms_fingerprint += ms[0];
+            st->ms_qc += ms[1];
+            st->ms_exhaustive += ms[2];
+            st->ms_exh_items += ms[3];
+            st->ms_emit += ms[4];
+            st->passes += 1;
+        }
+        return M6502_OK;
+    }
+    return set_err(ctx, M6502_E_NOMEM, "device buffers kept overflowing");
+}
+
+int check_cfg(m6502_ctx* ctx, const m6502_search_cfg* cfg) {
+    if (!cfg) return set_err(ctx, M6502_E_INVAL, "cfg is NULL");
+    if (cfg->semantics > M6502_SEM_GO) return set_err(ctx, M6502_E_INVAL, "bad semantics");
+    if (cfg->sweep > M6502_SWEEP_FULL) return set_err(ctx, M6502_E_INVAL, "bad sweep");
+    if (cfg->exh_mode > M6502_EXH_BRUTE) return set_err(ctx, M6502_E_INVAL, "bad exh_mode");
+    if (cfg->max_cand_len > 1) return set_err(ctx, M6502_E_INVAL, "max_cand_len > 1 is not supported by this build");
+    return M6502_OK;
+}
+
+int finish(m6502_ctx* ctx, m6502_rule* out, uint64_t cap, uint64_t* n_out) {
+    uint64_t n = ctx->staging.size();
+    if (n_out) *n_out = n;
+    if (out && cap) std::memcpy(out, ctx->staging.data(), std::min(n, cap) * sizeof(m6502_rule));
+    ctx->staging.clear();
+    if (n > cap) return set_err(ctx, M6502_E_OVERFLOW, "rule buffer too small");
+    return M6502_OK;
+}
+
+bool valid_seq(const uint16_t* s, uint64_t n) {
+    for (uint64_t i = 0; i < n; i++) if ((s[i] & 0xFF) >= NUM_OPS) return false;
+    return true;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* m6502_version(void) { return "m6502-b200 1.0 (sm_100a)"; }
+
+int m6502_create(m6502_ctx** out, const m6502_opts* opts) {
+    if (!out) return M6502_E_INVAL;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return M6502_E_NODEV;
+    m6502_ctx* ctx = new m6502_ctx();
+    if (opts) {
+        ctx->device = opts->device;
+        if (opts->targets_per_pass) ctx->pass_targets = opts->targets_per_pass;
+    }
+    if (ctx->device < 0 || ctx->device >= ndev) { delete ctx; return M6502_E_INVAL; }
+    if (cudaSetDevice(ctx->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess) {
+        delete ctx;
+        return M6502_E_CUDA;
+    }
+    bool ev_ok = true;
+    for (cudaEvent_t& e : ctx->sev) ev_ok = ev_ok && cudaEventCreate(&e) == cudaSuccess;
+    if (!ev_ok) {
+        delete ctx;
+        return M6502_E_CUDA;
+    }
+    cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, ctx->device);
+    int rc = init_ctx(ctx);
+    if (rc != M6502_OK) {
+        fprintf(stderr, "m6502_create: %s\n", ctx->err.c_str());
+        m6502_destroy(ctx);
+        return rc;
+    }
+    *out = ctx;
+    return M6502_OK;
+}
+
+void m6502_destroy(m6502_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    DevBuf* bufs[] = {&ctx->cfp1, &ctx->cmeta1, &ctx->targets, &ctx->ids, &ctx->tfp, &ctx->tmeta,
+                      &ctx->surv, &ctx->fail, &ctx->items, &ctx->rules, &ctx->cnt, &ctx->best,
+                      &ctx->pins, &ctx->poffs, &ctx->cins, &ctx->coffs, &ctx->pout, &ctx->pfd,
+                      &ctx->enum_count};
+    for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
+    for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* m6502_last_error(const m6502_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+void* m6502_stream(m6502_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int m6502_check_pairs(m6502_ctx* ctx, uint64_t n, const uint16_t* t_insns, const uint32_t* t_offs,
+                      const uint16_t* c_insns, const uint32_t* c_offs, uint8_t dead_flags,
+                      uint32_t checks, uint32_t sweep, uint32_t exh_mode, uint8_t* out,
+                      uint8_t* flagdiff) {
+    if (!ctx) return M6502_E_INVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (n == 0) return M6502_OK;
+    if (!t_insns || !t_offs || !c_insns || !c_offs || !out) return set_err(ctx, M6502_E_INVAL, "NULL buffer");
+    if (sweep > M6502_SWEEP_FULL || exh_mode > M6502_EXH_BRUTE) return set_err(ctx, M6502_E_INVAL, "bad sweep mode");
+    for (uint64_t i = 0; i < n; i++) {
+        uint32_t tl = t_offs[i + 1] - t_offs[i], cl = c_offs[i + 1] - c_offs[i];
+        if (t_offs[i + 1] < t_offs[i] || c_offs[i + 1] < c_offs[i] || tl < 1 || tl > kMaxSeq || cl < 1 || cl > kMaxSeq)
+            return set_err(ctx, M6502_E_INVAL, "sequence length must be 1..16");
+    }
+    if (!valid_seq(t_insns + t_offs[0], t_offs[n] - t_offs[0]) || !valid_seq(c_insns + c_offs[0], c_offs[n] - c_offs[0]))
+        return set_err(ctx, M6502_E_INVAL, "opcode out of range");
+    CK(cudaSetDevice(ctx->device));
+    const size_t tin = t_offs[n], cin = c_offs[n];
+    TRY(ensure(ctx, ctx->pins, tin * 2));
+    TRY(ensure(ctx, ctx->cins, cin * 2));
+    TRY(ensure(ctx, ctx->poffs, (n + 1) * 4));
+    TRY(ensure(ctx, ctx->coffs, (n + 1) * 4));
+    TRY(ensure(ctx, ctx->pout, n));
+    TRY(ensure(ctx, ctx->pfd, n));
+    TRY(ensure(ctx, ctx->fail, n * 4));
+    CK(cudaMemcpyAsync(ctx->pins.p, t_insns, tin * 2, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->cins.p, c_insns, cin * 2, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->poffs.p, t_offs, (n + 1) * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->coffs.p, c_offs, (n + 1) * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CsrSource src{(const uint16_t*)ctx->pins.p, (const uint32_t*)ctx->poffs.p, (const uint16_t*)ctx->cins.p,
+                  (const uint32_t*)ctx->coffs.p, dead_flags};
+    uint32_t grid = (uint32_t)std::min<uint64_t>((n + kWarpsPerBlock - 1) / kWarpsPerBlock, (uint64_t)ctx->sms * 16);
+    k_pair_vectors<<<grid, 256, 0, ctx->stream>>>(src, n, (uint8_t*)ctx->pout.p, (uint8_t*)ctx->pfd.p);
+    CKL("k_pair_vectors");
+    std::vector<uint8_t> fl;
+    if (checks & M6502_CHECK_EXH) {
+        Counters* cnt = (Counters*)ctx->cnt.p;
+        uint64_t icap = std::max<uint64_t>(ctx->items.bytes / sizeof(Item), 1u << 16);
+        for (int attempt = 0;; attempt++) {
+            TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
+            CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), ctx->stream));
+            unsigned long long hn = n;
+            CK(cudaMemcpyAsync(&cnt->surv, &hn, sizeof hn, cudaMemcpyHostToDevice, ctx->stream));
+            ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, sweep, exh_mode == M6502_EXH_BRUTE};
+            k_exhaustive<CsrSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &cnt->surv, n, ea);
+            CKL("k_exhaustive");
+            k_exh_items<CsrSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
+            CKL("k_exh_items");
+            Counters hc;
+            CK(cudaMemcpyAsync(&hc, cnt, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (hc.items <= icap) break;
+            if (attempt >= 4) return set_err(ctx, M6502_E_NOMEM, "work-item queue kept overflowing");
+            icap = hc.items + hc.items / 4 + 1024;
+        }
+        fl.resize(n * 4);
+        CK(cudaMemcpyAsync(fl.data(), ctx->fail.p, n * 4, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    CK(cudaMemcpyAsync(out, ctx->pout.p, n, cudaMemcpyDeviceToHost, ctx->stream));
+    if (flagdiff) CK(cudaMemcpyAsync(flagdiff, ctx->pfd.p, n, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const uint32_t* f32 = (const uint32_t*)fl.data();
+    for (uint64_t i = 0; i < n; i++) {
+        uint8_t r = out[i] & (uint8_t)(checks & 3u);
+        if ((checks & M6502_CHECK_EXH) && f32[i] == 0) r |= 4;
+        out[i] = r;
+    }
+    return M6502_OK;
+}
+
+int m6502_fingerprint(m6502_ctx* ctx, uint64_t n, const uint16_t* insns, const uint32_t* offs, uint8_t* out) {
+    if (!ctx) return M6502_E_INVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (n == 0) return M6502_OK;
+    if (!insns || !offs || !out) return set_err(ctx, M6502_E_INVAL, "NULL buffer");
+    for (uint64_t i = 0; i < n; i++) {
+        uint32_t l = offs[i + 1] - offs[i];
+        if (offs[i + 1] < offs[i] || l > kMaxSeq) return set_err(ctx, M6502_E_INVAL, "sequence length must be 0..16");
+    }
+    if (!valid_seq(insns + offs[0], offs[n] - offs[0])) return set_err(ctx, M6502_E_INVAL, "opcode out of range");
+    CK(cudaSetDevice(ctx->device));
+    TRY(ensure(ctx, ctx->pins, (size_t)offs[n] * 2 + 2));
+    TRY(ensure(ctx, ctx->poffs, (n + 1) * 4));
+    TRY(ensure(ctx, ctx->tfp, n * 32 * 8));
+    CK(cudaMemcpyAsync(ctx->pins.p, insns, (size_t)offs[n] * 2, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->poffs.p, offs, (n + 1) * 4, cudaMemcpyHostToDevice, ctx->stream));
+    k_fingerprint<CsrSeqs><<<ctx->fp_blocks, 256, 0, ctx->stream>>>(
+        CsrSeqs{(const uint16_t*)ctx->pins.p, (const uint32_t*)ctx->poffs.p}, n, (uint64_t*)ctx->tfp.p, nullptr);
+    CKL("k_fingerprint");
+    std::vector<uint64_t> h(n * 32);
+    CK(cudaMemcpyAsync(h.data(), ctx->tfp.p, n * 32 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    for (uint64_t i = 0; i < n; i++)
+        for (int v = 0; v < 8; v++)
+            for (int b = 0; b < 8; b++) out[i * 64 + v * 8 + b] = (uint8_t)(h[i * 32 + v] >> (8 * b));
+    return M6502_OK;
+}
+
+int m6502_exec_batch(m6502_ctx* ctx, uint64_t n, const uint16_t* insns, const uint32_t* offs,
+                     const uint64_t* states_in, uint64_t* states_out) {
+    if (!ctx) return M6502_E_INVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (n == 0) return M6502_OK;
+    if (!insns || !offs || !states_in || !states_out) return set_err(ctx, M6502_E_INVAL, "NULL buffer");
+    for (uint64_t i = 0; i < n; i++)
+        if (offs[i + 1] < offs[i]) return set_err(ctx, M6502_E_INVAL, "offsets must not decrease");
+    if (!valid_seq(insns + offs[0], offs[n] - offs[0])) return set_err(ctx, M6502_E_INVAL, "opcode out of range");
+    CK(cudaSetDevice(ctx->device));
+    TRY(ensure(ctx, ctx->pins, (size_t)offs[n] * 2 + 2));
+    TRY(ensure(ctx, ctx->poffs, (n + 1) * 4));
+    TRY(ensure(ctx, ctx->tfp, n * 16));
+    uint64_t* d_in = (uint64_t*)ctx->tfp.p;
+    uint64_t* d_out = d_in + n;
+    CK(cudaMemcpyAsync(ctx->pins.p, insns, (size_t)offs[n] * 2, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->poffs.p, offs, (n + 1) * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(d_in, states_in, n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    uint32_t grid = (uint32_t)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sms * 16);
+    k_exec_batch<<<grid, 256, 0, ctx->stream>>>(CsrSeqs{(const uint16_t*)ctx->pins.p, (const uint32_t*)ctx->poffs.p},
+                                                n, d_in, d_out);
+    CKL("k_exec_batch");
+    CK(cudaMemcpyAsync(states_out, d_out, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return M6502_OK;
+}
+
+int m6502_search(m6502_ctx* ctx, const m6502_search_cfg* cfg, const uint16_t* targets, uint64_t n,
+                 uint32_t tlen, m6502_rule* out, uint64_t cap, uint64_t* n_out, m6502_stats* stats) {
+    if (!ctx) return M6502_E_INVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    TRY(check_cfg(ctx, cfg));
+    if (tlen < 1 || tlen > 3) return set_err(ctx, M6502_E_INVAL, "target length must be 1..3");
+    if (n > 0xFFFFFFFFull) return set_err(ctx, M6502_E_INVAL, "too many targets for one call");
+    if (n && !targets) return set_err(ctx, M6502_E_INVAL, "NULL targets");
+    const bool on_dev = (cfg->flags & M6502_TARGETS_ON_DEVICE) != 0;
+    if (!on_dev && !valid_seq(targets, n * tlen)) return set_err(ctx, M6502_E_INVAL, "opcode out of range");
+    CK(cudaSetDevice(ctx->device));
+    m6502_stats st;
+    std::memset(&st, 0, sizeof st);
+    ctx->staging.clear();
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    for (uint64_t b = 0; b < n; b += ctx->pass_targets) {
+        uint64_t nt = std::min<uint64_t>(ctx->pass_targets, n - b);
+        const uint16_t* d_t;
+        if (on_dev) {
+            d_t = targets + b * tlen;
+        } else {
+            TRY(ensure(ctx, ctx->targets, nt * tlen * 2));
+            CK(cudaMemcpyAsync(ctx->targets.p, targets + b * tlen, nt * tlen * 2, cudaMemcpyHostToDevice, ctx->stream));
+            d_t = (const uint16_t*)ctx->targets.p;
+        }
+        TRY(run_pass(ctx, *cfg, d_t, nt, tlen, nullptr, b, &st));
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    st.ms_device = ms;
+    if (stats) *stats = st;
+    return finish(ctx, out, cap, n_out);
+}
+
+int m6502_enumerate(m6502_ctx* ctx, const m6502_search_cfg* cfg, uint32_t tlen, uint32_t first,
+                    uint32_t last, m6502_rule* out, uint64_t cap, uint64_t* n_out, m6502_stats* stats) {
+    if (!ctx) return M6502_E_INVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    TRY(check_cfg(ctx, cfg));
+    if (tlen < 2 || tlen > 3) return set_err(ctx, M6502_E_INVAL, "enumeration length must be 2 or 3");
+    if (last > (uint32_t)kNumInsns) last = kNumInsns;
+    if (first > last) return set_err(ctx, M6502_E_INVAL, "first > last");
+    CK(cudaSetDevice(ctx->device));
+    m6502_stats st;
+    std::memset(&st, 0, sizeof st);
+    ctx->staging.clear();
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    const uint64_t per_first = tlen == 2 ? (uint64_t)kNumInsns : (uint64_t)kNumInsns * kNumInsns;
+    // first-op slices sized so one slice holds at most ~pass_targets ids
+    const uint64_t ops_per_slice = std::max<uint64_t>(1, ctx->pass_targets / per_first);
+    TRY(ensure(ctx, ctx->enum_count, sizeof(unsigned long long)));
+    for (uint64_t f = first; f < last; f += ops_per_slice) {
+        uint64_t f1 = std::min<uint64_t>(last, f + ops_per_slice);
+        uint64_t id0 = f * per_first, id1 = f1 * per_first, span = id1 - id0;
+        TRY(ensure(ctx, ctx->targets, span * tlen * 2));
+        TRY(ensure(ctx, ctx->ids, span * 8));
+        CK(cudaMemsetAsync(ctx->enum_count.p, 0, sizeof(unsigned long long), ctx->stream));
+        uint32_t grid = (uint32_t)std::min<uint64_t>((span + 255) / 256, (uint64_t)ctx->sms * 16);
+        k_enum_targets<<<grid, 256, 0, ctx->stream>>>(id0, id1, tlen, (uint16_t*)ctx->targets.p,
+                                                       (uint64_t*)ctx->ids.p, span,
+                                                       (unsigned long long*)ctx->enum_count.p);
+        CKL("k_enum_targets");
+        unsigned long long nt = 0;
+        CK(cudaMemcpyAsync(&nt, ctx->enum_count.p, sizeof nt, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        for (uint64_t b = 0; b < nt; b += ctx->pass_targets) {
+            uint64_t m = std::min<uint64_t>(ctx->pass_targets, nt - b);
+            TRY(run_pass(ctx, *cfg, (const uint16_t*)ctx->targets.p + b * tlen, m, tlen,
+                         (const uint64_t*)ctx->ids.p + b, 0, &st));
+        }
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+    st.ms_device = ms;
+    if (stats) *stats = st;
+    return finish(ctx, out, cap, n_out);
+}
+
+}  // extern "C"

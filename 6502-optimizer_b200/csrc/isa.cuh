@@ -1,0 +1,380 @@
+// isa.cuh -- MOS 6502 instruction semantics for the B200 engine.
+//
+// The machine state is A, X, Y, P, S, M, S0, S1 (pkg/cpu/state.go:11-16).
+// Kernels keep it in eight 32-bit registers (one byte value each) and pack
+// it into one 64-bit word, byte i = field i, for comparisons and storage.
+// Every kernel arranges its work so that the instruction being executed is
+// the same across a warp (a warp sweeps one pair, or one lane per test
+// vector runs the same sequence), so the opcode switch below is a uniform
+// indirect branch with no divergence.
+#pragma once
+#include <cstdint>
+
+#if defined(__CUDACC__)
+#define M6502_HD __host__ __device__ __forceinline__
+#else
+#define M6502_HD inline
+#endif
+
+namespace m6502 {
+
+// Opcode numbering of pkg/inst/instruction.go:42-121.
+enum Op : uint32_t {
+    TAX, TAY, TXA, TYA, TSX, TXS, INX, INY, DEX, DEY,
+    ASL_A, LSR_A, ROL_A, ROR_A,
+    CLC, SEC, CLD, SED, CLI, SEI, CLV,
+    PHA, PLA, PHP, PLP, NOP,
+    LDA_IMM, LDX_IMM, LDY_IMM, ADC_IMM, SBC_IMM, AND_IMM, ORA_IMM, EOR_IMM,
+    CMP_IMM, CPX_IMM, CPY_IMM,
+    LDA_M, LDX_M, LDY_M, STA_M, STX_M, STY_M, ADC_M, SBC_M, AND_M, ORA_M, EOR_M,
+    CMP_M, CPX_M, CPY_M, INC_M, DEC_M, ASL_M, LSR_M, ROL_M, ROR_M, BIT_M,
+    NUM_OPS
+};
+
+constexpr int kNumInsns = 2863;      // 47 implied/M ops + 11 immediates x 256
+constexpr uint32_t kFlagC = 0x01, kFlagZ = 0x02, kFlagI = 0x04, kFlagD = 0x08;
+constexpr uint32_t kFlagB = 0x10, kFlagU = 0x20, kFlagV = 0x40, kFlagN = 0x80;
+constexpr uint32_t kPMask = 0xCF;    // pkg/cpu/state.go:20
+
+struct St {
+    uint32_t a, x, y, p, s, m, s0, s1;
+};
+
+M6502_HD bool has_imm(uint32_t op) { return op >= LDA_IMM && op <= CPY_IMM; }
+M6502_HD uint32_t nzf(uint32_t v) { return (v & 0x80u) | (v == 0u ? kFlagZ : 0u); }
+M6502_HD void set_nz(St& s, uint32_t v) { s.p = (s.p & 0x7Du) | nzf(v); }
+
+M6502_HD void op_adc(St& s, uint32_t m) {
+    uint32_t sum = s.a + m + (s.p & 1u);
+    uint32_t r = sum & 0xFFu;
+    uint32_t v = (s.a ^ r) & (m ^ r) & 0x80u;
+    s.p = (s.p & 0x3Cu) | nzf(r) | (sum >> 8) | (v >> 1);
+    s.a = r;
+}
+
+// a - m - (1 - c) computed as a + ~m + c; the carry out is "no borrow".
+M6502_HD void op_sbc(St& s, uint32_t m) {
+    uint32_t sum = s.a + (m ^ 0xFFu) + (s.p & 1u);
+    uint32_t r = sum & 0xFFu;
+    uint32_t v = (s.a ^ r) & (s.a ^ m) & 0x80u;
+    s.p = (s.p & 0x3Cu) | nzf(r) | (sum >> 8) | (v >> 1);
+    s.a = r;
+}
+
+M6502_HD void op_cmp(St& s, uint32_t reg, uint32_t m) {
+    s.p = (s.p & 0x7Cu) | nzf((reg - m) & 0xFFu) | (reg >= m ? 1u : 0u);
+}
+
+M6502_HD uint32_t op_asl(St& s, uint32_t v) {
+    uint32_t r = (v << 1) & 0xFFu;
+    s.p = (s.p & 0x7Cu) | nzf(r) | (v >> 7);
+    return r;
+}
+M6502_HD uint32_t op_lsr(St& s, uint32_t v) {
+    uint32_t r = v >> 1;
+    s.p = (s.p & 0x7Cu) | nzf(r) | (v & 1u);
+    return r;
+}
+M6502_HD uint32_t op_rol(St& s, uint32_t v) {
+    uint32_t r = ((v << 1) | (s.p & 1u)) & 0xFFu;
+    s.p = (s.p & 0x7Cu) | nzf(r) | (v >> 7);
+    return r;
+}
+M6502_HD uint32_t op_ror(St& s, uint32_t v) {
+    uint32_t r = (v >> 1) | ((s.p & 1u) << 7);
+    s.p = (s.p & 0x7Cu) | nzf(r) | (v & 1u);
+    return r;
+}
+M6502_HD void push(St& s, uint32_t v) { s.s1 = s.s0; s.s0 = v; s.s = (s.s - 1u) & 0xFFu; }
+M6502_HD uint32_t pull(St& s) {
+    uint32_t v = s.s0;
+    s.s0 = s.s1; s.s1 = 0; s.s = (s.s + 1u) & 0xFFu;
+    return v;
+}
+
+// One instruction; insn = op | imm << 8.  Semantics of pkg/cpu/exec.go:8-189
+// (binary-mode ADC/SBC, PHP pushes B and U, pulls zero S1).  An opcode
+// outside [0, 58) leaves the state unchanged; callers validate inputs.
+M6502_HD void exec(St& s, uint32_t insn) {
+    const uint32_t imm = insn >> 8;
+    switch (insn & 0xFFu) {
+    case TAX: s.x = s.a; set_nz(s, s.x); break;
+    case TAY: s.y = s.a; set_nz(s, s.y); break;
+    case TXA: s.a = s.x; set_nz(s, s.a); break;
+    case TYA: s.a = s.y; set_nz(s, s.a); break;
+    case TSX: s.x = s.s; set_nz(s, s.x); break;
+    case TXS: s.s = s.x; break;
+    case INX: s.x = (s.x + 1u) & 0xFFu; set_nz(s, s.x); break;
+    case INY: s.y = (s.y + 1u) & 0xFFu; set_nz(s, s.y); break;
+    case DEX: s.x = (s.x - 1u) & 0xFFu; set_nz(s, s.x); break;
+    case DEY: s.y = (s.y - 1u) & 0xFFu; set_nz(s, s.y); break;
+    case ASL_A: s.a = op_asl(s, s.a); break;
+    case LSR_A: s.a = op_lsr(s, s.a); break;
+    case ROL_A: s.a = op_rol(s, s.a); break;
+    case ROR_A: s.a = op_ror(s, s.a); break;
+    case CLC: s.p &= ~kFlagC; break;
+    case SEC: s.p |= kFlagC; break;
+    case CLD: s.p &= ~kFlagD; break;
+    case SED: s.p |= kFlagD; break;
+    case CLI: s.p &= ~kFlagI; break;
+    case SEI: s.p |= kFlagI; break;
+    case CLV: s.p &= ~kFlagV; break;
+    case PHA: push(s, s.a); break;
+    case PLA: s.a = pull(s); set_nz(s, s.a); break;
+    case PHP: push(s, s.p | kFlagB | kFlagU); break;
+    case PLP: s.p = pull(s); break;
+    case NOP: break;
+    case LDA_IMM: s.a = imm; set_nz(s, imm); break;
+    case LDX_IMM: s.x = imm; set_nz(s, imm); break;
+    case LDY_IMM: s.y = imm; set_nz(s, imm); break;
+    case ADC_IMM: op_adc(s, imm); break;
+    case SBC_IMM: op_sbc(s, imm); break;
+    case AND_IMM: s.a &= imm; set_nz(s, s.a); break;
+    case ORA_IMM: s.a |= imm; set_nz(s, s.a); break;
+    case EOR_IMM: s.a ^= imm; set_nz(s, s.a); break;
+    case CMP_IMM: op_cmp(s, s.a, imm); break;
+    case CPX_IMM: op_cmp(s, s.x, imm); break;
+    case CPY_IMM: op_cmp(s, s.y, imm); break;
+    case LDA_M: s.a = s.m; set_nz(s, s.a); break;
+    case LDX_M: s.x = s.m; set_nz(s, s.x); break;
+    case LDY_M: s.y = s.m; set_nz(s, s.y); break;
+    case STA_M: s.m = s.a; break;
+    case STX_M: s.m = s.x; break;
+    case STY_M: s.m = s.y; break;
+    case ADC_M: op_adc(s, s.m); break;
+    case SBC_M: op_sbc(s, s.m); break;
+    case AND_M: s.a &= s.m; set_nz(s, s.a); break;
+    case ORA_M: s.a |= s.m; set_nz(s, s.a); break;
+    case EOR_M: s.a ^= s.m; set_nz(s, s.a); break;
+    case CMP_M: op_cmp(s, s.a, s.m); break;
+    case CPX_M: op_cmp(s, s.x, s.m); break;
+    case CPY_M: op_cmp(s, s.y, s.m); break;
+    case INC_M: s.m = (s.m + 1u) & 0xFFu; set_nz(s, s.m); break;
+    case DEC_M: s.m = (s.m - 1u) & 0xFFu; set_nz(s, s.m); break;
+    case ASL_M: s.m = op_asl(s, s.m); break;
+    case LSR_M: s.m = op_lsr(s, s.m); break;
+    case ROL_M: s.m = op_rol(s, s.m); break;
+    case ROR_M: s.m = op_ror(s, s.m); break;
+    case BIT_M: s.p = (s.p & 0x3Du) | (s.m & 0xC0u) | ((s.a & s.m) == 0u ? kFlagZ : 0u); break;
+    default: break;
+    }
+}
+
+M6502_HD uint64_t pack(const St& s) {
+    return (uint64_t)(s.a | (s.x << 8) | (s.y << 16) | (s.p << 24)) |
+           ((uint64_t)(s.s | (s.m << 8) | (s.s0 << 16) | (s.s1 << 24)) << 32);
+}
+M6502_HD St unpack(uint64_t w) {
+    St s;
+    uint32_t lo = (uint32_t)w, hi = (uint32_t)(w >> 32);
+    s.a = lo & 0xFFu; s.x = (lo >> 8) & 0xFFu; s.y = (lo >> 16) & 0xFFu; s.p = lo >> 24;
+    s.s = hi & 0xFFu; s.m = (hi >> 8) & 0xFFu; s.s0 = (hi >> 16) & 0xFFu; s.s1 = hi >> 24;
+    return s;
+}
+
+// Comparison mask over a packed state: every byte, and in P the bits of
+// PMask that are not dead (statesEqualMasked, pkg/search/verifier.go:418-424).
+M6502_HD uint64_t cmp_mask(uint32_t dead) {
+    return 0xFFFFFFFF00FFFFFFull | ((uint64_t)(kPMask & ~dead & 0xFFu) << 24);
+}
+
+// ---- Static tables (host and device copies built from these functions) ----
+
+// Register bits of the reference's read/write masks (verifier.go:134-143).
+enum : uint32_t {
+    R_A = 1, R_P = 2, R_X = 4, R_Y = 8, R_S = 16, R_M = 32, R_S0 = 64, R_S1 = 128
+};
+
+// opReads, pkg/search/verifier.go:154-259.  These masks define which
+// extra registers the exhaustive sweep varies; they are the reference's
+// sweep-domain rule, not a complete dataflow model (see op_deps below).
+M6502_HD uint32_t op_reads(uint32_t op) {
+    switch (op) {
+    case TAX: case TAY: case ASL_A: case LSR_A: case AND_IMM: case ORA_IMM: case EOR_IMM:
+    case CMP_IMM: case STA_M: return R_A;
+    case TXA: case TXS: case INX: case DEX: case CPX_IMM: case STX_M: return R_X;
+    case TYA: case INY: case DEY: case CPY_IMM: case STY_M: return R_Y;
+    case TSX: return R_S;
+    case ROL_A: case ROR_A: case ADC_IMM: case SBC_IMM: return R_A | R_P;
+    case PHA: return R_A | R_S0 | R_S1;
+    case PHP: return R_P | R_S0 | R_S1;
+    case PLA: case PLP: return R_S0;
+    case LDA_M: case LDX_M: case LDY_M: case INC_M: case DEC_M: case ASL_M: case LSR_M:
+        return R_M;
+    case ADC_M: case SBC_M: return R_A | R_M | R_P;
+    case AND_M: case ORA_M: case EOR_M: case CMP_M: case BIT_M: return R_A | R_M;
+    case CPX_M: return R_X | R_M;
+    case CPY_M: return R_Y | R_M;
+    case ROL_M: case ROR_M: return R_M | R_P;
+    default: return 0;
+    }
+}
+
+// opWrites, pkg/search/pruner.go:76-163 (pruning only).
+M6502_HD uint32_t op_writes(uint32_t op) {
+    switch (op) {
+    case TAX: case TSX: case INX: case DEX: case LDX_IMM: case LDX_M: return R_X | R_P;
+    case TAY: case INY: case DEY: case LDY_IMM: case LDY_M: return R_Y | R_P;
+    case TXA: case TYA: case ASL_A: case LSR_A: case ROL_A: case ROR_A: case LDA_IMM:
+    case ADC_IMM: case SBC_IMM: case AND_IMM: case ORA_IMM: case EOR_IMM: case LDA_M:
+    case ADC_M: case SBC_M: case AND_M: case ORA_M: case EOR_M: return R_A | R_P;
+    case TXS: return R_S;
+    case CLC: case SEC: case CLD: case SED: case CLI: case SEI: case CLV: case CMP_IMM:
+    case CPX_IMM: case CPY_IMM: case CMP_M: case CPX_M: case CPY_M: case BIT_M: return R_P;
+    case PHA: case PHP: return R_S | R_S0 | R_S1;
+    case PLA: return R_A | R_P | R_S | R_S0;
+    case PLP: return R_P | R_S | R_S0;
+    case STA_M: case STX_M: case STY_M: return R_M;
+    case INC_M: case DEC_M: case ASL_M: case LSR_M: case ROL_M: case ROR_M: return R_M | R_P;
+    default: return 0;
+    }
+}
+
+// CUDA-pipeline byte size (cuda/6502_search_v2.cu:437-440) and the Go
+// catalog's (pkg/inst/catalog.go:50-56: zero-page ops have 1-byte encodings).
+M6502_HD uint32_t bytes_cuda(uint32_t op) { return op <= NOP ? 1u : 2u; }
+M6502_HD uint32_t bytes_go(uint32_t op) { return has_imm(op) ? 2u : 1u; }
+M6502_HD uint32_t cycles(uint32_t op) {
+    if (op == PHA || op == PHP) return 3;
+    if (op == PLA || op == PLP) return 4;
+    if (op >= INC_M && op <= ROR_M) return 5;
+    if (op >= LDA_M) return 3;
+    return 2;
+}
+
+// Pruner, pkg/search/pruner.go:6-181.
+M6502_HD bool should_prune(const uint16_t* seq, int n) {
+    for (int i = 0; i < n; i++) {
+        uint32_t op = seq[i] & 0xFFu;
+        if (op == NOP) return true;
+        if (i + 1 < n) {
+            uint32_t w1 = op_writes(op), nxt = seq[i + 1] & 0xFFu;
+            if (w1 & op_writes(nxt) & ~(R_P | R_S | R_S0 | R_S1) & ~op_reads(nxt)) return true;
+        }
+    }
+    int depth = 0;
+    for (int i = 0; i < n; i++) {
+        uint32_t op = seq[i] & 0xFFu;
+        if (op == PHA || op == PHP) { if (++depth > 2) return true; }
+        else if (op == PLA || op == PLP) { if (depth <= 0) return true; depth--; }
+    }
+    for (int i = 0; i + 1 < n; i++) {
+        uint32_t a = seq[i] & 0xFFu, b = seq[i + 1] & 0xFFu;
+        bool indep = !((op_writes(a) & op_reads(b)) || (op_reads(a) & op_writes(b)) ||
+                       (op_writes(a) & op_writes(b)));
+        uint32_t ka = (a << 16) | (seq[i] >> 8), kb = (b << 16) | (seq[i + 1] >> 8);
+        if (indep && ka > kb) return true;
+    }
+    return false;
+}
+
+// ---- Dataflow model for the exact cone decomposition of the sweep ----
+//
+// Thirteen locations: the seven byte registers and the six flags that the
+// comparison sees (P bits 4 and 5 are masked by PMask and never reach any
+// other location: PHP forces them to 1 in the pushed byte).
+enum Loc : uint32_t {
+    L_A, L_X, L_Y, L_S, L_M, L_S0, L_S1, L_C, L_Z, L_I, L_D, L_V, L_N, NUM_LOCS
+};
+constexpr uint32_t LB(uint32_t l) { return 1u << l; }
+constexpr uint32_t kFlagLocs = (1u << L_C) | (1u << L_Z) | (1u << L_I) | (1u << L_D) |
+                               (1u << L_V) | (1u << L_N);
+
+// Per opcode: which locations it writes, and for each written location the
+// set of input locations its new value can depend on (a superset is sound;
+// a missing input would not be).  Unwritten locations keep their value.
+// Returns the written-location mask; dep[l] is filled for every l.
+M6502_HD uint32_t op_deps(uint32_t op, uint16_t dep[NUM_LOCS]) {
+    for (uint32_t l = 0; l < NUM_LOCS; l++) dep[l] = (uint16_t)LB(l);
+    uint32_t w = 0;
+    auto set = [&](uint32_t l, uint32_t d) { dep[l] = (uint16_t)d; w |= LB(l); };
+    auto nz = [&](uint32_t d) { set(L_Z, d); set(L_N, d); };
+    const uint32_t A = LB(L_A), X = LB(L_X), Y = LB(L_Y), S = LB(L_S), M = LB(L_M),
+                   S0 = LB(L_S0), S1 = LB(L_S1), C = LB(L_C);
+    switch (op) {
+    case TAX: set(L_X, A); nz(A); break;
+    case TAY: set(L_Y, A); nz(A); break;
+    case TXA: set(L_A, X); nz(X); break;
+    case TYA: set(L_A, Y); nz(Y); break;
+    case TSX: set(L_X, S); nz(S); break;
+    case TXS: set(L_S, X); break;
+    case INX: case DEX: set(L_X, X); nz(X); break;
+    case INY: case DEY: set(L_Y, Y); nz(Y); break;
+    case ASL_A: case LSR_A: set(L_A, A); set(L_C, A); nz(A); break;
+    case ROL_A: case ROR_A: set(L_A, A | C); set(L_C, A); nz(A | C); break;
+    case CLC: case SEC: set(L_C, 0); break;
+    case CLD: case SED: set(L_D, 0); break;
+    case CLI: case SEI: set(L_I, 0); break;
+    case CLV: set(L_V, 0); break;
+    case PHA: set(L_S1, S0); set(L_S0, A); set(L_S, S); break;
+    case PHP: set(L_S1, S0); set(L_S0, kFlagLocs); set(L_S, S); break;
+    case PLA: set(L_A, S0); nz(S0); set(L_S0, S1); set(L_S1, 0); set(L_S, S); break;
+    case PLP:
+        for (uint32_t l = L_C; l <= L_N; l++) set(l, S0);
+        set(L_S0, S1); set(L_S1, 0); set(L_S, S);
+        break;
+    case NOP: break;
+    case LDA_IMM: set(L_A, 0); nz(0); break;
+    case LDX_IMM: set(L_X, 0); nz(0); break;
+    case LDY_IMM: set(L_Y, 0); nz(0); break;
+    case ADC_IMM: case SBC_IMM:
+        set(L_A, A | C); set(L_C, A | C); set(L_V, A | C); nz(A | C); break;
+    case AND_IMM: case ORA_IMM: case EOR_IMM: set(L_A, A); nz(A); break;
+    case CMP_IMM: set(L_C, A); nz(A); break;
+    case CPX_IMM: set(L_C, X); nz(X); break;
+    case CPY_IMM: set(L_C, Y); nz(Y); break;
+    case LDA_M: set(L_A, M); nz(M); break;
+    case LDX_M: set(L_X, M); nz(M); break;
+    case LDY_M: set(L_Y, M); nz(M); break;
+    case STA_M: set(L_M, A); break;
+    case STX_M: set(L_M, X); break;
+    case STY_M: set(L_M, Y); break;
+    case ADC_M: case SBC_M:
+        set(L_A, A | M | C); set(L_C, A | M | C); set(L_V, A | M | C); nz(A | M | C); break;
+    case AND_M: case ORA_M: case EOR_M: set(L_A, A | M); nz(A | M); break;
+    case CMP_M: set(L_C, A | M); nz(A | M); break;
+    case CPX_M: set(L_C, X | M); nz(X | M); break;
+    case CPY_M: set(L_C, Y | M); nz(Y | M); break;
+    case INC_M: case DEC_M: set(L_M, M); nz(M); break;
+    case ASL_M: case LSR_M: set(L_M, M); set(L_C, M); nz(M); break;
+    case ROL_M: case ROR_M: set(L_M, M | C); set(L_C, M); nz(M | C); break;
+    case BIT_M: set(L_N, M); set(L_V, M); set(L_Z, A | M); break;
+    default: break;
+    }
+    return w;
+}
+
+// Byte/bit of the packed 64-bit state holding each location.
+M6502_HD uint64_t loc_mask64(uint32_t l) {
+    switch (l) {
+    case L_A: return 0xFFull;
+    case L_X: return 0xFFull << 8;
+    case L_Y: return 0xFFull << 16;
+    case L_S: return 0xFFull << 32;
+    case L_M: return 0xFFull << 40;
+    case L_S0: return 0xFFull << 48;
+    case L_S1: return 0xFFull << 56;
+    case L_C: return (uint64_t)kFlagC << 24;
+    case L_Z: return (uint64_t)kFlagZ << 24;
+    case L_I: return (uint64_t)kFlagI << 24;
+    case L_D: return (uint64_t)kFlagD << 24;
+    case L_V: return (uint64_t)kFlagV << 24;
+    case L_N: return (uint64_t)kFlagN << 24;
+    default: return 0;
+    }
+}
+
+// P bit of each flag location (for dead-flag masking).
+M6502_HD uint32_t flag_bit(uint32_t l) {
+    switch (l) {
+    case L_C: return kFlagC;
+    case L_Z: return kFlagZ;
+    case L_I: return kFlagI;
+    case L_D: return kFlagD;
+    case L_V: return kFlagV;
+    case L_N: return kFlagN;
+    default: return 0;
+    }
+}
+
+}  // namespace m6502

@@ -1,0 +1,131 @@
+"""ctypes binding of libm6502gpu.so (include/m6502.h).
+
+The library is built in-tree (``make -C 6502-optimizer_b200``) and loaded
+from ``6502-optimizer_b200/lib``.  There is no fallback: if the library is
+missing or a call needs a GPU that is not there, the call raises.
+"""
+import ctypes
+import os
+import threading
+
+import numpy as np
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libm6502gpu.so")
+
+M6502_OK = 0
+M6502_E_INVAL = -1
+M6502_E_CUDA = -2
+M6502_E_NOMEM = -3
+M6502_E_OVERFLOW = -4
+M6502_E_NODEV = -5
+
+SEM_CUDA, SEM_GO = 0, 1
+SWEEP_REFERENCE, SWEEP_FULL = 0, 1
+EXH_CONES, EXH_BRUTE = 0, 1
+CHECK_QC, CHECK_MID, CHECK_EXH, CHECK_ALL = 1, 2, 4, 7
+TARGETS_ON_DEVICE = 1
+
+
+class M6502Error(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"m6502 error {code}: {msg}")
+        self.code = code
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("flags", ctypes.c_uint32),
+                ("targets_per_pass", ctypes.c_uint64)]
+
+
+class Rule(ctypes.Structure):
+    _fields_ = [("target", ctypes.c_uint64), ("cand", ctypes.c_uint16 * 3),
+                ("cand_len", ctypes.c_uint8), ("dead_flags", ctypes.c_uint8)]
+
+
+RULE_DTYPE = np.dtype([("target", "<u8"), ("cand", "<u2", (3,)), ("cand_len", "u1"),
+                       ("dead_flags", "u1")])
+assert RULE_DTYPE.itemsize == ctypes.sizeof(Rule) == 16
+
+
+class SearchCfg(ctypes.Structure):
+    _fields_ = [("semantics", ctypes.c_uint32), ("sweep", ctypes.c_uint32),
+                ("exh_mode", ctypes.c_uint32), ("stages", ctypes.c_uint32),
+                ("max_cand_len", ctypes.c_uint32), ("flags", ctypes.c_uint32),
+                ("dead_flags", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 7)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in
+                ("targets", "pairs", "qc_hits", "mid_hits", "exh_checked", "exh_passed",
+                 "rules", "exh_states", "exh_items", "exh_algo_ops", "passes")] + \
+               [(n, ctypes.c_double) for n in ("ms_device", "ms_fingerprint", "ms_qc", "ms_exhaustive",
+                                               "ms_exh_items", "ms_emit")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+_lib = None
+_lock = threading.Lock()
+
+# Exported symbols (kept in step with include/m6502.h; the host tests check both).
+SYMBOLS = (
+    "m6502_version", "m6502_create", "m6502_destroy", "m6502_last_error", "m6502_stream",
+    "m6502_check_pairs", "m6502_fingerprint", "m6502_exec_batch", "m6502_search", "m6502_enumerate",
+    "m6502_insn_table", "m6502_enumerate_targets", "m6502_disasm", "m6502_parse", "m6502_should_prune",
+    "m6502_seq_bytes", "m6502_seq_cycles", "m6502_op_deps", "m6502_format_jsonl",
+)
+
+
+def lib():
+    """Loads libm6502gpu.so once; raises if it has not been built."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise M6502Error(M6502_E_NODEV, f"{LIB_PATH} is missing: run `make -C 6502-optimizer_b200`")
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.POINTER
+        u8p, u16p, u32p, u64p = P(ctypes.c_uint8), P(ctypes.c_uint16), P(ctypes.c_uint32), P(ctypes.c_uint64)
+        vp = ctypes.c_void_p
+        L.m6502_version.restype = ctypes.c_char_p
+        L.m6502_create.argtypes = [P(vp), P(Opts)]
+        L.m6502_destroy.argtypes = [vp]
+        L.m6502_destroy.restype = None
+        L.m6502_last_error.argtypes = [vp]
+        L.m6502_last_error.restype = ctypes.c_char_p
+        L.m6502_stream.argtypes = [vp]
+        L.m6502_stream.restype = vp
+        L.m6502_check_pairs.argtypes = [vp, ctypes.c_uint64, u16p, u32p, u16p, u32p, ctypes.c_uint8,
+                                        ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, u8p, u8p]
+        L.m6502_fingerprint.argtypes = [vp, ctypes.c_uint64, u16p, u32p, u8p]
+        L.m6502_exec_batch.argtypes = [vp, ctypes.c_uint64, u16p, u32p, u64p, u64p]
+        L.m6502_search.argtypes = [vp, P(SearchCfg), vp, ctypes.c_uint64, ctypes.c_uint32, vp,
+                                   ctypes.c_uint64, u64p, P(Stats)]
+        L.m6502_enumerate.argtypes = [vp, P(SearchCfg), ctypes.c_uint32, ctypes.c_uint32,
+                                      ctypes.c_uint32, vp, ctypes.c_uint64, u64p, P(Stats)]
+        L.m6502_insn_table.argtypes = [ctypes.c_uint32, u16p]
+        L.m6502_enumerate_targets.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, u16p,
+                                              ctypes.c_uint64]
+        L.m6502_enumerate_targets.restype = ctypes.c_uint64
+        L.m6502_disasm.argtypes = [ctypes.c_uint16, ctypes.c_char_p, ctypes.c_int]
+        L.m6502_parse.argtypes = [ctypes.c_char_p, u16p, ctypes.c_int]
+        L.m6502_should_prune.argtypes = [u16p, ctypes.c_int]
+        L.m6502_seq_bytes.argtypes = [u16p, ctypes.c_int, ctypes.c_uint32]
+        L.m6502_seq_cycles.argtypes = [u16p, ctypes.c_int]
+        L.m6502_op_deps.argtypes = [ctypes.c_int, u16p]
+        L.m6502_format_jsonl.argtypes = [u16p, ctypes.c_int, P(Rule), ctypes.c_uint8,
+                                         ctypes.c_char_p, ctypes.c_int]
+        _lib = L
+        return L
+
+
+def ptr(a, ctype):
+    """ctypes pointer to a contiguous numpy array."""
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def u16(seq):
+    return np.ascontiguousarray(np.asarray(seq, dtype=np.uint16))

@@ -1,0 +1,210 @@
+"""Engine context and the batched verifier (mirror of pkg/search/verifier.go).
+
+``Engine`` owns one ``m6502_ctx`` (one CUDA stream on one device).  The
+module-level functions QuickCheck / MidCheck / ExhaustiveCheck (+Masked) /
+FlagDiff / Fingerprint / ShouldPrune keep the Go signatures and run on a
+shared default engine; the batch methods take many pairs at once.
+"""
+import ctypes
+import threading
+
+import numpy as np
+
+from . import _lib
+from ._lib import M6502Error
+
+
+def _csr(seqs):
+    offs = np.zeros(len(seqs) + 1, dtype=np.uint32)
+    for i, s in enumerate(seqs):
+        offs[i + 1] = offs[i] + len(s)
+    flat = np.zeros(max(int(offs[-1]), 1), dtype=np.uint16)
+    k = 0
+    for s in seqs:
+        flat[k:k + len(s)] = s
+        k += len(s)
+    return flat, offs
+
+
+class Engine:
+    def __init__(self, device=0, targets_per_pass=0):
+        self._L = _lib.lib()
+        self._ctx = ctypes.c_void_p()
+        opts = _lib.Opts(device, 0, targets_per_pass)
+        rc = self._L.m6502_create(ctypes.byref(self._ctx), ctypes.byref(opts))
+        if rc != _lib.M6502_OK:
+            raise M6502Error(rc, "m6502_create failed (no CUDA device?)")
+        self._lock = threading.Lock()
+
+    def close(self):
+        if self._ctx:
+            self._L.m6502_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        if rc != _lib.M6502_OK:
+            raise M6502Error(rc, self._L.m6502_last_error(self._ctx).decode())
+
+    @property
+    def stream(self):
+        return self._L.m6502_stream(self._ctx)
+
+    # ---- pairwise verifier ----
+    def check_pairs(self, targets, candidates, dead_flags=0, checks=_lib.CHECK_ALL,
+                    sweep=_lib.SWEEP_REFERENCE, exh_mode=_lib.EXH_CONES, flagdiff=False):
+        """Verdict bits per pair (bit0 QC, bit1 MidCheck, bit2 Exhaustive)."""
+        if len(targets) != len(candidates):
+            raise ValueError("targets and candidates differ in length")
+        n = len(targets)
+        tf, to = _csr(targets)
+        cf, co = _csr(candidates)
+        out = np.zeros(max(n, 1), dtype=np.uint8)
+        fd = np.zeros(max(n, 1), dtype=np.uint8)
+        P = _lib.ptr
+        with self._lock:
+            self._check(self._L.m6502_check_pairs(
+                self._ctx, n, P(tf, ctypes.c_uint16), P(to, ctypes.c_uint32), P(cf, ctypes.c_uint16),
+                P(co, ctypes.c_uint32), dead_flags, checks, sweep, exh_mode, P(out, ctypes.c_uint8),
+                P(fd, ctypes.c_uint8) if flagdiff else None))
+        return (out[:n], fd[:n]) if flagdiff else out[:n]
+
+    def fingerprints(self, seqs):
+        f, o = _csr(seqs)
+        out = np.zeros((max(len(seqs), 1), 64), dtype=np.uint8)
+        with self._lock:
+            self._check(self._L.m6502_fingerprint(self._ctx, len(seqs), _lib.ptr(f, ctypes.c_uint16),
+                                                  _lib.ptr(o, ctypes.c_uint32), _lib.ptr(out, ctypes.c_uint8)))
+        return out[:len(seqs)]
+
+    def exec_states(self, seqs, states):
+        """Runs seqs[i] from states[i] (tuples A,X,Y,P,S,M,S0,S1) on the device."""
+        f, o = _csr(seqs)
+        st = np.asarray(states, dtype=np.uint8).reshape(len(seqs), 8)
+        packed = np.ascontiguousarray(st).view(np.uint64).reshape(-1).copy()
+        out = np.zeros(max(len(seqs), 1), dtype=np.uint64)
+        with self._lock:
+            self._check(self._L.m6502_exec_batch(self._ctx, len(seqs), _lib.ptr(f, ctypes.c_uint16),
+                                                 _lib.ptr(o, ctypes.c_uint32), _lib.ptr(packed, ctypes.c_uint64),
+                                                 _lib.ptr(out, ctypes.c_uint64)))
+        b = out[:len(seqs)].view(np.uint8).reshape(-1, 8)
+        return [tuple(int(x) for x in row) for row in b]
+
+    # ---- search ----
+    @staticmethod
+    def _cfg(semantics, dead_flags, sweep, exh_mode, stages, max_cand_len, flags=0):
+        c = _lib.SearchCfg()
+        c.semantics, c.sweep, c.exh_mode, c.stages = semantics, sweep, exh_mode, stages
+        c.max_cand_len, c.flags, c.dead_flags = max_cand_len, flags, dead_flags
+        return c
+
+    def _run(self, fn, cap, *args):
+        st = _lib.Stats()
+        n_out = ctypes.c_uint64(0)
+        while True:
+            out = np.zeros(max(cap, 1), dtype=_lib.RULE_DTYPE)
+            rc = fn(*args, out.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(n_out), ctypes.byref(st))
+            if rc == _lib.M6502_E_OVERFLOW:
+                cap = int(n_out.value)
+                continue
+            self._check(rc)
+            return out[:n_out.value], st.as_dict()
+
+    def search(self, targets, dead_flags=0, semantics=_lib.SEM_CUDA, sweep=_lib.SWEEP_FULL,
+               exh_mode=_lib.EXH_CONES, stages=_lib.CHECK_ALL, max_cand_len=1, cap=None,
+               device_ptr=None):
+        """Searches targets (n x tlen array of packed insns, or a device pointer with
+        device_ptr=(ptr, n, tlen)) for shorter replacements.  Returns (rules, stats)."""
+        if device_ptr is not None:
+            tptr, n, tlen = device_ptr
+            flags = _lib.TARGETS_ON_DEVICE
+            keep = None
+        else:
+            keep = np.ascontiguousarray(np.asarray(targets, dtype=np.uint16))
+            if keep.ndim != 2:
+                raise ValueError("targets must be an n x tlen array")
+            n, tlen = keep.shape
+            tptr = keep.ctypes.data_as(ctypes.c_void_p)
+            flags = 0
+        cfg = self._cfg(semantics, dead_flags, sweep, exh_mode, stages, max_cand_len, flags)
+        cap = cap if cap is not None else max(1024, n // 2)
+        with self._lock:
+            rules, st = self._run(self._L.m6502_search, cap, self._ctx, ctypes.byref(cfg), tptr, n, tlen)
+        del keep
+        return rules, st
+
+    def enumerate(self, target_len=2, dead_flags=0, semantics=_lib.SEM_CUDA, sweep=_lib.SWEEP_FULL,
+                  exh_mode=_lib.EXH_CONES, stages=_lib.CHECK_ALL, first=0, last=2863, cap=1 << 21):
+        cfg = self._cfg(semantics, dead_flags, sweep, exh_mode, stages, 1)
+        with self._lock:
+            return self._run(self._L.m6502_enumerate, cap, self._ctx, ctypes.byref(cfg), target_len,
+                             first, last)
+
+
+_default = None
+_default_lock = threading.Lock()
+
+
+def default_engine():
+    global _default
+    with _default_lock:
+        if _default is None:
+            _default = Engine()
+        return _default
+
+
+# ---- Go verifier API (pkg/search/verifier.go) ----
+def _one(target, candidate, dead, checks, sweep=_lib.SWEEP_REFERENCE):
+    return int(default_engine().check_pairs([list(target)], [list(candidate)], dead, checks, sweep)[0])
+
+
+def QuickCheck(target, candidate):
+    return bool(_one(target, candidate, 0, _lib.CHECK_QC) & 1)
+
+
+def QuickCheckMasked(target, candidate, dead_flags):
+    return bool(_one(target, candidate, dead_flags, _lib.CHECK_QC) & 1)
+
+
+def MidCheck(target, candidate):
+    return bool(_one(target, candidate, 0, _lib.CHECK_MID) & 2)
+
+
+def MidCheckMasked(target, candidate, dead_flags):
+    return bool(_one(target, candidate, dead_flags, _lib.CHECK_MID) & 2)
+
+
+def ExhaustiveCheck(target, candidate, sweep=_lib.SWEEP_REFERENCE):
+    return bool(_one(target, candidate, 0, _lib.CHECK_EXH, sweep) & 4)
+
+
+def ExhaustiveCheckMasked(target, candidate, dead_flags, sweep=_lib.SWEEP_REFERENCE):
+    return bool(_one(target, candidate, dead_flags, _lib.CHECK_EXH, sweep) & 4)
+
+
+def FlagDiff(target, candidate):
+    _, fd = default_engine().check_pairs([list(target)], [list(candidate)], 0, 0, flagdiff=True)
+    return int(fd[0])
+
+
+def Fingerprint(seq):
+    return bytes(default_engine().fingerprints([list(seq)])[0])
+
+
+def ShouldPrune(seq):
+    a = _lib.u16(seq)
+    r = _lib.lib().m6502_should_prune(_lib.ptr(a, ctypes.c_uint16), len(a))
+    if r < 0:
+        raise ValueError("opcode out of range")
+    return bool(r)
+
+
+TestVectorCount = 8
+MidCheckVectorCount = 32
+FingerprintLen = 64
+DeadNone, DeadAll = 0x00, 0xFF

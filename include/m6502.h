@@ -1,0 +1,211 @@
+/*
+ * m6502.h -- C ABI of libm6502gpu.so, the B200 engine for the 6502
+ * superoptimizer's equivalence-checking path (QuickCheck -> MidCheck ->
+ * ExhaustiveCheck, target enumeration and rule emission).
+ *
+ * Conventions
+ *  - An instruction is a uint16_t: op | (imm << 8), op in [0, 58) numbered
+ *    as the reference's pkg/inst/instruction.go:42-121, imm the 8-bit
+ *    immediate (0 for non-immediate ops).
+ *  - All buffers passed in are caller-owned HOST memory unless a flag says
+ *    otherwise; the library keeps no pointer after a call returns.
+ *  - Every call returns M6502_OK (0) or a negative M6502_E_* code; the text
+ *    of the last error of a context is m6502_last_error(ctx).
+ *  - Calls on one context are serialised by the context; different contexts
+ *    are independent (one CUDA stream each), so a goroutine / thread pool may
+ *    give each worker its own context.
+ *  - Device-side waits are bounded; nothing in the library spins forever.
+ */
+#ifndef M6502_H
+#define M6502_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define M6502_ABI_VERSION 1
+
+enum {
+    M6502_OK = 0,
+    M6502_E_INVAL = -1,     /* bad argument (opcode >= 58, length out of range, NULL) */
+    M6502_E_CUDA = -2,      /* a CUDA call failed; see m6502_last_error */
+    M6502_E_NOMEM = -3,     /* device allocation failed */
+    M6502_E_OVERFLOW = -4,  /* caller's output capacity too small; *n_out holds the need */
+    M6502_E_NODEV = -5      /* no CUDA device / the library was built without one */
+};
+
+/* Which reference pipeline's rules a search reproduces. */
+enum {
+    M6502_SEM_CUDA = 0, /* cuda/6502_search_v2.cu:848-977: every passing candidate,
+                           CUDA byte sizes, QC -> MidCheck -> Exhaustive */
+    M6502_SEM_GO = 1    /* pkg/search/worker.go:119-245: first passing candidate in Go
+                           order, Go byte sizes, QC -> Exhaustive, masked pass with
+                           DeadFlags = FlagDiff */
+};
+
+/* Input space of ExhaustiveCheck for pairs reading >= 3 extra registers. */
+enum {
+    M6502_SWEEP_REFERENCE = 0, /* 32 representative values per register
+                                  (pkg/search/verifier.go:377-415) */
+    M6502_SWEEP_FULL = 1       /* all 256 values of every swept register */
+};
+
+/* How the exhaustive sweep is evaluated (same verdicts, different cost). */
+enum {
+    M6502_EXH_CONES = 0, /* exact decomposition by per-output input cones */
+    M6502_EXH_BRUTE = 1  /* every state of the product space */
+};
+
+/* Stage / check bits. */
+enum {
+    M6502_CHECK_QC = 1,   /* QuickCheck: 8 vectors (verifier.go:84-93, 427-439) */
+    M6502_CHECK_MID = 2,  /* MidCheck: 32 vectors (verifier.go:96-105, 442-454) */
+    M6502_CHECK_EXH = 4,  /* ExhaustiveCheck (verifier.go:262-415, 457-588) */
+    M6502_CHECK_ALL = 7
+};
+
+/* m6502_search_cfg.flags */
+enum {
+    M6502_TARGETS_ON_DEVICE = 1 /* `targets` is a device pointer (already in HBM) */
+};
+
+typedef struct m6502_ctx m6502_ctx;
+
+typedef struct m6502_opts {
+    int32_t device;            /* CUDA device ordinal */
+    uint32_t flags;            /* reserved, 0 */
+    uint64_t targets_per_pass; /* targets per device pass; 0 = 2^21 */
+} m6502_opts;
+
+/* One rule: the target (index into the caller's list, or the enumeration
+ * id for m6502_enumerate) and its replacement. */
+typedef struct m6502_rule {
+    uint64_t target;    /* index into the caller's list, or enumeration id */
+    uint16_t cand[3];   /* replacement instructions, op | imm << 8 */
+    uint8_t cand_len;   /* 1..3 */
+    uint8_t dead_flags; /* flags the rule needs dead (SEM_CUDA: the run's mask;
+                           SEM_GO: FlagDiff of the masked pass, else 0) */
+} m6502_rule;           /* 16 bytes */
+
+typedef struct m6502_search_cfg {
+    uint32_t semantics;    /* M6502_SEM_* */
+    uint32_t sweep;        /* M6502_SWEEP_* */
+    uint32_t exh_mode;     /* M6502_EXH_* */
+    uint32_t stages;       /* M6502_CHECK_* bits of the pipeline; 0 = all.  Without
+                              EXH the MidCheck survivors are the rules
+                              (cuda/6502_search_v2.cu --no-exhaust). */
+    uint32_t max_cand_len; /* candidate lengths searched: 1 (default) */
+    uint32_t flags;        /* M6502_TARGETS_ON_DEVICE */
+    uint8_t dead_flags;    /* dead-flags mask of the run */
+    uint8_t reserved[7];
+} m6502_search_cfg;
+
+typedef struct m6502_stats {
+    uint64_t targets;     /* targets processed */
+    uint64_t pairs;       /* (target, candidate) pairs decided */
+    uint64_t qc_hits;     /* pairs passing byte filter, prune and QuickCheck */
+    uint64_t mid_hits;    /* ... and MidCheck (== qc_hits without MID) */
+    uint64_t exh_checked; /* pairs given to ExhaustiveCheck */
+    uint64_t exh_passed;  /* pairs ExhaustiveCheck accepted */
+    uint64_t rules;       /* rules emitted */
+    uint64_t exh_states;  /* states the exhaustive kernels evaluated */
+    uint64_t exh_items;   /* large sweeps split into device work-queue items */
+    uint64_t exh_algo_ops; /* algorithmic ops of the accepted pairs: product-sweep
+                              states x (10 per executed instruction + 3) */
+    uint64_t passes;      /* device passes (blocks of targets) */
+    double ms_device;     /* device time of the whole call, CUDA events */
+    double ms_fingerprint, ms_qc, ms_exhaustive, ms_exh_items, ms_emit; /* per-stage
+                              device time summed over passes, CUDA events */
+} m6502_stats;
+
+/* ---- context ---- */
+const char *m6502_version(void);
+int m6502_create(m6502_ctx **out, const m6502_opts *opts); /* opts may be NULL */
+void m6502_destroy(m6502_ctx *ctx);
+const char *m6502_last_error(const m6502_ctx *ctx);
+void *m6502_stream(m6502_ctx *ctx); /* the context's cudaStream_t */
+
+/* ---- pairwise verifier ----
+ * Replaces QuickCheck / MidCheck / ExhaustiveCheck (+Masked) and FlagDiff
+ * of pkg/search/verifier.go:84, 96, 262, 427, 442, 457, 591 for a batch of
+ * n pairs.  Pair i is (target i, candidate i); sequences are given as
+ * insns + offsets (CSR: sequence i is insns[offs[i] .. offs[i+1])), each
+ * 1..16 instructions.  out[i] bit 0 = QC, bit 1 = MidCheck, bit 2 =
+ * ExhaustiveCheck, for the bits requested in `checks` (each check is
+ * evaluated on its own, as the Go functions are).  flagdiff (optional) gets
+ * FlagDiff(target, candidate). */
+int m6502_check_pairs(m6502_ctx *ctx, uint64_t n,
+                      const uint16_t *t_insns, const uint32_t *t_offs,
+                      const uint16_t *c_insns, const uint32_t *c_offs,
+                      uint8_t dead_flags, uint32_t checks, uint32_t sweep, uint32_t exh_mode,
+                      uint8_t *out, uint8_t *flagdiff);
+
+/* Fingerprint (pkg/search/verifier.go:114-129) of n sequences (CSR),
+ * 64 bytes each. */
+int m6502_fingerprint(m6502_ctx *ctx, uint64_t n, const uint16_t *insns, const uint32_t *offs,
+                      uint8_t *out);
+
+/* Runs sequence i (CSR, any length) from packed input state states_in[i]
+ * and writes the packed result to states_out[i]: cpu.Exec over the
+ * sequence (pkg/cpu/exec.go:8-189).  Packed state: byte 0 A, 1 X, 2 Y,
+ * 3 P, 4 S, 5 M, 6 S0, 7 S1 (little-endian uint64_t). */
+int m6502_exec_batch(m6502_ctx *ctx, uint64_t n, const uint16_t *insns, const uint32_t *offs,
+                     const uint64_t *states_in, uint64_t *states_out);
+
+/* ---- search ----
+ * Searches n targets of tlen (1..3) instructions each (row-major in
+ * `targets`) for shorter replacements among all candidates of length
+ * 1..cfg->max_cand_len, through QC -> MidCheck -> ExhaustiveCheck on the
+ * device.  Rules are written to out (capacity cap); *n_out gets the rule
+ * count.  If cap is too small the call returns M6502_E_OVERFLOW with
+ * *n_out = the number needed and out holding the first cap rules.  Rule
+ * order is unspecified.  Replaces processTask/processTaskMasked
+ * (pkg/search/worker.go:119-245) and flush_batch (cuda/6502_search_v2.cu:848-977). */
+int m6502_search(m6502_ctx *ctx, const m6502_search_cfg *cfg, const uint16_t *targets,
+                 uint64_t n, uint32_t tlen, m6502_rule *out, uint64_t cap, uint64_t *n_out,
+                 m6502_stats *stats);
+
+/* All pruned targets of length tlen (2 or 3) whose first instruction has
+ * index in [first, last) of the CUDA-order table, searched as m6502_search
+ * does (cuda/6502_search_v2.cu:979-1043; pkg/search/search.go:22-76).
+ * rule.target is the enumeration id: sum of table indices i_k * 2863^(L-1-k). */
+int m6502_enumerate(m6502_ctx *ctx, const m6502_search_cfg *cfg, uint32_t tlen, uint32_t first,
+                    uint32_t last, m6502_rule *out, uint64_t cap, uint64_t *n_out,
+                    m6502_stats *stats);
+
+/* ---- host helpers (no GPU needed) ---- */
+/* The 2863 instructions in CUDA order (cuda/6502_search_v2.cu:741-752) or Go
+ * order (pkg/search/enumerator.go:14-38). */
+int m6502_insn_table(uint32_t semantics, uint16_t *out);
+/* Host enumeration of the pruned length-tlen (1..3) targets whose first
+ * instruction has CUDA-order index in [first, last), in CUDA order
+ * (cuda/6502_search_v2.cu:985-1037).  Writes at most cap targets (row-major)
+ * and returns the total count; out may be NULL to count only. */
+uint64_t m6502_enumerate_targets(uint32_t tlen, uint32_t first, uint32_t last, uint16_t *out,
+                                 uint64_t cap);
+/* Disassemble (pkg/inst/catalog.go:59-86); returns the text length. */
+int m6502_disasm(uint16_t insn, char *buf, int cap);
+/* parseAssembly (cmd/6502opt/main.go:302-322): "LDA #$42 : TAX" -> insns.
+ * Returns the count, or M6502_E_INVAL. */
+int m6502_parse(const char *text, uint16_t *out, int cap);
+/* ShouldPrune (pkg/search/pruner.go:6-34). */
+int m6502_should_prune(const uint16_t *seq, int n);
+/* SeqByteSize under the semantics' byte sizes; SeqCycles. */
+int m6502_seq_bytes(const uint16_t *seq, int n, uint32_t semantics);
+int m6502_seq_cycles(const uint16_t *seq, int n);
+/* Dataflow model used by the cone decomposition: for opcode op, deps[l] is
+ * the set of input locations location l's new value may depend on
+ * (locations A,X,Y,S,M,S0,S1,C,Z,I,D,V,N = bits 0..12).  Returns the mask
+ * of written locations, or M6502_E_INVAL. */
+int m6502_op_deps(int op, uint16_t deps[13]);
+/* One JSONL rule line of cuda/6502_search_v2.cu:912-930. */
+int m6502_format_jsonl(const uint16_t *target, int tlen, const m6502_rule *rule,
+                       uint8_t run_dead_flags, char *buf, int cap);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
