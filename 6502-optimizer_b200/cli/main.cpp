@@ -1,0 +1,406 @@
+// 6502opt -- command-line driver over libm6502gpu.so, mirroring the
+// reference CLI (cmd/6502opt/main.go) and the CUDA pipeline's flags
+// (cuda/6502_search_v2.cu:768-789):
+//
+//   6502opt enumerate [--max-target N] [--output FILE] [--dead-flags M] [-v]
+//                     [--jsonl] [--semantics go|cuda] [--sweep full|reference]
+//                     [--first-op-start A] [--first-op-end B] [--no-exhaust]
+//                     [--gpu-id N] [--checkpoint FILE] [--workers N]
+//   6502opt target "LDA #$00 : TAX" [--max-candidate N] [--dead-flags M] [-v]
+//   6502opt verify-jsonl FILE [--dead-flags M] [-v] [--sweep full|reference]
+//
+// All checking runs on the GPU through the C ABI; there is no CPU path.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "m6502.h"
+
+namespace {
+
+struct Args {
+    std::vector<std::string> pos;
+    std::map<std::string, std::string> kv;
+    bool has(const std::string& k) const { return kv.count(k) != 0; }
+    std::string get(const std::string& k, const std::string& d) const {
+        auto it = kv.find(k);
+        return it == kv.end() ? d : it->second;
+    }
+    long num(const std::string& k, long d) const { return has(k) ? std::strtol(kv.at(k).c_str(), nullptr, 0) : d; }
+};
+
+const char* kFlagsNoValue[] = {"-v", "--verbose", "--jsonl", "--no-exhaust", "--help", "-h"};
+
+Args parse_args(int argc, char** argv, int start) {
+    Args a;
+    for (int i = start; i < argc; i++) {
+        std::string s = argv[i];
+        bool novalue = false;
+        for (const char* f : kFlagsNoValue) novalue = novalue || s == f;
+        if (novalue) { a.kv[s] = "1"; continue; }
+        if (s.rfind("--", 0) == 0 || (s.size() == 2 && s[0] == '-')) {
+            size_t eq = s.find('=');
+            if (eq != std::string::npos) a.kv[s.substr(0, eq)] = s.substr(eq + 1);
+            else if (i + 1 < argc) a.kv[s] = argv[++i];
+            else a.kv[s] = "";
+            continue;
+        }
+        a.pos.push_back(s);
+    }
+    return a;
+}
+
+// parseDeadFlags (cmd/6502opt/main.go:285-299): none, all, or hex.
+bool parse_dead(const std::string& s0, uint8_t* out) {
+    std::string s;
+    for (char c : s0) s += (char)std::tolower((unsigned char)c);
+    if (s == "none" || s.empty()) { *out = 0; return true; }
+    if (s == "all") { *out = 0xFF; return true; }
+    if (s.rfind("0x", 0) == 0) s = s.substr(2);
+    char* end = nullptr;
+    unsigned long v = std::strtoul(s.c_str(), &end, 16);
+    if (s.empty() || *end || v > 0xFF) return false;
+    *out = (uint8_t)v;
+    return true;
+}
+
+// DeadFlagDesc (pkg/result/output.go:77-101).
+std::string dead_desc(uint8_t m) {
+    if (!m) return "";
+    if (m == 0xFF) return "all";
+    const std::pair<uint8_t, const char*> f[] = {{0x01, "C"}, {0x02, "Z"}, {0x04, "I"}, {0x08, "D"}, {0x40, "V"}, {0x80, "N"}};
+    std::string s;
+    for (auto& p : f)
+        if (m & p.first) { if (!s.empty()) s += ","; s += p.second; }
+    return s;
+}
+
+std::string disasm(uint16_t insn) {
+    char b[32];
+    m6502_disasm(insn, b, sizeof b);
+    return b;
+}
+
+std::string disasm_seq(const uint16_t* s, int n) {
+    std::string r;
+    for (int i = 0; i < n; i++) { if (i) r += " : "; r += disasm(s[i]); }
+    return r;
+}
+
+m6502_ctx* open_ctx(int device) {
+    m6502_opts o{};
+    o.device = device;
+    m6502_ctx* ctx = nullptr;
+    int rc = m6502_create(&ctx, &o);
+    if (rc != M6502_OK) {
+        std::fprintf(stderr, "error: cannot open GPU %d (code %d): the engine needs a CUDA device\n", device, rc);
+        std::exit(2);
+    }
+    return ctx;
+}
+
+void die(m6502_ctx* ctx, int rc, const char* what) {
+    std::fprintf(stderr, "error: %s failed (%d): %s\n", what, rc, ctx ? m6502_last_error(ctx) : "");
+    std::exit(1);
+}
+
+struct OutRule {
+    std::vector<uint16_t> src, rep;
+    int bytes_saved, cycles_saved;
+    uint8_t dead;
+};
+
+std::string json_str(const std::string& s) {
+    std::string r = "\"";
+    for (char c : s) {
+        if (c == '"' || c == '\\') { r += '\\'; r += c; }
+        else r += c;
+    }
+    return r + "\"";
+}
+
+// WriteJSON (pkg/result/output.go:21-35): pretty array, 2-space indent.
+void write_json(std::ostream& os, const std::vector<OutRule>& rules) {
+    if (rules.empty()) { os << "[]\n"; return; }
+    os << "[\n";
+    for (size_t i = 0; i < rules.size(); i++) {
+        const OutRule& r = rules[i];
+        os << "  {\n    \"source\": [\n";
+        for (size_t k = 0; k < r.src.size(); k++)
+            os << "      " << json_str(disasm(r.src[k])) << (k + 1 < r.src.size() ? ",\n" : "\n");
+        os << "    ],\n    \"replacement\": [\n";
+        for (size_t k = 0; k < r.rep.size(); k++)
+            os << "      " << json_str(disasm(r.rep[k])) << (k + 1 < r.rep.size() ? ",\n" : "\n");
+        os << "    ],\n    \"bytes_saved\": " << r.bytes_saved << ",\n    \"cycles_saved\": " << r.cycles_saved;
+        std::string d = dead_desc(r.dead);
+        if (!d.empty()) os << ",\n    \"dead_flags\": " << json_str(d);
+        os << "\n  }" << (i + 1 < rules.size() ? ",\n" : "\n");
+    }
+    os << "]\n";
+}
+
+std::vector<uint16_t> decode_target(uint64_t id, int len, const uint16_t* tab) {
+    std::vector<uint16_t> t((size_t)len);
+    for (int k = len - 1; k >= 0; k--) { t[(size_t)k] = tab[id % 2863]; id /= 2863; }
+    return t;
+}
+
+int cmd_enumerate(const Args& a) {
+    uint8_t dead = 0;
+    if (!parse_dead(a.get("--dead-flags", "none"), &dead)) {
+        std::fprintf(stderr, "invalid --dead-flags value: use none, all, or hex (e.g. 0xFF)\n");
+        return 1;
+    }
+    int max_target = (int)a.num("--max-target", 2);
+    bool jsonl = a.has("--jsonl");
+    std::string sem = a.get("--semantics", jsonl ? "cuda" : "go");
+    bool go = sem == "go";
+    std::string sweep = a.get("--sweep", go ? "reference" : "full");
+    bool verbose = a.has("-v") || a.has("--verbose");
+    uint32_t first = (uint32_t)a.num("--first-op-start", 0), last = (uint32_t)a.num("--first-op-end", 2863);
+    if (max_target < 2 || max_target > 3) { std::fprintf(stderr, "--max-target must be 2 or 3\n"); return 1; }
+    m6502_ctx* ctx = open_ctx((int)a.num("--gpu-id", 0));
+    uint16_t tab[2863];
+    m6502_insn_table(M6502_SEM_CUDA, tab);
+    FILE* info = jsonl ? stderr : stdout;
+    std::fprintf(info, "6502 Superoptimizer\n  Max target length: %d\n  Instructions: %d per position\n  Workers: %s\n",
+                 max_target, 2863, a.get("--workers", "GPU").c_str());
+    if (dead) std::fprintf(info, "  Dead flags: 0x%02X (%s)\n", dead, dead_desc(dead).c_str());
+    std::fprintf(info, "\n");
+
+    // Resume watermark: a checkpoint file holds the next first-op index to run.
+    std::string ckpt = a.get("--checkpoint", "");
+    if (!ckpt.empty()) {
+        std::ifstream in(ckpt);
+        uint32_t w;
+        if (in >> w && w > first) { first = std::min(w, last); std::fprintf(stderr, "resuming at first-op %u\n", first); }
+    }
+    m6502_search_cfg cfg{};
+    cfg.semantics = go ? M6502_SEM_GO : M6502_SEM_CUDA;
+    cfg.sweep = sweep == "reference" ? M6502_SWEEP_REFERENCE : M6502_SWEEP_FULL;
+    cfg.stages = a.has("--no-exhaust") ? (M6502_CHECK_QC | M6502_CHECK_MID) : M6502_CHECK_ALL;
+    cfg.max_cand_len = 1;
+    cfg.dead_flags = dead;
+    std::vector<OutRule> all;
+    uint64_t total_rules = 0;
+    for (int len = 2; len <= max_target; len++) {
+        if (verbose) std::fprintf(info, "=== Searching target length %d ===\n", len);
+        // Slices of first-op indices keep host buffers bounded and allow resume.
+        const uint32_t slice = len == 2 ? 2863 : 4;
+        for (uint32_t f = first; f < last; f += slice) {
+            uint32_t f1 = std::min(last, f + slice);
+            std::vector<m6502_rule> out(1u << 20);
+            uint64_t n = 0;
+            m6502_stats st{};
+            int rc;
+            while ((rc = m6502_enumerate(ctx, &cfg, (uint32_t)len, f, f1, out.data(), out.size(), &n, &st)) ==
+                   M6502_E_OVERFLOW)
+                out.resize(n);
+            if (rc != M6502_OK) die(ctx, rc, "m6502_enumerate");
+            total_rules += n;
+            std::sort(out.begin(), out.begin() + (long)n, [](const m6502_rule& x, const m6502_rule& y) {
+                return x.target != y.target ? x.target < y.target : x.cand[0] < y.cand[0];
+            });
+            for (uint64_t i = 0; i < n; i++) {
+                const m6502_rule& r = out[i];
+                std::vector<uint16_t> t = decode_target(r.target, len, tab);
+                if (jsonl) {
+                    char buf[512];
+                    m6502_format_jsonl(t.data(), len, &r, dead, buf, sizeof buf);
+                    std::fputs(buf, stdout);
+                    std::fputc('\n', stdout);
+                } else {
+                    uint32_t semb = go ? M6502_SEM_GO : M6502_SEM_CUDA;
+                    OutRule o{t, std::vector<uint16_t>(r.cand, r.cand + r.cand_len),
+                              m6502_seq_bytes(t.data(), len, semb) - m6502_seq_bytes(r.cand, r.cand_len, semb),
+                              m6502_seq_cycles(t.data(), len) - m6502_seq_cycles(r.cand, r.cand_len), r.dead_flags};
+                    if (verbose)
+                        std::printf("  FOUND%s: %s -> %s (-%d bytes, -%d cycles)\n",
+                                    r.dead_flags ? (" (dead flags 0x" + std::string(1, "0123456789ABCDEF"[r.dead_flags >> 4]) +
+                                                    std::string(1, "0123456789ABCDEF"[r.dead_flags & 15]) + ")").c_str() : "",
+                                    disasm_seq(t.data(), len).c_str(), disasm_seq(r.cand, r.cand_len).c_str(),
+                                    o.bytes_saved, o.cycles_saved);
+                    all.push_back(std::move(o));
+                }
+            }
+            if (jsonl) std::fflush(stdout);
+            std::fprintf(stderr, "  [len %d] first-op %u..%u | targets:%llu | QC:%llu Mid:%llu Ex:%llu | found:%llu | %.0f ms\n",
+                         len, f, f1, (unsigned long long)st.targets, (unsigned long long)st.qc_hits,
+                         (unsigned long long)st.mid_hits, (unsigned long long)st.exh_checked,
+                         (unsigned long long)n, st.ms_device);
+            if (!ckpt.empty()) { std::ofstream o(ckpt); o << f1 << "\n"; }
+        }
+    }
+    if (!jsonl) {
+        std::stable_sort(all.begin(), all.end(), [](const OutRule& x, const OutRule& y) {
+            return x.bytes_saved != y.bytes_saved ? x.bytes_saved > y.bytes_saved : x.cycles_saved > y.cycles_saved;
+        });
+        std::printf("\nFound %zu optimizations\n", all.size());
+        std::string output = a.get("--output", "");
+        if (!output.empty()) {
+            std::ofstream os(output);
+            if (!os) { std::fprintf(stderr, "cannot write %s\n", output.c_str()); return 1; }
+            write_json(os, all);
+            std::printf("Written to %s\n", output.c_str());
+        }
+    } else {
+        std::fprintf(stderr, "Results found:      %llu\n", (unsigned long long)total_rules);
+    }
+    m6502_destroy(ctx);
+    return 0;
+}
+
+int cmd_target(const Args& a) {
+    if (a.pos.empty()) { std::fprintf(stderr, "usage: 6502opt target \"INSN : INSN ...\"\n"); return 1; }
+    std::string input;
+    for (size_t i = 0; i < a.pos.size(); i++) { if (i) input += " "; input += a.pos[i]; }
+    uint16_t seq[16];
+    int n = m6502_parse(input.c_str(), seq, 16);
+    if (n < 0) { std::fprintf(stderr, "failed to parse: %s\n", input.c_str()); return 1; }
+    if (n > 3) { std::fprintf(stderr, "targets of more than 3 instructions: use `6502opt stoke`\n"); return 1; }
+    uint8_t dead = 0;
+    if (!parse_dead(a.get("--dead-flags", "none"), &dead)) { std::fprintf(stderr, "invalid --dead-flags\n"); return 1; }
+    long maxc = a.num("--max-candidate", 4);
+    std::printf("Target: %s (%d bytes, %d cycles)\n", input.c_str(), m6502_seq_bytes(seq, n, M6502_SEM_GO),
+                m6502_seq_cycles(seq, n));
+    m6502_ctx* ctx = open_ctx((int)a.num("--gpu-id", 0));
+    m6502_search_cfg cfg{};
+    cfg.semantics = M6502_SEM_GO;
+    cfg.sweep = M6502_SWEEP_REFERENCE;
+    cfg.max_cand_len = maxc >= 1 ? 1 : 0;
+    cfg.dead_flags = dead;
+    m6502_rule out[4];
+    uint64_t k = 0;
+    int rc = maxc >= 1 ? m6502_search(ctx, &cfg, seq, 1, (uint32_t)n, out, 4, &k, nullptr) : M6502_OK;
+    if (rc != M6502_OK) die(ctx, rc, "m6502_search");
+    // SearchSingle(Masked) returns the best rule: most bytes, then cycles saved.
+    int best = -1, bb = -1, bc = -1;
+    for (uint64_t i = 0; i < k; i++) {
+        int b = m6502_seq_bytes(seq, n, M6502_SEM_GO) - m6502_seq_bytes(out[i].cand, out[i].cand_len, M6502_SEM_GO);
+        int c = m6502_seq_cycles(seq, n) - m6502_seq_cycles(out[i].cand, out[i].cand_len);
+        if (b > bb || (b == bb && c > bc)) { best = (int)i; bb = b; bc = c; }
+    }
+    if (best < 0) std::printf("No shorter replacement found.\n");
+    else std::printf("Replacement: %s (-%d bytes, -%d cycles)\n", disasm_seq(out[best].cand, out[best].cand_len).c_str(), bb, bc);
+    m6502_destroy(ctx);
+    return 0;
+}
+
+// Value of a string field in one JSON object line (no nesting needed here).
+bool json_field(const std::string& line, const std::string& key, std::string* out) {
+    std::string pat = "\"" + key + "\"";
+    size_t p = line.find(pat);
+    if (p == std::string::npos) return false;
+    p = line.find(':', p + pat.size());
+    if (p == std::string::npos) return false;
+    p = line.find('"', p);
+    if (p == std::string::npos) return false;
+    std::string v;
+    for (size_t i = p + 1; i < line.size(); i++) {
+        if (line[i] == '\\' && i + 1 < line.size()) { v += line[++i]; continue; }
+        if (line[i] == '"') { *out = v; return true; }
+        v += line[i];
+    }
+    return false;
+}
+
+int cmd_verify(const Args& a) {
+    if (a.pos.empty()) { std::fprintf(stderr, "usage: 6502opt verify-jsonl FILE\n"); return 1; }
+    uint8_t dead = 0;
+    if (!parse_dead(a.get("--dead-flags", "none"), &dead)) { std::fprintf(stderr, "invalid --dead-flags\n"); return 1; }
+    bool verbose = a.has("-v") || a.has("--verbose");
+    uint32_t sweep = a.get("--sweep", "reference") == "full" ? M6502_SWEEP_FULL : M6502_SWEEP_REFERENCE;
+    std::ifstream in(a.pos[0]);
+    if (!in) { std::fprintf(stderr, "cannot open %s\n", a.pos[0].c_str()); return 1; }
+    m6502_ctx* ctx = open_ctx((int)a.num("--gpu-id", 0));
+    uint64_t total = 0, passed = 0, failed = 0, skipped = 0;
+    std::vector<uint16_t> ti, ci;
+    std::vector<uint32_t> to{0}, co{0};
+    std::vector<std::pair<uint64_t, std::string>> names;
+    auto flush = [&]() {
+        size_t n = names.size();
+        if (!n) return;
+        std::vector<uint8_t> res(n);
+        int rc = m6502_check_pairs(ctx, n, ti.data(), to.data(), ci.data(), co.data(), dead, M6502_CHECK_EXH, sweep,
+                                   M6502_EXH_CONES, res.data(), nullptr);
+        if (rc != M6502_OK) die(ctx, rc, "m6502_check_pairs");
+        for (size_t i = 0; i < n; i++) {
+            if (res[i] & M6502_CHECK_EXH) {
+                passed++;
+                if (verbose) std::printf("  [%llu] PASS: %s\n", (unsigned long long)names[i].first, names[i].second.c_str());
+            } else {
+                failed++;
+                std::printf("  [%llu] FAIL: %s\n", (unsigned long long)names[i].first, names[i].second.c_str());
+            }
+        }
+        ti.clear(); ci.clear(); to.assign(1, 0); co.assign(1, 0); names.clear();
+    };
+    std::string line;
+    while (std::getline(in, line)) {
+        size_t b = line.find_first_not_of(" \t\r\n");
+        if (b == std::string::npos) continue;
+        total++;
+        std::string src, rep;
+        uint16_t s[16], r[16];
+        int ns, nr;
+        if (!json_field(line, "source_asm", &src) || !json_field(line, "replacement_asm", &rep)) {
+            std::fprintf(stderr, "  [%llu] JSON parse error\n", (unsigned long long)total);
+            skipped++;
+            continue;
+        }
+        if ((ns = m6502_parse(src.c_str(), s, 16)) < 0) {
+            std::fprintf(stderr, "  [%llu] Cannot parse source \"%s\"\n", (unsigned long long)total, src.c_str());
+            skipped++;
+            continue;
+        }
+        if ((nr = m6502_parse(rep.c_str(), r, 16)) < 0) {
+            std::fprintf(stderr, "  [%llu] Cannot parse replacement \"%s\"\n", (unsigned long long)total, rep.c_str());
+            skipped++;
+            continue;
+        }
+        ti.insert(ti.end(), s, s + ns);
+        to.push_back((uint32_t)ti.size());
+        ci.insert(ci.end(), r, r + nr);
+        co.push_back((uint32_t)ci.size());
+        names.emplace_back(total, src + " -> " + rep);
+        if (names.size() >= (1u << 20)) flush();
+    }
+    flush();
+    std::printf("\nVerification complete: %llu total, %llu passed, %llu failed, %llu skipped\n",
+                (unsigned long long)total, (unsigned long long)passed, (unsigned long long)failed,
+                (unsigned long long)skipped);
+    m6502_destroy(ctx);
+    if (failed) {
+        std::fprintf(stderr, "Error: %llu rules failed verification\n", (unsigned long long)failed);
+        return 1;
+    }
+    return 0;
+}
+
+void usage() {
+    std::fprintf(stderr,
+                 "6502opt -- 6502 superoptimizer on the B200 engine\n\n"
+                 "  enumerate      enumerate all target sequences and find shorter replacements\n"
+                 "  target         find the optimal replacement for one instruction sequence\n"
+                 "  verify-jsonl   verify JSONL rules with ExhaustiveCheck on the GPU\n");
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc < 2) { usage(); return 1; }
+    std::string cmd = argv[1];
+    Args a = parse_args(argc, argv, 2);
+    if (cmd == "enumerate") return cmd_enumerate(a);
+    if (cmd == "target") return cmd_target(a);
+    if (cmd == "verify-jsonl") return cmd_verify(a);
+    usage();
+    return 1;
+}

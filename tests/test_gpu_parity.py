@@ -179,7 +179,7 @@ def test_enumerate_length2_published_counts(engine):
     assert st["mid_hits"] == PUBLISHED["mid_hits"]
     assert st["exh_checked"] == PUBLISHED["mid_hits"]
     assert len(rules) == st["rules"] == PUBLISHED["rules"]
-    assert len({int(r["target"]) * 4096 + int(r["cand"][0]) for r in rules}) == len(rules)
+    assert len({int(r["target"]) * 65536 + int(r["cand"][0]) for r in rules}) == len(rules)
 
 
 def test_enumerate_slices_union_equals_whole(engine):
