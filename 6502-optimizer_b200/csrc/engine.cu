@@ -815,6 +815,89 @@ __global__ void k_enum_targets(uint64_t id0, uint64_t id1, uint32_t len, uint16_
 }
 
 // ---------------------------------------------------------------------------
+// Fixed-scratch variant of the exhaustive check (m6502_exhaustive_static)
+// ---------------------------------------------------------------------------
+// For callers that cannot allocate device memory, the scratch of this one
+// variant -- a ticket counter and one fail flag per pair -- lives in a fixed
+// array compiled into the library.  Every GPU that loads the library holds
+// it (a little over 4 MiB) until the process exits.  All calls share it, so
+// calls that overlap on the GPU race; each call clears the part that must
+// start at zero.
+constexpr uint64_t kStaticMaxPairs = M6502_STATIC_MAX_PAIRS;
+
+struct StaticScratch {
+    Counters cnt;
+    uint32_t fail[kStaticMaxPairs];
+};
+
+static __device__ __align__(256) unsigned char g_static_scratch[sizeof(StaticScratch)];
+
+// CSR pairs in caller-owned device memory.  The inputs were never seen by
+// the host, so lengths and opcodes are validated here; an invalid pair is
+// reported instead of evaluated.
+struct StaticCsrSource {
+    const uint16_t* t_ins;
+    const uint32_t* t_off;
+    const uint16_t* c_ins;
+    const uint32_t* c_off;
+    uint32_t dead_;
+    __device__ bool load(uint64_t p, uint16_t* st, uint16_t* sc, int& tn, int& cn, uint32_t& dead,
+                         int lane) const {
+        uint32_t t0 = t_off[p], t1 = t_off[p + 1], c0 = c_off[p], c1 = c_off[p + 1];
+        dead = dead_;
+        if (t1 <= t0 || c1 <= c0 || t1 - t0 > (uint32_t)kMaxSeq || c1 - c0 > (uint32_t)kMaxSeq) return false;
+        tn = (int)(t1 - t0);
+        cn = (int)(c1 - c0);
+        bool ok = true;
+        if (lane < tn) { st[lane] = t_ins[t0 + lane]; ok = (st[lane] & 0xFFu) < NUM_OPS; }
+        if (lane < cn) { sc[lane] = c_ins[c0 + lane]; ok = ok && (sc[lane] & 0xFFu) < NUM_OPS; }
+        return __all_sync(kFull, ok);
+    }
+};
+
+// One pair per warp, every cone swept in-warp (no work-item queue, so the
+// only scratch is the ticket and the fail flags).  fail: 0 equivalent,
+// 1 not equivalent, 2 invalid pair.
+__global__ void __launch_bounds__(256) k_exhaustive_static(StaticCsrSource src, uint64_t n, uint32_t sweep,
+                                                            StaticScratch* scr) {
+    __shared__ uint16_t s_t[kWarpsPerBlock][kMaxSeq], s_c[kWarpsPerBlock][kMaxSeq];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned long long nstates = 0;
+    for (;;) {
+        unsigned long long p = 0;
+        if (lane == 0) p = atomicAdd(&scr->cnt.exh_ticket, 1ull);
+        p = __shfl_sync(kFull, p, 0);
+        if (p >= n) break;
+        PairView pv;
+        pv.t = s_t[w]; pv.c = s_c[w];
+        pv.tn = pv.cn = 0;
+        bool valid = src.load(p, s_t[w], s_c[w], pv.tn, pv.cn, pv.dead, lane);
+        __syncwarp();
+        if (!valid) {
+            if (lane == 0) scr->fail[p] = 2u;
+            continue;
+        }
+        Flow fl = dataflow(pv, lane);
+        const bool rep = sweep == M6502_SWEEP_REFERENCE && fl.k >= 3;
+        Groups g = make_groups(fl, pv.dead, rep, false, lane);
+        bool ok = true;
+        for (int i = 0; i < g.n && ok; i++) {
+            Fields f = make_fields(g.cone[i], fl.swept, rep);
+            ok = sweep_states(pv, f, g.mask[i], 0, 1ull << g.bits[i], nullptr, &nstates, lane);
+        }
+        if (lane == 0) scr->fail[p] = ok ? 0u : 1u;
+        __syncwarp();
+    }
+}
+
+__global__ void k_static_verdicts(const StaticScratch* scr, uint64_t n, uint8_t* __restrict__ out) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t f = scr->fail[i];
+        out[i] = f == 0 ? 1 : (f == 1 ? 0 : 0xFF);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 struct DevBuf {
@@ -1349,6 +1432,89 @@ int m6502_enumerate(m6502_ctx* ctx, const m6502_search_cfg* cfg, uint32_t tlen, 
     st.ms_device = ms;
     if (stats) *stats = st;
     return finish(ctx, out, cap, n_out);
+}
+
+
+}  // extern "C"
+
+namespace {
+
+// Per-device set-up of the fixed-scratch entry point: constant tables and
+// the device address of g_static_scratch (in host code the array's name is
+// only a stand-in, never a device address).
+struct StaticDevice {
+    bool ready = false;
+    StaticScratch* scratch = nullptr;
+    int blocks = 0;
+};
+constexpr int kStaticMaxDevices = 64;
+StaticDevice g_static_dev[kStaticMaxDevices];
+std::mutex g_static_mu;
+
+int static_setup(int dev, StaticDevice** out) {
+    std::lock_guard<std::mutex> lk(g_static_mu);
+    StaticDevice& d = g_static_dev[dev];
+    if (!d.ready) {
+        uint64_t vec[32];
+        for (int v = 0; v < 32; v++) {
+            uint64_t x = 0;
+            for (int b = 0; b < 8; b++) x |= (uint64_t)kVectors[v][b] << (8 * b);
+            vec[v] = x;
+        }
+        uint16_t dep[NUM_OPS][NUM_LOCS], wr[NUM_OPS], sw[NUM_OPS];
+        for (uint32_t op = 0; op < NUM_OPS; op++) {
+            wr[op] = (uint16_t)op_deps(op, dep[op]);
+            sw[op] = (uint16_t)sweep_locs_of_reads(op_reads(op));
+        }
+        uint32_t rep[32];
+        for (int i = 0; i < 32; i++) rep[i] = kRepValues[i];
+        if (cudaMemcpyToSymbol(c_vec, vec, sizeof vec) != cudaSuccess ||
+            cudaMemcpyToSymbol(c_dep, dep, sizeof dep) != cudaSuccess ||
+            cudaMemcpyToSymbol(c_wr, wr, sizeof wr) != cudaSuccess ||
+            cudaMemcpyToSymbol(c_sweep, sw, sizeof sw) != cudaSuccess ||
+            cudaMemcpyToSymbol(c_rep, rep, sizeof rep) != cudaSuccess)
+            return M6502_E_CUDA;
+        void* ptr = nullptr;
+        if (cudaGetSymbolAddress(&ptr, g_static_scratch) != cudaSuccess || !ptr) return M6502_E_CUDA;
+        int sms = 0, occ = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_exhaustive_static, 256, 0) != cudaSuccess)
+            return M6502_E_CUDA;
+        d.scratch = (StaticScratch*)ptr;
+        d.blocks = sms * std::max(occ, 1);
+        d.ready = true;
+    }
+    *out = &d;
+    return M6502_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int m6502_exhaustive_static(uint64_t n, const uint16_t* t_insns, const uint32_t* t_offs,
+                            const uint16_t* c_insns, const uint32_t* c_offs, uint8_t dead_flags,
+                            uint32_t sweep, uint8_t* out, void* stream) {
+    if (n > kStaticMaxPairs) return M6502_E_TOOBIG;
+    if (sweep > M6502_SWEEP_FULL) return M6502_E_INVAL;
+    if (n == 0) return M6502_OK;
+    if (!t_insns || !t_offs || !c_insns || !c_offs || !out) return M6502_E_INVAL;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return M6502_E_NODEV;
+    if (dev < 0 || dev >= kStaticMaxDevices) return M6502_E_INVAL;
+    StaticDevice* d = nullptr;
+    int rc = static_setup(dev, &d);
+    if (rc != M6502_OK) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (cudaMemsetAsync(&d->scratch->cnt, 0, sizeof(Counters), st) != cudaSuccess) return M6502_E_CUDA;
+    StaticCsrSource src{t_insns, t_offs, c_insns, c_offs, dead_flags};
+    uint64_t grid = std::min<uint64_t>((uint64_t)d->blocks, (n + kWarpsPerBlock - 1) / kWarpsPerBlock);
+    k_exhaustive_static<<<(uint32_t)grid, 256, 0, st>>>(src, n, sweep, d->scratch);
+    if (cudaGetLastError() != cudaSuccess) return M6502_E_CUDA;
+    uint64_t vgrid = std::min<uint64_t>((n + 255) / 256, 4096);
+    k_static_verdicts<<<(uint32_t)vgrid, 256, 0, st>>>(d->scratch, n, out);
+    if (cudaGetLastError() != cudaSuccess) return M6502_E_CUDA;
+    return M6502_OK;
 }
 
 }  // extern "C"

@@ -19,6 +19,8 @@ M6502_E_CUDA = -2
 M6502_E_NOMEM = -3
 M6502_E_OVERFLOW = -4
 M6502_E_NODEV = -5
+M6502_E_TOOBIG = -6
+STATIC_MAX_PAIRS = 1 << 20
 
 SEM_CUDA, SEM_GO = 0, 1
 SWEEP_REFERENCE, SWEEP_FULL = 0, 1
@@ -75,6 +77,7 @@ SYMBOLS = (
     "m6502_check_pairs", "m6502_fingerprint", "m6502_exec_batch", "m6502_search", "m6502_enumerate",
     "m6502_insn_table", "m6502_enumerate_targets", "m6502_disasm", "m6502_parse", "m6502_should_prune",
     "m6502_seq_bytes", "m6502_seq_cycles", "m6502_op_deps", "m6502_format_jsonl",
+    "m6502_exhaustive_static",
 )
 
 
@@ -118,6 +121,8 @@ def lib():
         L.m6502_op_deps.argtypes = [ctypes.c_int, u16p]
         L.m6502_format_jsonl.argtypes = [u16p, ctypes.c_int, P(Rule), ctypes.c_uint8,
                                          ctypes.c_char_p, ctypes.c_int]
+        L.m6502_exhaustive_static.argtypes = [ctypes.c_uint64, vp, vp, vp, vp, ctypes.c_uint8, ctypes.c_uint32,
+                                              vp, vp]
         _lib = L
         return L
 

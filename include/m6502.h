@@ -34,7 +34,8 @@ enum {
     M6502_E_CUDA = -2,      /* a CUDA call failed; see m6502_last_error */
     M6502_E_NOMEM = -3,     /* device allocation failed */
     M6502_E_OVERFLOW = -4,  /* caller's output capacity too small; *n_out holds the need */
-    M6502_E_NODEV = -5      /* no CUDA device / the library was built without one */
+    M6502_E_NODEV = -5,     /* no CUDA device / the library was built without one */
+    M6502_E_TOOBIG = -6     /* request exceeds a fixed capacity (m6502_exhaustive_static) */
 };
 
 /* Which reference pipeline's rules a search reproduces. */
@@ -154,6 +155,33 @@ int m6502_fingerprint(m6502_ctx *ctx, uint64_t n, const uint16_t *insns, const u
  * 3 P, 4 S, 5 M, 6 S0, 7 S1 (little-endian uint64_t). */
 int m6502_exec_batch(m6502_ctx *ctx, uint64_t n, const uint16_t *insns, const uint32_t *offs,
                      const uint64_t *states_in, uint64_t *states_out);
+
+/* ExhaustiveCheck(Masked) for callers that cannot allocate device memory.
+ *
+ * No counterpart in the reference: it is an extra entry point of this
+ * library.  Some callers cannot call cudaMalloc: a process whose device memory
+ * is fully claimed by another allocator (a framework's caching allocator, a
+ * fixed memory budget), or a latency-critical path on which cudaMalloc /
+ * cudaFree would synchronise the whole device.  This call allocates nothing:
+ * its scratch (one flag per pair and a work ticket) is a fixed array inside
+ * the library, M6502_STATIC_MAX_PAIRS pairs long (a little over 4 MiB on every
+ * GPU that loads the library, held until the process exits).
+ *
+ * All pointers are caller-owned DEVICE memory on the current device: pairs
+ * as CSR (t_insns/t_offs, c_insns/c_offs, n + 1 offsets each, 1..16
+ * instructions per sequence).  out[i] = 1 equivalent, 0 not equivalent, 0xFF
+ * invalid pair (length or opcode out of range).  Runs asynchronously on
+ * `stream` (a cudaStream_t; NULL = the legacy default stream); read `out`
+ * after synchronising it.  Returns M6502_E_TOOBIG for n >
+ * M6502_STATIC_MAX_PAIRS.  The first call on a device uploads the instruction
+ * tables and looks up the scratch address; make that first call before any
+ * stream capture.  Every call shares the one scratch array and leaves it
+ * holding its own results, so calls that overlap on the GPU race: issue them
+ * on one stream, or wait for one before the next. */
+#define M6502_STATIC_MAX_PAIRS (1u << 20)
+int m6502_exhaustive_static(uint64_t n, const uint16_t *t_insns, const uint32_t *t_offs,
+                            const uint16_t *c_insns, const uint32_t *c_offs, uint8_t dead_flags,
+                            uint32_t sweep, uint8_t *out, void *stream);
 
 /* ---- search ----
  * Searches n targets of tlen (1..3) instructions each (row-major in
