@@ -142,14 +142,16 @@ def run_reference(args):
 
 
 def load_traffic():
-    """Per-launch DRAM bytes of the dominant kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
+    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of
+    each kernel from the committed ncu summary, profiles/traffic.txt."""
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
+    out = {}
     if os.path.exists(p):
-        try:
-            return json.load(open(p))
-        except ValueError:
-            return {}
-    return {}
+        for line in open(p):
+            parts = line.split()
+            if len(parts) == 2 and parts[1].isdigit():
+                out[parts[0]] = int(parts[1])
+    return out
 
 
 def run_engine(args):
@@ -268,7 +270,8 @@ def run_engine(args):
             "roofline": {"bound": "int-issue", "kernel": dominant, "achieved": achieved / 1e12,
                          "peak": peak_lane_ops / 1e12, "unit": "Tlane-op/s",
                          "frac": achieved / peak_lane_ops if peak_lane_ops else None,
-                         "traffic": traffic, "algorithmic": alg,
+                         "traffic": traffic, "traffic_unit": "DRAM bytes per launch (one 2^21-target pass)",
+                         "algorithmic": alg,
                          "peak_basis": f"{sms} SMs x 128 int32 lanes x {f_mhz:.0f} MHz (median SM clock sampled)",
                          "note": "exhaustive work is counted as the full product sweep; the cone "
                                  "decomposition evaluates fewer states, so frac may exceed 1 "
