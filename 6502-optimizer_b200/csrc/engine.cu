@@ -138,7 +138,7 @@ constexpr uint32_t kSurvLen2 = 1u << 23, kSurvMasked = 1u << 24;
 __host__ __device__ __forceinline__ uint32_t fd_pack(uint32_t fd) { return (fd & 0x0Fu) | ((fd >> 2) & 0x30u); }
 
 struct Counters {
-    unsigned long long qc, mid, surv, exh_ticket, items, item_ticket, rules, exh_pass, states, algo;
+    unsigned long long qc, mid, surv, exh_ticket, items, item_ticket, rules, exh_pass, states, algo, probe_rejects;
 };
 
 struct Item {   // one chunk of a large cone sweep
@@ -236,31 +236,59 @@ __device__ __forceinline__ uint32_t fld(const Fields& f, int i, uint64_t s) {
     return v | f.base[i];
 }
 
+// Per-byte compare masks of a packed output mask.
+struct OutMask {
+    uint32_t a, x, y, p, s, m, s0, s1;
+};
+__device__ __forceinline__ OutMask out_mask(uint64_t om) {
+    return OutMask{(uint32_t)om & 0xFFu,         (uint32_t)(om >> 8) & 0xFFu,  (uint32_t)(om >> 16) & 0xFFu,
+                   (uint32_t)(om >> 24) & 0xFFu, (uint32_t)(om >> 32) & 0xFFu, (uint32_t)(om >> 40) & 0xFFu,
+                   (uint32_t)(om >> 48) & 0xFFu, (uint32_t)(om >> 56) & 0xFFu};
+}
+
+// Nonzero when target and candidate disagree on a compared output from
+// the input state with index s.
+__device__ __forceinline__ uint32_t state_diff(const PairView& pv, const Fields& f, const OutMask& m, uint64_t s) {
+    St in;
+    in.a = fld(f, 0, s); in.x = fld(f, 1, s); in.y = fld(f, 2, s); in.s = fld(f, 3, s);
+    in.m = fld(f, 4, s); in.s0 = fld(f, 5, s); in.s1 = fld(f, 6, s); in.p = fld(f, 7, s);
+    St t = in, c = in;
+    for (int i = 0; i < pv.tn; i++) exec(t, pv.t[i]);
+    for (int i = 0; i < pv.cn; i++) exec(c, pv.c[i]);
+    return ((t.a ^ c.a) & m.a) | ((t.x ^ c.x) & m.x) | ((t.y ^ c.y) & m.y) | ((t.p ^ c.p) & m.p) |
+           ((t.s ^ c.s) & m.s) | ((t.m ^ c.m) & m.m) | ((t.s0 ^ c.s0) & m.s0) | ((t.s1 ^ c.s1) & m.s1);
+}
+
+// Probe: 64 pseudo-random states of the pair's whole sweep domain, all
+// outputs compared.  A mismatch anywhere in the domain decides the pair
+// (not equivalent) without the cone analysis; passing decides nothing.
+__device__ __forceinline__ bool probe_domain(const PairView& pv, uint32_t swept, bool rep, uint32_t dead,
+                                             uint64_t salt, int lane) {
+    Fields f = make_fields(swept, swept, rep);
+    const OutMask m = out_mask(cmp_mask(dead));
+    const uint64_t dom = (f.bits >= 64) ? ~0ull : ((1ull << f.bits) - 1);
+    for (int it = 0; it < 2; it++) {
+        uint64_t z = salt + (uint64_t)(lane + 32 * it) * 0x9E3779B97F4A7C15ull;
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        if (__any_sync(kFull, state_diff(pv, f, m, z & dom) != 0)) return false;
+    }
+    return true;
+}
+
 // Sweeps states [s0, s1) of one cone; true when target and candidate agree
 // on the compared outputs in every state.  Warp-collective.  When `stop`
 // becomes nonzero (another item of the same pair failed) the sweep ends
 // early; its result is then irrelevant.
 __device__ __forceinline__ bool sweep_states(const PairView& pv, const Fields& f, uint64_t om, uint64_t s0,
-                             uint64_t s1, const volatile uint32_t* stop, unsigned long long* nstates,
-                             int lane) {
-    const uint32_t ma = (uint32_t)om & 0xFFu, mx = (uint32_t)(om >> 8) & 0xFFu,
-                   my = (uint32_t)(om >> 16) & 0xFFu, mp = (uint32_t)(om >> 24) & 0xFFu,
-                   ms = (uint32_t)(om >> 32) & 0xFFu, mm = (uint32_t)(om >> 40) & 0xFFu,
-                   m0 = (uint32_t)(om >> 48) & 0xFFu, m1 = (uint32_t)(om >> 56) & 0xFFu;
+                                             uint64_t s1, const volatile uint32_t* stop, unsigned long long* nstates,
+                                             int lane) {
+    const OutMask m = out_mask(om);
     uint64_t iter = 0;
     for (uint64_t b = s0; b < s1; b += 32, iter++) {
         uint64_t s = b + (uint64_t)lane;
-        uint32_t d = 0;
-        if (s < s1) {
-            St in;
-            in.a = fld(f, 0, s); in.x = fld(f, 1, s); in.y = fld(f, 2, s); in.s = fld(f, 3, s);
-            in.m = fld(f, 4, s); in.s0 = fld(f, 5, s); in.s1 = fld(f, 6, s); in.p = fld(f, 7, s);
-            St t = in, c = in;
-            for (int i = 0; i < pv.tn; i++) exec(t, pv.t[i]);
-            for (int i = 0; i < pv.cn; i++) exec(c, pv.c[i]);
-            d = ((t.a ^ c.a) & ma) | ((t.x ^ c.x) & mx) | ((t.y ^ c.y) & my) | ((t.p ^ c.p) & mp) |
-                ((t.s ^ c.s) & ms) | ((t.m ^ c.m) & mm) | ((t.s0 ^ c.s0) & m0) | ((t.s1 ^ c.s1) & m1);
-        }
+        uint32_t d = s < s1 ? state_diff(pv, f, m, s) : 0u;
         if (__any_sync(kFull, d != 0)) {
             if (lane == 0) *nstates += (b - s0) + 32;
             return false;
@@ -455,7 +483,54 @@ __device__ __forceinline__ void append_surv(bool pass, Surv rec, Surv* out, uint
     }
 }
 
-// QC (+ MidCheck) of targets x all length-1 candidates.
+// Everything after a vector-0 match for one (target, candidate) pair: byte
+// filter, pruner, QC vectors 1-7, then MidCheck vectors 8-31 (CUDA pipeline)
+// or the Go worker's unmasked / masked split with FlagDiff.  Returns true
+// and the survivor code when the pair goes on to ExhaustiveCheck.
+template <bool GO>
+__device__ __forceinline__ bool qc_candidate(const uint64_t* __restrict__ trow, uint64_t t0, uint64_t c0, uint32_t tb,
+                                             uint32_t cm, uint32_t c, const uint64_t* __restrict__ cfp,
+                                             uint64_t loose, uint64_t exact, uint32_t dead, uint32_t stages,
+                                             unsigned long long& nqc, unsigned long long& nmid, uint32_t& code) {
+    const uint32_t cb = GO ? ((cm >> 2) & 3u) : (cm & 3u);
+    if ((cm & 0x90u) || cb >= tb) return false;   // pruned, padding, or not shorter
+    bool qc = true, ex = ((t0 ^ c0) & exact) == 0;
+    for (int v = 1; v < 8 && qc; v++) {
+        uint64_t x = trow[v] ^ cfp[(uint64_t)v * kNumInsns + c];
+        qc = (x & loose) == 0;
+        ex = ex && (x & exact) == 0;
+    }
+    if (!qc) return false;
+    if (!GO) {
+        nqc++;
+        bool mid = true;
+        if (stages & M6502_CHECK_MID)
+            for (int v = 8; v < 32 && mid; v++)
+                mid = ((trow[v] ^ cfp[(uint64_t)v * kNumInsns + c]) & loose) == 0;
+        if (!mid) return false;
+        nmid++;
+        code = c;
+        return true;
+    }
+    if (ex) {           // processTask: unmasked QC passes
+        nqc++; nmid++;
+        code = c;
+        return true;
+    }
+    if (dead) {         // processTaskMasked: masked QC passes, unmasked does not
+        uint32_t fd = 0;
+        for (int v = 0; v < 8; v++) fd |= (uint32_t)((trow[v] ^ cfp[(uint64_t)v * kNumInsns + c]) >> 24) & kPMask;
+        if (fd) {
+            nqc++; nmid++;
+            code = c | kSurvMasked | (fd_pack(fd) << 25);
+            return true;
+        }
+    }
+    return false;
+}
+
+// QC (+ MidCheck) of targets x all length-1 candidates, scanning: every
+// pair gets one masked 64-bit compare of its vector-0 outputs.
 constexpr int kQcTile = 64;
 constexpr int kQcPerThread = 12;   // 256 x 12 = 3072 >= 2863 candidates
 
@@ -502,39 +577,74 @@ __global__ void __launch_bounds__(256) k_qc1(const uint64_t* __restrict__ tfp, c
                 bool pass = false;
                 uint32_t code = 0;
                 const uint32_t c = threadIdx.x + 256u * (uint32_t)j;
-                if (hm & (1u << j)) {
-                    const uint32_t cb = GO ? ((cm[j] >> 2) & 3u) : (cm[j] & 3u);
-                    if (!(cm[j] & 0x90u) && cb < tb) {   // not pruned, not padding, shorter
-                        bool qc = true, ex = ((t0 ^ c0[j]) & exact) == 0;
-                        for (int v = 1; v < 8 && qc; v++) {
-                            uint64_t x = trow[v] ^ cfp[(uint64_t)v * kNumInsns + c];
-                            qc = (x & loose) == 0;
-                            ex = ex && (x & exact) == 0;
-                        }
-                        if (qc) {
-                            if (!GO) {
-                                nqc++;
-                                bool mid = true;
-                                if (stages & M6502_CHECK_MID)
-                                    for (int v = 8; v < 32 && mid; v++)
-                                        mid = ((trow[v] ^ cfp[(uint64_t)v * kNumInsns + c]) & loose) == 0;
-                                if (mid) { nmid++; pass = true; code = c; }
-                            } else if (ex) {           // processTask: unmasked QC passes
-                                nqc++; nmid++; pass = true; code = c;
-                            } else if (dead) {         // processTaskMasked
-                                uint32_t fd = 0;
-                                for (int v = 0; v < 8; v++)
-                                    fd |= (uint32_t)((trow[v] ^ cfp[(uint64_t)v * kNumInsns + c]) >> 24) & kPMask;
-                                if (fd) { nqc++; nmid++; pass = true; code = c | kSurvMasked | (fd_pack(fd) << 25); }
-                            }
-                        }
-                    }
-                }
+                if (hm & (1u << j))
+                    pass = qc_candidate<GO>(trow, t0, c0[j], tb, cm[j], c, cfp, loose, exact, dead, stages,
+                                            nqc, nmid, code);
                 append_surv(pass, Surv{t, code}, surv, cap, &cnt->surv, lane);
             }
         }
     }
     // one atomic per warp for the stage counters
+    for (int o = 16; o; o >>= 1) {
+        nqc += __shfl_down_sync(kFull, nqc, o);
+        nmid += __shfl_down_sync(kFull, nmid, o);
+    }
+    if (lane == 0) {
+        if (nqc) atomicAdd(&cnt->qc, nqc);
+        if (nmid) atomicAdd(&cnt->mid, nmid);
+    }
+}
+
+// QC (+ MidCheck) of targets x all length-1 candidates as an exact join:
+// the non-pruned candidates sorted by masked vector-0 output (skeys/sidx,
+// built per dead-flags mask) sit in shared memory; a warp takes one target,
+// binary-searches its masked vector-0 output, and checks only the
+// candidates with an equal key -- the only ones a QuickCheck can pass, since
+// vector 0 is one of its 8 vectors.  Same survivors as k_qc1.
+template <bool GO>
+__global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tfp, const uint8_t* __restrict__ tmeta,
+                                                  uint32_t nt, const uint64_t* __restrict__ cfp,
+                                                  const uint8_t* __restrict__ cmeta, const uint64_t* __restrict__ skeys,
+                                                  const uint16_t* __restrict__ sidx, uint32_t nsorted, uint32_t dead,
+                                                  uint32_t stages, Surv* __restrict__ surv, uint64_t cap,
+                                                  Counters* __restrict__ cnt) {
+    __shared__ uint64_t s_key[kNumInsns];
+    __shared__ uint16_t s_idx[kNumInsns];
+    __shared__ uint8_t s_meta[kNumInsns];
+    for (uint32_t i = threadIdx.x; i < nsorted; i += blockDim.x) {
+        s_key[i] = skeys[i];
+        s_idx[i] = sidx[i];
+    }
+    for (uint32_t i = threadIdx.x; i < (uint32_t)kNumInsns; i += blockDim.x) s_meta[i] = cmeta[i];
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint64_t loose = cmp_mask(dead), exact = cmp_mask(0);
+    unsigned long long nqc = 0, nmid = 0;
+    for (uint32_t t = blockIdx.x * kWarpsPerBlock + w; t < nt; t += gridDim.x * kWarpsPerBlock) {
+        const uint64_t* trow = tfp + (uint64_t)t * 32;
+        const uint64_t t0 = trow[0];
+        const uint64_t key = t0 & loose;
+        uint32_t lo = 0, hi = nsorted;            // lower bound of key
+        while (lo < hi) {
+            uint32_t mid = (lo + hi) >> 1;
+            if (s_key[mid] < key) lo = mid + 1; else hi = mid;
+        }
+        uint32_t end = lo;
+        while (end < nsorted && s_key[end] == key) end++;
+        if (lo == end) continue;
+        const uint32_t tb = GO ? (tmeta[t] >> 4) : (tmeta[t] & 15u);
+        for (uint32_t base = lo; base < end; base += 32) {
+            const uint32_t i = base + (uint32_t)lane;
+            bool pass = false;
+            uint32_t code = 0;
+            if (i < end) {
+                const uint32_t c = s_idx[i];
+                pass = qc_candidate<GO>(trow, t0, cfp[c], tb, s_meta[c], c, cfp, loose, exact, dead, stages,
+                                        nqc, nmid, code);
+            }
+            append_surv(pass, Surv{t, code}, surv, cap, &cnt->surv, lane);
+        }
+    }
     for (int o = 16; o; o >>= 1) {
         nqc += __shfl_down_sync(kFull, nqc, o);
         nmid += __shfl_down_sync(kFull, nmid, o);
@@ -552,7 +662,7 @@ __global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long
     __shared__ uint16_t s_t[kWarpsPerBlock][kMaxSeq], s_c[kWarpsPerBlock][kMaxSeq];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t n = min((uint64_t)*n_pairs_ptr, n_cap);
-    unsigned long long nstates = 0;
+    unsigned long long nstates = 0, probe_rej = 0;
     for (;;) {
         unsigned long long p = 0;
         if (lane == 0) p = atomicAdd(&a.cnt->exh_ticket, 1ull);
@@ -562,6 +672,17 @@ __global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long
         pv.t = s_t[w]; pv.c = s_c[w];
         src.load(p, s_t[w], s_c[w], pv.tn, pv.cn, pv.dead, lane);
         __syncwarp();
+        {
+            uint32_t sw = 0;
+            for (int i = 0; i < pv.tn; i++) sw |= c_sweep[pv.t[i] & 0xFFu];
+            for (int i = 0; i < pv.cn; i++) sw |= c_sweep[pv.c[i] & 0xFFu];
+            const bool prep = a.sweep == M6502_SWEEP_REFERENCE && __popc(sw) >= 3;
+            if (!probe_domain(pv, sw | LB(L_A) | LB(L_C), prep, pv.dead, p, lane)) {
+                if (lane == 0) { a.fail[p] = 1u; probe_rej++; }
+                __syncwarp();
+                continue;
+            }
+        }
         Flow fl = dataflow(pv, lane);
         const bool rep = a.sweep == M6502_SWEEP_REFERENCE && fl.k >= 3;
         Groups g = make_groups(fl, pv.dead, rep, a.brute != 0, lane);
@@ -597,6 +718,7 @@ __global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long
         __syncwarp();
     }
     if (lane == 0 && nstates) atomicAdd(&a.cnt->states, nstates);
+    if (lane == 0 && probe_rej) atomicAdd(&a.cnt->probe_rejects, probe_rej);
 }
 
 template <class Src>
@@ -921,6 +1043,10 @@ struct m6502_ctx {
     DevBuf cfp1, cmeta1, targets, ids, tfp, tmeta, surv, fail, items, rules, cnt, best, pins, poffs,
         cins, coffs, pout, pfd, enum_count;
     std::vector<m6502_rule> staging;
+    std::vector<uint64_t> h_cfp0;     // vector-0 outputs of the length-1 candidates (host copy)
+    std::vector<uint8_t> h_cmeta;
+    DevBuf join_keys[256], join_idx[256];
+    uint32_t join_n[256] = {};
 };
 
 namespace {
@@ -1018,11 +1144,33 @@ int init_ctx(m6502_ctx* ctx) {
         uint16_t one = tab[c];
         meta[c] = (uint8_t)(bytes_cuda(op) | (bytes_go(op) << 2) | (should_prune(&one, 1) ? 0x10 : 0));
     }
+    ctx->h_cfp0.assign(tr.begin(), tr.begin() + kNumInsns);
+    ctx->h_cmeta = meta;
     CK(cudaMemcpyAsync(ctx->cfp1.p, tr.data(), tr.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->cmeta1.p, meta.data(), meta.size(), cudaMemcpyHostToDevice, ctx->stream));
     TRY(ensure(ctx, ctx->cnt, sizeof(Counters)));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->ready = true;
+    return M6502_OK;
+}
+
+// Sorted (masked vector-0 output, candidate) table of the non-pruned
+// length-1 candidates for one dead-flags mask, built once per mask.
+int join_table(m6502_ctx* ctx, uint32_t dead) {
+    if (ctx->join_n[dead]) return M6502_OK;
+    const uint64_t loose = cmp_mask(dead);
+    std::vector<std::pair<uint64_t, uint16_t>> v;
+    for (int c = 0; c < kNumInsns; c++)
+        if (!(ctx->h_cmeta[c] & 0x10)) v.emplace_back(ctx->h_cfp0[c] & loose, (uint16_t)c);
+    std::sort(v.begin(), v.end());
+    std::vector<uint64_t> keys(v.size());
+    std::vector<uint16_t> idx(v.size());
+    for (size_t i = 0; i < v.size(); i++) { keys[i] = v[i].first; idx[i] = v[i].second; }
+    TRY(ensure(ctx, ctx->join_keys[dead], keys.size() * 8));
+    TRY(ensure(ctx, ctx->join_idx[dead], idx.size() * 2));
+    CK(cudaMemcpy(ctx->join_keys[dead].p, keys.data(), keys.size() * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(ctx->join_idx[dead].p, idx.data(), idx.size() * 2, cudaMemcpyHostToDevice));
+    ctx->join_n[dead] = (uint32_t)v.size();
     return M6502_OK;
 }
 
@@ -1055,8 +1203,24 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             FixedSeqs{d_targets, tlen}, nt, (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p);
         CKL("k_fingerprint(targets)");
         CK(cudaEventRecord(ctx->sev[1], ctx->stream));
+        const bool scan = (cfg.flags & M6502_QC_SCAN) != 0;
         uint32_t qgrid = (uint32_t)std::min<uint64_t>(ctx->qc_blocks, (nt + kQcTile - 1) / kQcTile);
-        if (go)
+        if (!scan) {
+            TRY(join_table(ctx, dead));
+            uint32_t jgrid = (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8, (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
+            const uint64_t* jk = (const uint64_t*)ctx->join_keys[dead].p;
+            const uint16_t* ji = (const uint16_t*)ctx->join_idx[dead].p;
+            if (go)
+                k_qc_join<true><<<jgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
+                                                                (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
+                                                                (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
+                                                                dead, stages, (Surv*)ctx->surv.p, scap, cnt);
+            else
+                k_qc_join<false><<<jgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
+                                                                 (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
+                                                                 (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
+                                                                 dead, stages, (Surv*)ctx->surv.p, scap, cnt);
+        } else if (go)
             k_qc1<true><<<qgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
                                                         (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
                                                         (uint8_t*)ctx->cmeta1.p, dead, stages,
@@ -1127,6 +1291,7 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             st->exh_states += hc.states;
             st->exh_items += hc.items;
             st->exh_algo_ops += hc.algo;
+            st->exh_probe_rejects += hc.probe_rejects;
             float ms[5];
             for (int i = 0; i < 5; i++) cudaEventElapsedTime(&ms[i], ctx->sev[i], ctx->sev[i + 1]);
             st->ms_fingerprint += ms[0];
@@ -1211,6 +1376,10 @@ void m6502_destroy(m6502_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (int i = 0; i < 256; i++) {
+        if (ctx->join_keys[i].p) cudaFree(ctx->join_keys[i].p);
+        if (ctx->join_idx[i].p) cudaFree(ctx->join_idx[i].p);
+    }
     DevBuf* bufs[] = {&ctx->cfp1, &ctx->cmeta1, &ctx->targets, &ctx->ids, &ctx->tfp, &ctx->tmeta,
                       &ctx->surv, &ctx->fail, &ctx->items, &ctx->rules, &ctx->cnt, &ctx->best,
                       &ctx->pins, &ctx->poffs, &ctx->cins, &ctx->coffs, &ctx->pout, &ctx->pfd,

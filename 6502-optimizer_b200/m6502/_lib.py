@@ -27,6 +27,7 @@ SWEEP_REFERENCE, SWEEP_FULL = 0, 1
 EXH_CONES, EXH_BRUTE = 0, 1
 CHECK_QC, CHECK_MID, CHECK_EXH, CHECK_ALL = 1, 2, 4, 7
 TARGETS_ON_DEVICE = 1
+QC_SCAN = 2
 
 
 class M6502Error(RuntimeError):
@@ -60,7 +61,7 @@ class SearchCfg(ctypes.Structure):
 class Stats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in
                 ("targets", "pairs", "qc_hits", "mid_hits", "exh_checked", "exh_passed",
-                 "rules", "exh_states", "exh_items", "exh_algo_ops", "passes")] + \
+                 "rules", "exh_states", "exh_items", "exh_algo_ops", "passes", "exh_probe_rejects")] + \
                [(n, ctypes.c_double) for n in ("ms_device", "ms_fingerprint", "ms_qc", "ms_exhaustive",
                                                "ms_exh_items", "ms_emit")]
 

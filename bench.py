@@ -265,7 +265,7 @@ def run_engine(args):
             "len2_wall_s": total_ms / args.steps / 1000.0,
             "rules": total_rules,
             "stage_counts": {k: s0[k] for k in ("qc_hits", "mid_hits", "exh_checked", "exh_passed", "rules",
-                                                  "exh_states", "exh_items")},
+                                                  "exh_states", "exh_items", "exh_probe_rejects")},
             "stages_ms": stages,
             "roofline": {"bound": "int-issue", "kernel": dominant, "achieved": achieved / 1e12,
                          "peak": peak_lane_ops / 1e12, "unit": "Tlane-op/s",

@@ -70,7 +70,9 @@ enum {
 
 /* m6502_search_cfg.flags */
 enum {
-    M6502_TARGETS_ON_DEVICE = 1 /* `targets` is a device pointer (already in HBM) */
+    M6502_TARGETS_ON_DEVICE = 1, /* `targets` is a device pointer (already in HBM) */
+    M6502_QC_SCAN = 2            /* QuickCheck by scanning every pair instead of the
+                                    exact join on vector-0 outputs (same survivors) */
 };
 
 typedef struct m6502_ctx m6502_ctx;
@@ -117,6 +119,8 @@ typedef struct m6502_stats {
     uint64_t exh_algo_ops; /* algorithmic ops of the accepted pairs: product-sweep
                               states x (10 per executed instruction + 3) */
     uint64_t passes;      /* device passes (blocks of targets) */
+    uint64_t exh_probe_rejects; /* pairs a random-state probe of the sweep domain
+                              rejected before the cone analysis */
     double ms_device;     /* device time of the whole call, CUDA events */
     double ms_fingerprint, ms_qc, ms_exhaustive, ms_exh_items, ms_emit; /* per-stage
                               device time summed over passes, CUDA events */

@@ -133,6 +133,22 @@ def test_config1_go_semantics(engine, dead, n):
     assert got == sorted(want)
 
 
+@pytest.mark.parametrize("semantics", [_lib.SEM_CUDA, _lib.SEM_GO])
+def test_qc_join_equals_scan(engine, semantics):
+    """The exact join on vector-0 outputs and the full scan of every pair give
+    the same stage counts and rule sets (length-2 and length-3 targets)."""
+    for targets in (oracle.draw_targets(0, 2, 2000), oracle.draw_targets(1, 3, 300)):
+        for dead in (0x00, 0x01, 0xC3, 0xFF):
+            a, sa = engine.search(targets, dead_flags=dead, semantics=semantics, sweep=_lib.SWEEP_REFERENCE)
+            b, sb = engine.search(targets, dead_flags=dead, semantics=semantics, sweep=_lib.SWEEP_REFERENCE,
+                                  qc_scan=True)
+            key = lambda rs: sorted((int(r["target"]), tuple(int(x) for x in r["cand"]), int(r["dead_flags"]))  # noqa: E731
+                                    for r in rs)
+            assert key(a) == key(b)
+            for k in ("qc_hits", "mid_hits", "exh_checked", "exh_passed"):
+                assert sa[k] == sb[k], (k, dead)
+
+
 def test_search_random_length3_targets(engine):
     """Length-3 targets (CUDA semantics, reference sweep) against the oracle."""
     targets = oracle.draw_targets(1, 3, 48)
