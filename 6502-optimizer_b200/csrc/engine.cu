@@ -43,6 +43,11 @@ constexpr int kWarpsPerBlock = 8;    // 256-thread CTAs
 constexpr uint64_t kSmallSweep = 1ull << 17;  // sweep in-warp up to this many states
 constexpr uint64_t kProbe = 1ull << 12;       // in-warp probe of a large cone
 constexpr uint64_t kChunk = 1ull << 16;       // states per work item
+// Largest cone a pair may need swept (2^34 states, about 0.1 s of the whole
+// GPU).  Pairs of long sequences that read many registers can need far
+// more; they get the verdict "undecided" instead of an endless sweep.
+constexpr uint32_t kMaxConeBits = 34;
+constexpr unsigned kTicketBatch = 16;          // pairs a warp takes per ticket atomic
 
 // Test vectors: TestVectors + MidCheckVectors of pkg/search/verifier.go:18-67
 // (A, X, Y, P, S, M, S0, S1).  Vectors 0..7 are QuickCheck's.
@@ -468,19 +473,29 @@ __global__ void __launch_bounds__(256) k_fingerprint(Src src, uint64_t n, uint64
     }
 }
 
-// Warp-aggregated append of one record per passing lane (all 32 lanes call).
-__device__ __forceinline__ void append_surv(bool pass, Surv rec, Surv* out, uint64_t cap,
+// Survivor appends staged per warp in shared memory: one global atomic per
+// flush of up to kStage records instead of one per warp-iteration with a hit
+// (a single hot counter otherwise serialises millions of appends).
+constexpr int kStage = 64;
+__device__ __forceinline__ void stage_flush(Surv* buf, int& n, Surv* out, uint64_t cap,
                                             unsigned long long* counter, int lane) {
+    if (n == 0) return;
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(counter, (unsigned long long)n);
+    base = __shfl_sync(kFull, base, 0);
+    for (int i = lane; i < n; i += 32)
+        if (base + (unsigned long long)i < cap) out[base + i] = buf[i];
+    __syncwarp();
+    n = 0;
+}
+__device__ __forceinline__ void stage_push(bool pass, Surv rec, Surv* buf, int& n, Surv* out, uint64_t cap,
+                                           unsigned long long* counter, int lane) {
     unsigned vote = __ballot_sync(kFull, pass);
     if (!vote) return;
-    int leader = __ffs(vote) - 1;
-    unsigned long long base = 0;
-    if (lane == leader) base = atomicAdd(counter, (unsigned long long)__popc(vote));
-    base = __shfl_sync(kFull, base, leader);
-    if (pass) {
-        unsigned long long idx = base + (unsigned long long)__popc(vote & ((1u << lane) - 1u));
-        if (idx < cap) out[idx] = rec;
-    }
+    if (pass) buf[n + __popc(vote & ((1u << lane) - 1u))] = rec;
+    __syncwarp();
+    n += __popc(vote);
+    if (n > kStage - 32) stage_flush(buf, n, out, cap, counter, lane);
 }
 
 // Everything after a vector-0 match for one (target, candidate) pair: byte
@@ -542,7 +557,10 @@ __global__ void __launch_bounds__(256) k_qc1(const uint64_t* __restrict__ tfp, c
                                               Counters* __restrict__ cnt) {
     __shared__ uint64_t s_t0[kQcTile];
     __shared__ uint8_t s_tb[kQcTile];
+    __shared__ Surv s_stage[kWarpsPerBlock][kStage];
     const int lane = threadIdx.x & 31;
+    Surv* stage = s_stage[threadIdx.x >> 5];
+    int nstage = 0;
     const uint64_t loose = cmp_mask(dead), exact = cmp_mask(0);
     uint64_t c0[kQcPerThread];
     uint32_t cm[kQcPerThread];
@@ -580,10 +598,11 @@ __global__ void __launch_bounds__(256) k_qc1(const uint64_t* __restrict__ tfp, c
                 if (hm & (1u << j))
                     pass = qc_candidate<GO>(trow, t0, c0[j], tb, cm[j], c, cfp, loose, exact, dead, stages,
                                             nqc, nmid, code);
-                append_surv(pass, Surv{t, code}, surv, cap, &cnt->surv, lane);
+                stage_push(pass, Surv{t, code}, stage, nstage, surv, cap, &cnt->surv, lane);
             }
         }
     }
+    stage_flush(stage, nstage, surv, cap, &cnt->surv, lane);
     // one atomic per warp for the stage counters
     for (int o = 16; o; o >>= 1) {
         nqc += __shfl_down_sync(kFull, nqc, o);
@@ -611,6 +630,9 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tf
     __shared__ uint64_t s_key[kNumInsns];
     __shared__ uint16_t s_idx[kNumInsns];
     __shared__ uint8_t s_meta[kNumInsns];
+    __shared__ Surv s_stage[kWarpsPerBlock][kStage];
+    Surv* stage = s_stage[threadIdx.x >> 5];
+    int nstage = 0;
     for (uint32_t i = threadIdx.x; i < nsorted; i += blockDim.x) {
         s_key[i] = skeys[i];
         s_idx[i] = sidx[i];
@@ -642,9 +664,10 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tf
                 pass = qc_candidate<GO>(trow, t0, cfp[c], tb, s_meta[c], c, cfp, loose, exact, dead, stages,
                                         nqc, nmid, code);
             }
-            append_surv(pass, Surv{t, code}, surv, cap, &cnt->surv, lane);
+            stage_push(pass, Surv{t, code}, stage, nstage, surv, cap, &cnt->surv, lane);
         }
     }
+    stage_flush(stage, nstage, surv, cap, &cnt->surv, lane);
     for (int o = 16; o; o >>= 1) {
         nqc += __shfl_down_sync(kFull, nqc, o);
         nmid += __shfl_down_sync(kFull, nmid, o);
@@ -663,10 +686,15 @@ __global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t n = min((uint64_t)*n_pairs_ptr, n_cap);
     unsigned long long nstates = 0, probe_rej = 0;
+    unsigned long long next = 0, lim = 0;   // this warp's batch of tickets
     for (;;) {
-        unsigned long long p = 0;
-        if (lane == 0) p = atomicAdd(&a.cnt->exh_ticket, 1ull);
-        p = __shfl_sync(kFull, p, 0);
+        if (next >= lim) {
+            unsigned long long b = 0;
+            if (lane == 0) b = atomicAdd(&a.cnt->exh_ticket, (unsigned long long)kTicketBatch);
+            next = __shfl_sync(kFull, b, 0);
+            lim = next + kTicketBatch;
+        }
+        const unsigned long long p = next++;
         if (p >= n) break;
         PairView pv;
         pv.t = s_t[w]; pv.c = s_c[w];
@@ -686,6 +714,13 @@ __global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long
         Flow fl = dataflow(pv, lane);
         const bool rep = a.sweep == M6502_SWEEP_REFERENCE && fl.k >= 3;
         Groups g = make_groups(fl, pv.dead, rep, a.brute != 0, lane);
+        bool too_big = false;
+        for (int i = 0; i < g.n; i++) too_big = too_big || g.bits[i] > kMaxConeBits;
+        if (too_big) {
+            if (lane == 0) a.fail[p] = 3u;   // undecided: sweep beyond the cap
+            __syncwarp();
+            continue;
+        }
         bool ok = true;
         uint32_t big = 0;   // groups left for the work queue
         for (int i = 0; i < g.n && ok; i++) {
@@ -946,6 +981,7 @@ __global__ void k_enum_targets(uint64_t id0, uint64_t id1, uint32_t len, uint16_
 // calls that overlap on the GPU race; each call clears the part that must
 // start at zero.
 constexpr uint64_t kStaticMaxPairs = M6502_STATIC_MAX_PAIRS;
+constexpr uint32_t kStaticMaxConeBits = 28;   // in-warp sweeps only: at most 2^28 states per cone
 
 struct StaticScratch {
     Counters cnt;
@@ -979,7 +1015,7 @@ struct StaticCsrSource {
 
 // One pair per warp, every cone swept in-warp (no work-item queue, so the
 // only scratch is the ticket and the fail flags).  fail: 0 equivalent,
-// 1 not equivalent, 2 invalid pair.
+// 1 not equivalent, 2 invalid pair, 3 undecided (a cone beyond 2^28 states).
 __global__ void __launch_bounds__(256) k_exhaustive_static(StaticCsrSource src, uint64_t n, uint32_t sweep,
                                                             StaticScratch* scr) {
     __shared__ uint16_t s_t[kWarpsPerBlock][kMaxSeq], s_c[kWarpsPerBlock][kMaxSeq];
@@ -1002,6 +1038,13 @@ __global__ void __launch_bounds__(256) k_exhaustive_static(StaticCsrSource src, 
         Flow fl = dataflow(pv, lane);
         const bool rep = sweep == M6502_SWEEP_REFERENCE && fl.k >= 3;
         Groups g = make_groups(fl, pv.dead, rep, false, lane);
+        bool too_big = false;
+        for (int i = 0; i < g.n; i++) too_big = too_big || g.bits[i] > kStaticMaxConeBits;
+        if (too_big) {
+            if (lane == 0) scr->fail[p] = 3u;   // undecided: one warp cannot sweep it in bounded time
+            __syncwarp();
+            continue;
+        }
         bool ok = true;
         for (int i = 0; i < g.n && ok; i++) {
             Fields f = make_fields(g.cone[i], fl.swept, rep);
@@ -1015,7 +1058,7 @@ __global__ void __launch_bounds__(256) k_exhaustive_static(StaticCsrSource src, 
 __global__ void k_static_verdicts(const StaticScratch* scr, uint64_t n, uint8_t* __restrict__ out) {
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t f = scr->fail[i];
-        out[i] = f == 0 ? 1 : (f == 1 ? 0 : 0xFF);
+        out[i] = f == 0 ? 1 : (f == 1 ? 0 : (f == 3 ? 0xFE : 0xFF));
     }
 }
 
@@ -1461,6 +1504,7 @@ int m6502_check_pairs(m6502_ctx* ctx, uint64_t n, const uint16_t* t_insns, const
     for (uint64_t i = 0; i < n; i++) {
         uint8_t r = out[i] & (uint8_t)(checks & 3u);
         if ((checks & M6502_CHECK_EXH) && f32[i] == 0) r |= 4;
+        if ((checks & M6502_CHECK_EXH) && f32[i] == 3) r |= 8;
         out[i] = r;
     }
     return M6502_OK;

@@ -140,7 +140,9 @@ void *m6502_stream(m6502_ctx *ctx); /* the context's cudaStream_t */
  * insns + offsets (CSR: sequence i is insns[offs[i] .. offs[i+1])), each
  * 1..16 instructions.  out[i] bit 0 = QC, bit 1 = MidCheck, bit 2 =
  * ExhaustiveCheck, for the bits requested in `checks` (each check is
- * evaluated on its own, as the Go functions are).  flagdiff (optional) gets
+ * evaluated on its own, as the Go functions are).  Bit 3 marks a pair whose
+ * exhaustive sweep would exceed 2^34 states in one output cone (only long
+ * sequences reading many registers): it is left undecided, bit 2 clear.  flagdiff (optional) gets
  * FlagDiff(target, candidate). */
 int m6502_check_pairs(m6502_ctx *ctx, uint64_t n,
                       const uint16_t *t_insns, const uint32_t *t_offs,
@@ -174,7 +176,8 @@ int m6502_exec_batch(m6502_ctx *ctx, uint64_t n, const uint16_t *insns, const ui
  * All pointers are caller-owned DEVICE memory on the current device: pairs
  * as CSR (t_insns/t_offs, c_insns/c_offs, n + 1 offsets each, 1..16
  * instructions per sequence).  out[i] = 1 equivalent, 0 not equivalent, 0xFF
- * invalid pair (length or opcode out of range).  Runs asynchronously on
+ * invalid pair (length or opcode out of range), 0xFE undecided (an output
+ * cone beyond 2^28 states, which one warp cannot sweep in bounded time).  Runs asynchronously on
  * `stream` (a cudaStream_t; NULL = the legacy default stream); read `out`
  * after synchronising it.  Returns M6502_E_TOOBIG for n >
  * M6502_STATIC_MAX_PAIRS.  The first call on a device uploads the instruction
