@@ -8,6 +8,8 @@
 //                     [--gpu-id N] [--checkpoint FILE] [--workers N]
 //   6502opt target "LDA #$00 : TAX" [--max-candidate N] [--dead-flags M] [-v]
 //   6502opt verify-jsonl FILE [--dead-flags M] [-v] [--sweep full|reference]
+//   6502opt stoke --target "PHA : TXA : PLA" [--chains N] [--iterations I] [--decay D]
+//                 [--output FILE] [-v] [--dead-flags M] [--cost ref|hamming] [--seed S]
 //
 // All checking runs on the GPU through the C ABI; there is no CPU path.
 #include <algorithm>
@@ -384,12 +386,87 @@ int cmd_verify(const Args& a) {
     return 0;
 }
 
+// stoke (cmd/6502opt/main.go:204-276): batched chains on the GPU, unique
+// proven rewrites printed as stoke.Deduplicate (pkg/stoke/search.go:179-190)
+// leaves them.
+int cmd_stoke(const Args& a) {
+    std::string target = a.get("--target", "");
+    if (target.empty()) { std::fprintf(stderr, "--target is required\n"); return 1; }
+    uint16_t seq[16];
+    int n = m6502_parse(target.c_str(), seq, 16);
+    if (n < 0 || n > 14) { std::fprintf(stderr, "failed to parse target: %s\n", target.c_str()); return 1; }
+    uint8_t dead = 0;
+    if (!parse_dead(a.get("--dead-flags", "none"), &dead)) { std::fprintf(stderr, "invalid --dead-flags\n"); return 1; }
+    m6502_stoke_cfg cfg{};
+    cfg.chains_per_target = (uint32_t)a.num("--chains", 128);
+    cfg.steps = (uint64_t)a.num("--iterations", 10000000);
+    cfg.steps_per_epoch = (uint32_t)a.num("--steps-per-epoch", 1000);
+    cfg.decay = std::strtod(a.get("--decay", "0.9999").c_str(), nullptr);
+    cfg.seed = (uint64_t)a.num("--seed", (long)std::chrono::steady_clock::now().time_since_epoch().count());
+    cfg.cost = a.get("--cost", "ref") == "hamming" ? M6502_COST_HAMMING : M6502_COST_REF;
+    cfg.sweep = a.get("--sweep", "reference") == "full" ? M6502_SWEEP_FULL : M6502_SWEEP_REFERENCE;
+    cfg.dead_flags = dead;
+    bool verbose = a.has("-v") || a.has("--verbose");
+    uint32_t offs[2] = {0, (uint32_t)n};
+    if (verbose)
+        std::printf("STOKE search: %u chains x %llu iterations (decay=%.6f)\nTarget: %s (%d bytes, %d cycles)\n\n",
+                    cfg.chains_per_target, (unsigned long long)cfg.steps, cfg.decay, disasm_seq(seq, n).c_str(),
+                    m6502_seq_bytes(seq, n, M6502_SEM_GO), m6502_seq_cycles(seq, n));
+    m6502_ctx* ctx = open_ctx((int)a.num("--gpu-id", 0));
+    m6502_stoke_result res;
+    std::vector<m6502_stoke_proof> proofs(1u << 16);
+    uint64_t np = 0;
+    m6502_stoke_stats st{};
+    int rc;
+    while ((rc = m6502_stoke_run(ctx, &cfg, seq, offs, 1, &res, proofs.data(), proofs.size(), &np, &st)) ==
+           M6502_E_OVERFLOW)
+        proofs.resize(np);
+    if (rc != M6502_OK) die(ctx, rc, "m6502_stoke_run");
+    // Deduplicate by replacement, keeping the first occurrence.
+    std::vector<OutRule> uniq;
+    std::vector<std::vector<uint16_t>> seen;
+    for (uint64_t i = 0; i < np; i++) {
+        std::vector<uint16_t> r(proofs[i].cand, proofs[i].cand + proofs[i].cand_len);
+        if (std::find(seen.begin(), seen.end(), r) != seen.end()) continue;
+        seen.push_back(r);
+        if (verbose)
+            std::printf("  Chain %u @ iter %llu: %s VERIFIED\n", proofs[i].chain, (unsigned long long)proofs[i].step,
+                        disasm_seq(r.data(), (int)r.size()).c_str());
+        uniq.push_back(OutRule{std::vector<uint16_t>(seq, seq + n), r,
+                               m6502_seq_bytes(seq, n, M6502_SEM_GO) - m6502_seq_bytes(r.data(), (int)r.size(), M6502_SEM_GO),
+                               m6502_seq_cycles(seq, n) - m6502_seq_cycles(r.data(), (int)r.size()), proofs[i].dead_flags});
+    }
+    if (verbose)
+        std::printf("\nSTOKE complete: %llu verified results in %.0f ms\n", (unsigned long long)np, st.ms_device);
+    std::printf("\n%zu unique optimizations found\n", uniq.size());
+    for (size_t i = 0; i < uniq.size(); i++) {
+        const OutRule& r = uniq[i];
+        if (r.dead)
+            std::printf("  %zu. %s (-%d bytes, -%d cycles, dead flags: %s)\n", i + 1,
+                        disasm_seq(r.rep.data(), (int)r.rep.size()).c_str(), r.bytes_saved, r.cycles_saved,
+                        dead_desc(r.dead).c_str());
+        else
+            std::printf("  %zu. %s (-%d bytes, -%d cycles)\n", i + 1, disasm_seq(r.rep.data(), (int)r.rep.size()).c_str(),
+                        r.bytes_saved, r.cycles_saved);
+    }
+    std::string output = a.get("--output", "");
+    if (!output.empty() && !uniq.empty()) {
+        std::ofstream os(output);
+        if (!os) { std::fprintf(stderr, "cannot write %s\n", output.c_str()); return 1; }
+        write_json(os, uniq);
+        std::printf("Written to %s\n", output.c_str());
+    }
+    m6502_destroy(ctx);
+    return 0;
+}
+
 void usage() {
     std::fprintf(stderr,
                  "6502opt -- 6502 superoptimizer on the B200 engine\n\n"
                  "  enumerate      enumerate all target sequences and find shorter replacements\n"
                  "  target         find the optimal replacement for one instruction sequence\n"
-                 "  verify-jsonl   verify JSONL rules with ExhaustiveCheck on the GPU\n");
+                 "  verify-jsonl   verify JSONL rules with ExhaustiveCheck on the GPU\n"
+                 "  stoke          STOKE stochastic search (batched MCMC chains on the GPU)\n");
 }
 
 }  // namespace
@@ -401,6 +478,7 @@ int main(int argc, char** argv) {
     if (cmd == "enumerate") return cmd_enumerate(a);
     if (cmd == "target") return cmd_target(a);
     if (cmd == "verify-jsonl") return cmd_verify(a);
+    if (cmd == "stoke") return cmd_stoke(a);
     usage();
     return 1;
 }

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -40,14 +41,14 @@ namespace {
 constexpr unsigned kFull = 0xFFFFFFFFu;
 constexpr int kMaxSeq = 16;          // longest sequence the pairwise API takes
 constexpr int kWarpsPerBlock = 8;    // 256-thread CTAs
-constexpr uint64_t kSmallSweep = 1ull << 17;  // sweep in-warp up to this many states
+constexpr uint64_t kSmallSweep = 1ull << 13;  // sweep in-warp up to this many states
 constexpr uint64_t kProbe = 1ull << 12;       // in-warp probe of a large cone
-constexpr uint64_t kChunk = 1ull << 16;       // states per work item
+constexpr uint64_t kChunk = 1ull << 15;       // states per work item
 // Largest cone a pair may need swept (2^34 states, about 0.1 s of the whole
 // GPU).  Pairs of long sequences that read many registers can need far
 // more; they get the verdict "undecided" instead of an endless sweep.
 constexpr uint32_t kMaxConeBits = 34;
-constexpr unsigned kTicketBatch = 16;          // pairs a warp takes per ticket atomic
+constexpr unsigned kTicketBatch = 4;           // pairs a warp takes per ticket atomic
 
 // Test vectors: TestVectors + MidCheckVectors of pkg/search/verifier.go:18-67
 // (A, X, Y, P, S, M, S0, S1).  Vectors 0..7 are QuickCheck's.
@@ -644,8 +645,8 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tf
     unsigned long long nqc = 0, nmid = 0;
     for (uint32_t t = blockIdx.x * kWarpsPerBlock + w; t < nt; t += gridDim.x * kWarpsPerBlock) {
         const uint64_t* trow = tfp + (uint64_t)t * 32;
-        const uint64_t t0 = trow[0];
-        const uint64_t key = t0 & loose;
+        const uint64_t tv = trow[lane];   // lane v holds the target's output on vector v
+        const uint64_t key = __shfl_sync(kFull, tv, 0) & loose;
         uint32_t lo = 0, hi = nsorted;            // lower bound of key
         while (lo < hi) {
             uint32_t mid = (lo + hi) >> 1;
@@ -655,16 +656,32 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tf
         while (end < nsorted && s_key[end] == key) end++;
         if (lo == end) continue;
         const uint32_t tb = GO ? (tmeta[t] >> 4) : (tmeta[t] & 15u);
-        for (uint32_t base = lo; base < end; base += 32) {
-            const uint32_t i = base + (uint32_t)lane;
+        for (uint32_t i = lo; i < end; i++) {
+            const uint32_t c = s_idx[i];
+            const uint32_t cm = s_meta[c];
+            const uint32_t cb = GO ? ((cm >> 2) & 3u) : (cm & 3u);
+            if ((cm & 0x10u) || cb >= tb) continue;          // pruned or not shorter (uniform)
+            const uint64_t x = tv ^ cfp[(uint64_t)lane * kNumInsns + c];
+            const unsigned lo_eq = __ballot_sync(kFull, (x & loose) == 0);
+            const unsigned ex_eq = __ballot_sync(kFull, (x & exact) == 0);
+            if ((lo_eq & 0xFFu) != 0xFFu) continue;          // QuickCheck fails
             bool pass = false;
-            uint32_t code = 0;
-            if (i < end) {
-                const uint32_t c = s_idx[i];
-                pass = qc_candidate<GO>(trow, t0, cfp[c], tb, s_meta[c], c, cfp, loose, exact, dead, stages,
-                                        nqc, nmid, code);
+            uint32_t code = c;
+            if (!GO) {
+                nqc += lane == 0;
+                const bool mid = !(stages & M6502_CHECK_MID) || lo_eq == kFull;
+                if (mid) { nmid += lane == 0; pass = true; }
+            } else if ((ex_eq & 0xFFu) == 0xFFu) {           // processTask: unmasked QC passes
+                nqc += lane == 0; nmid += lane == 0; pass = true;
+            } else if (dead) {                               // processTaskMasked, FlagDiff != 0
+                uint32_t fd = lane < 8 ? ((uint32_t)(x >> 24) & kPMask) : 0u;
+                fd = __reduce_or_sync(kFull, fd);
+                if (fd) {
+                    nqc += lane == 0; nmid += lane == 0; pass = true;
+                    code = c | kSurvMasked | (fd_pack(fd) << 25);
+                }
             }
-            stage_push(pass, Surv{t, code}, stage, nstage, surv, cap, &cnt->surv, lane);
+            stage_push(pass && lane == 0, Surv{t, code}, stage, nstage, surv, cap, &cnt->surv, lane);
         }
     }
     stage_flush(stage, nstage, surv, cap, &cnt->surv, lane);
@@ -1090,6 +1107,7 @@ struct m6502_ctx {
     std::vector<uint8_t> h_cmeta;
     DevBuf join_keys[256], join_idx[256];
     uint32_t join_n[256] = {};
+    DevBuf st_tins, st_toffs, st_tout, st_tbytes, st_chains, st_entries, st_vidx, st_proven, st_cnt, st_pidx;
 };
 
 namespace {
@@ -1426,7 +1444,9 @@ void m6502_destroy(m6502_ctx* ctx) {
     DevBuf* bufs[] = {&ctx->cfp1, &ctx->cmeta1, &ctx->targets, &ctx->ids, &ctx->tfp, &ctx->tmeta,
                       &ctx->surv, &ctx->fail, &ctx->items, &ctx->rules, &ctx->cnt, &ctx->best,
                       &ctx->pins, &ctx->poffs, &ctx->cins, &ctx->coffs, &ctx->pout, &ctx->pfd,
-                      &ctx->enum_count};
+                      &ctx->enum_count, &ctx->st_tins, &ctx->st_toffs, &ctx->st_tout, &ctx->st_tbytes,
+                      &ctx->st_chains, &ctx->st_entries, &ctx->st_vidx, &ctx->st_proven, &ctx->st_cnt,
+                      &ctx->st_pidx};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
@@ -1731,3 +1751,5 @@ int m6502_exhaustive_static(uint64_t n, const uint16_t* t_insns, const uint32_t*
 }
 
 }  // extern "C"
+
+#include "stoke.cuh"

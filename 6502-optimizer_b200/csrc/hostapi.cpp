@@ -163,6 +163,44 @@ uint64_t m6502_enumerate_targets(uint32_t tlen, uint32_t first, uint32_t last, u
     return n;
 }
 
+namespace {
+// splitmix64 (Steele, Lea & Flood 2014).
+uint64_t splitmix64(uint64_t* x) {
+    uint64_t z = (*x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+// Uniform index in [0, bound): rejection of the top partial block of 2^64.
+uint32_t uniform_index(uint64_t* x, uint32_t bound) {
+    uint64_t rem = (UINT64_MAX % bound + 1) % bound;
+    uint64_t lim = rem ? UINT64_MAX - rem + 1 : 0;
+    for (;;) {
+        uint64_t r = splitmix64(x);
+        if (lim == 0 || r < lim) return (uint32_t)(r % bound);
+    }
+}
+}  // namespace
+
+int m6502_draw_targets(uint64_t seed, uint32_t min_len, uint32_t max_len, uint64_t n, int reject_pruned,
+                       uint16_t* insns, uint32_t* offs) {
+    if (min_len < 1 || max_len < min_len || max_len > 16 || !insns || !offs) return M6502_E_INVAL;
+    uint16_t tab[kNumInsns];
+    m6502_insn_table(M6502_SEM_CUDA, tab);
+    uint64_t x = seed, k = 0;
+    offs[0] = 0;
+    for (uint64_t i = 0; i < n;) {
+        uint32_t len = min_len == max_len ? min_len : min_len + uniform_index(&x, max_len - min_len + 1);
+        uint16_t s[16];
+        for (uint32_t p = 0; p < len; p++) s[p] = tab[uniform_index(&x, kNumInsns)];
+        if (reject_pruned && should_prune(s, (int)len)) continue;
+        std::memcpy(insns + k, s, len * sizeof(uint16_t));
+        k += len;
+        offs[++i] = (uint32_t)k;
+    }
+    return M6502_OK;
+}
+
 int m6502_op_deps(int op, uint16_t deps[13]) {
     if (op < 0 || op >= (int)NUM_OPS || !deps) return M6502_E_INVAL;
     return (int)op_deps((uint32_t)op, deps);

@@ -1,0 +1,497 @@
+// stoke.cuh -- batched STOKE (stochastic superoptimisation) on B200.
+// Included at the end of engine.cu (one translation unit: it shares the
+// constant tables and the exhaustive kernels).
+//
+// The reference runs one goroutine per MCMC chain (pkg/stoke/search.go:88-163):
+// mutate (mutator.go:30-115), cost on the test vectors (cost.go:32-81),
+// Metropolis accept with T *= decay (mcmc.go:51-81), and ExhaustiveCheck of
+// every shorter zero-mismatch best (search.go:102-155).  Here one warp runs
+// one chain: all 32 lanes draw the same random numbers (one splitmix64 state
+// per chain, so the control flow is warp-uniform), lane v evaluates the
+// candidate on test vector v, and the cost is a warp reduction.  Chains run in
+// epochs of S steps; after each epoch the shorter zero-cost bests found during
+// it are checked on all 32 vectors and proved by the exhaustive kernels, and
+// the chains of proven targets restart (the reference's NewChain) or stop.
+
+namespace {
+
+struct StokeChain {
+    uint16_t cur[kMaxSeq];
+    uint16_t best[kMaxSeq];
+    uint64_t rng;
+    uint64_t step;          // steps this chain has run (all restarts)
+    uint64_t since;         // steps since the last (re)start
+    float temp;
+    int32_t cost, best_cost;
+    uint32_t target;
+    uint32_t accepted;
+    uint8_t len, best_len, status, pad;   // status: 0 (re)start, 1 running, 2 stopped
+};
+
+struct StokeEntry {        // a shorter zero-cost best awaiting proof
+    uint32_t chain, target;
+    uint64_t step;
+    uint16_t ins[kMaxSeq];
+    uint8_t len, dead_flags, pad[6];
+};
+
+struct StokeCounters {
+    unsigned long long entries, vec_ok, proofs, undecided, accepted;
+};
+
+struct StokeTargets {
+    const uint16_t* ins;
+    const uint32_t* off;
+    const uint64_t* out;    // [target][32] outputs on the test vectors (P & PMask)
+    const uint8_t* bytes;   // Go byte size of each target
+};
+
+struct StokeParams {
+    uint32_t cost_mode;     // M6502_COST_*
+    uint32_t dead;
+    uint32_t max_len;       // 0: max(len + 2, 10)
+    uint32_t chains_per_target;
+    uint32_t steps;         // steps of this epoch
+    uint64_t seed;
+    float decay;            // per-step temperature factor
+    float t_start;
+    const uint32_t* proven; // per target: 1 once proved (stop_on_proof)
+    uint32_t stop_on_proof;
+};
+
+__device__ __forceinline__ uint64_t sm_next(uint64_t& x) {
+    uint64_t z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+// Uniform integer in [0, n): high half of a 32x32 product (bias < n / 2^32).
+__device__ __forceinline__ uint32_t sm_below(uint64_t& x, uint32_t n) {
+    return (uint32_t)(((sm_next(x) >> 32) * (uint64_t)n) >> 32);
+}
+__device__ __forceinline__ float sm_unit(uint64_t& x) { return (float)(sm_next(x) >> 40) * (1.0f / 16777216.0f); }
+
+// randomInstruction (mutator.go:108-115): opcode uniform over the 58 opcodes,
+// immediate uniform over 0..255 when the opcode takes one.
+__device__ __forceinline__ uint16_t random_insn(uint64_t& rng) {
+    uint32_t op = sm_below(rng, NUM_OPS);
+    uint32_t imm = has_imm(op) ? sm_below(rng, 256) : 0u;
+    return (uint16_t)(op | (imm << 8));
+}
+
+// Cost of the sequence in seq[0..len) against the target outputs `tv` (this
+// lane's vector).  COST_REF: 1000 x mismatching QC vectors + bytes +
+// cycles / 100 (cost.go:32-81); COST_HAMMING: differing output bits over the
+// 32 vectors + bytes + cycles / 100.  `zero` is true when no vector differs.
+__device__ __forceinline__ int32_t stoke_cost(const uint16_t* seq, int len, uint64_t tv, uint64_t mask,
+                                              uint32_t mode, int lane, bool& zero) {
+    St s = unpack(c_vec[lane]);
+    for (int i = 0; i < len; i++) exec(s, seq[i]);
+    const uint64_t x = (fp_of(s) ^ tv) & mask;
+    uint32_t b = 0, c = 0;
+    if (lane < len) { b = bytes_go(seq[lane] & 0xFFu); c = cycles(seq[lane] & 0xFFu); }
+    b = __reduce_add_sync(kFull, b);
+    c = __reduce_add_sync(kFull, c);
+    int32_t base = (int32_t)(b + c / 100u);
+    if (mode == M6502_COST_REF) {
+        unsigned mism = __ballot_sync(kFull, x != 0) & 0xFFu;
+        zero = mism == 0;
+        return 1000 * __popc(mism) + base;
+    }
+    uint32_t h = __reduce_add_sync(kFull, (uint32_t)__popcll(x));
+    zero = h == 0;
+    return (int32_t)h + base;
+}
+
+// One epoch of every chain: warp per chain.
+__global__ void __launch_bounds__(256) k_stoke_epoch(StokeChain* __restrict__ chains, uint32_t n_chains,
+                                                      StokeTargets tg, StokeParams prm,
+                                                      StokeEntry* __restrict__ entries, uint64_t ecap,
+                                                      StokeCounters* __restrict__ sc) {
+    __shared__ uint16_t s_buf[kWarpsPerBlock][2][kMaxSeq];
+    __shared__ uint16_t s_best[kWarpsPerBlock][kMaxSeq];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t ci = blockIdx.x * kWarpsPerBlock + (uint32_t)w;
+    if (ci >= n_chains) return;
+    StokeChain& ch = chains[ci];
+    const uint32_t t = ci / prm.chains_per_target;
+    uint32_t status = ch.status;
+    if (prm.stop_on_proof && prm.proven[t]) status = 2;
+    if (status == 2) {
+        if (lane == 0) ch.status = 2;
+        return;
+    }
+    const uint32_t t0 = tg.off[t], tlen = tg.off[t + 1] - t0;
+    const uint64_t tv = tg.out[(uint64_t)t * 32 + lane];
+    const uint32_t tbytes = tg.bytes[t];
+    const uint64_t mask = cmp_mask(prm.dead);
+    const int max_len = (int)(prm.max_len ? prm.max_len : max(tlen + 2u, 10u));
+    uint16_t* cur = s_buf[w][0];
+    uint16_t* cand = s_buf[w][1];
+    uint16_t* best = s_best[w];
+    int len, best_len;
+    int32_t cost, best_cost;
+    float temp;
+    uint64_t rng, step = ch.step, since = ch.since;
+    uint32_t accepted = 0;
+    bool zero;
+    if (status == 0) {   // NewChain (mcmc.go:28-49): start from the target
+        if (lane < (int)tlen) { cur[lane] = tg.ins[t0 + lane]; best[lane] = cur[lane]; }
+        __syncwarp();
+        len = best_len = (int)tlen;
+        rng = prm.seed + (uint64_t)ci * 0x9E3779B97F4A7C15ull + step;
+        temp = prm.t_start;
+        since = 0;
+        cost = best_cost = stoke_cost(cur, len, tv, mask, prm.cost_mode, lane, zero);
+    } else {
+        if (lane < kMaxSeq) { cur[lane] = ch.cur[lane]; best[lane] = ch.best[lane]; }
+        __syncwarp();
+        len = ch.len; best_len = ch.best_len;
+        cost = ch.cost; best_cost = ch.best_cost;
+        temp = ch.temp; rng = ch.rng;
+    }
+    for (uint32_t it = 0; it < prm.steps; it++, step++, since++) {
+        // Mutate (mutator.go:30-44): replace 40%, swap 20%, delete 20%,
+        // insert 10%, change immediate 10%.
+        const uint32_t r = sm_below(rng, 100);
+        int kind = r < 40 ? 0 : r < 60 ? 1 : r < 80 ? 2 : r < 90 ? 3 : 4;
+        int nlen = len, pos = 0;
+        uint16_t ins = 0;
+        if (kind == 3 && len >= max_len) kind = 0;              // InsertInstruction falls back
+        if (kind == 4) {
+            const unsigned immpos = __ballot_sync(kFull, lane < len && has_imm(cur[lane] & 0xFFu));
+            if (!immpos) kind = 0;                                // ChangeImmediate falls back
+            else {
+                uint32_t j = sm_below(rng, (uint32_t)__popc(immpos));
+                unsigned m = immpos;
+                for (uint32_t q = 0; q < j; q++) m &= m - 1;
+                pos = __ffs(m) - 1;
+                ins = (uint16_t)((cur[pos] & 0xFFu) | (sm_below(rng, 256) << 8));
+            }
+        }
+        if (kind == 0) { pos = (int)sm_below(rng, (uint32_t)len); ins = random_insn(rng); }
+        else if (kind == 1) { if (len >= 2) pos = (int)sm_below(rng, (uint32_t)(len - 1)); }
+        else if (kind == 2) { if (len > 1) { pos = (int)sm_below(rng, (uint32_t)len); nlen = len - 1; } }
+        else if (kind == 3) { pos = (int)sm_below(rng, (uint32_t)(len + 1)); ins = random_insn(rng); nlen = len + 1; }
+        if (lane < kMaxSeq) {
+            uint16_t v = cur[lane];
+            if (kind == 0 || kind == 4) v = lane == pos ? ins : cur[lane];
+            else if (kind == 1 && len >= 2) v = lane == pos ? cur[pos + 1] : (lane == pos + 1 ? cur[pos] : cur[lane]);
+            else if (kind == 2 && len > 1) v = lane < pos ? cur[lane] : (lane + 1 < kMaxSeq ? cur[lane + 1] : 0);
+            else if (kind == 3) v = lane < pos ? cur[lane] : (lane == pos ? ins : cur[lane - 1]);
+            cand[lane] = v;
+        }
+        __syncwarp();
+        const int32_t ncost = stoke_cost(cand, nlen, tv, mask, prm.cost_mode, lane, zero);
+        // Metropolis accept (mcmc.go:51-81)
+        const int32_t delta = ncost - cost;
+        bool acc = delta <= 0;
+        if (!acc && temp > 0.0f) acc = sm_unit(rng) < __expf(-(float)delta / temp);
+        if (acc) {
+            uint16_t* tmp = cur; cur = cand; cand = tmp;
+            len = nlen;
+            cost = ncost;
+            accepted++;
+            if (ncost < best_cost) {
+                if (lane < kMaxSeq) best[lane] = cur[lane];
+                __syncwarp();
+                best_len = len;
+                best_cost = ncost;
+                // verification trigger (search.go:101): zero mismatches and shorter
+                uint32_t bb = (lane < best_len) ? bytes_go(best[lane] & 0xFFu) : 0u;
+                bb = __reduce_add_sync(kFull, bb);
+                if (zero && bb < tbytes) {
+                    unsigned long long e = 0;
+                    if (lane == 0) e = atomicAdd(&sc->entries, 1ull);
+                    e = __shfl_sync(kFull, e, 0);
+                    if (e < ecap) {
+                        if (lane < kMaxSeq) entries[e].ins[lane] = best[lane];
+                        if (lane == 0) {
+                            entries[e].chain = ci; entries[e].target = t; entries[e].step = step;
+                            entries[e].len = (uint8_t)best_len; entries[e].dead_flags = 0;
+                        }
+                    }
+                }
+            }
+        }
+        temp *= prm.decay;
+        __syncwarp();
+    }
+    if (lane < kMaxSeq) { ch.cur[lane] = cur[lane]; ch.best[lane] = best[lane]; }
+    if (lane == 0) {
+        ch.len = (uint8_t)len; ch.best_len = (uint8_t)best_len;
+        ch.cost = cost; ch.best_cost = best_cost;
+        ch.temp = temp; ch.rng = rng; ch.step = step; ch.since = since;
+        ch.target = t; ch.status = 1;
+        ch.accepted += accepted;
+        atomicAdd(&sc->accepted, (unsigned long long)accepted);
+    }
+}
+
+// All 32 test vectors of each entry (a shorter zero-cost best): entries
+// that agree on every vector go on to ExhaustiveCheck (their indices are
+// compacted into vidx); FlagDiff over the QC vectors is recorded for masked runs.
+__global__ void k_stoke_vectors(StokeEntry* __restrict__ entries, uint64_t ecap, StokeTargets tg, uint32_t dead,
+                                uint32_t* __restrict__ vidx, StokeCounters* __restrict__ sc) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t n = min((uint64_t)sc->entries, ecap);
+    const uint64_t mask = cmp_mask(dead);
+    for (uint64_t e = (uint64_t)blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); e < n;
+         e += (uint64_t)gridDim.x * kWarpsPerBlock) {
+        StokeEntry& en = entries[e];
+        St s = unpack(c_vec[lane]);
+        for (int i = 0; i < en.len; i++) exec(s, en.ins[i]);
+        const uint64_t x = fp_of(s) ^ tg.out[(uint64_t)en.target * 32 + lane];
+        const bool ok = __all_sync(kFull, (x & mask) == 0);
+        uint32_t fd = lane < 8 ? ((uint32_t)(x >> 24) & kPMask) : 0u;
+        fd = __reduce_or_sync(kFull, fd);
+        if (lane == 0) {
+            en.dead_flags = (uint8_t)(dead ? fd : 0u);   // FlagDiff (verifier.go:591-604)
+            if (ok) vidx[atomicAdd(&sc->vec_ok, 1ull)] = (uint32_t)e;
+        }
+    }
+}
+
+// Pairs (target, entry) of the entries that passed all vectors.
+struct StokeSource {
+    const StokeEntry* entries;
+    const uint32_t* vidx;
+    StokeTargets tg;
+    uint32_t dead_;
+    __device__ void load(uint64_t p, uint16_t* st, uint16_t* sc, int& tn, int& cn, uint32_t& dead,
+                         int lane) const {
+        const StokeEntry& e = entries[vidx[p]];
+        const uint32_t t0 = tg.off[e.target];
+        tn = (int)(tg.off[e.target + 1] - t0);
+        cn = e.len;
+        if (lane < tn) st[lane] = tg.ins[t0 + lane];
+        if (lane < cn) sc[lane] = e.ins[lane];
+        dead = dead_;
+    }
+};
+
+// Proven entries become proofs; their chains restart (search.go:151-154) and
+// their targets are marked proven.
+__global__ void k_stoke_collect(const StokeEntry* __restrict__ entries, const uint32_t* __restrict__ vidx,
+                                const uint32_t* __restrict__ fail, StokeCounters* __restrict__ sc,
+                                StokeChain* __restrict__ chains, uint32_t* __restrict__ proven,
+                                uint32_t* __restrict__ proof_idx, uint64_t pcap) {
+    const uint64_t n = sc->vec_ok;
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+        if (fail[p] == 3) { atomicAdd(&sc->undecided, 1ull); continue; }
+        if (fail[p] != 0) continue;
+        const uint32_t e = vidx[p];
+        unsigned long long k = atomicAdd(&sc->proofs, 1ull);
+        if (k < pcap) proof_idx[k] = e;
+        proven[entries[e].target] = 1;
+        chains[entries[e].chain].status = 0;
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* t_insns, const uint32_t* t_offs,
+                    uint32_t n_targets, m6502_stoke_result* results, m6502_stoke_proof* proofs, uint64_t cap,
+                    uint64_t* n_proofs, m6502_stoke_stats* stats) {
+    if (!ctx) return M6502_E_INVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!cfg || !t_insns || !t_offs || (n_targets && !results)) return set_err(ctx, M6502_E_INVAL, "NULL argument");
+    if (cfg->cost > M6502_COST_HAMMING || cfg->sweep > M6502_SWEEP_FULL || cfg->max_len > (uint32_t)kMaxSeq)
+        return set_err(ctx, M6502_E_INVAL, "bad STOKE configuration");
+    if (cfg->proposal != M6502_PROPOSAL_UNIFORM)
+        return set_err(ctx, M6502_E_INVAL, "this build has the uniform proposal only");
+    for (uint32_t t = 0; t < n_targets; t++) {
+        uint32_t l = t_offs[t + 1] - t_offs[t];
+        if (t_offs[t + 1] < t_offs[t] || l < 1 || l > (uint32_t)kMaxSeq - 2)
+            return set_err(ctx, M6502_E_INVAL, "STOKE targets must have 1..14 instructions");
+    }
+    if (!valid_seq(t_insns + t_offs[0], t_offs[n_targets] - t_offs[0])) return set_err(ctx, M6502_E_INVAL, "opcode out of range");
+    if (n_proofs) *n_proofs = 0;
+    if (n_targets == 0) return M6502_OK;
+    CK(cudaSetDevice(ctx->device));
+    const uint32_t cpt = cfg->chains_per_target ? cfg->chains_per_target : 128;
+    const uint64_t n_chains64 = (uint64_t)cpt * n_targets;
+    if (n_chains64 > (1ull << 26)) return set_err(ctx, M6502_E_INVAL, "too many chains");
+    const uint32_t n_chains = (uint32_t)n_chains64;
+    const uint64_t steps = cfg->steps ? cfg->steps : 1000000ull;
+    const uint32_t spe = cfg->steps_per_epoch ? cfg->steps_per_epoch : 1000u;
+    const size_t tin = t_offs[n_targets];
+    // targets and their vector outputs
+    TRY(ensure(ctx, ctx->st_tins, tin * 2 + 2));
+    TRY(ensure(ctx, ctx->st_toffs, ((size_t)n_targets + 1) * 4));
+    TRY(ensure(ctx, ctx->st_tout, (size_t)n_targets * 32 * 8));
+    TRY(ensure(ctx, ctx->st_tbytes, n_targets));
+    std::vector<uint8_t> tb(n_targets);
+    for (uint32_t t = 0; t < n_targets; t++) {
+        uint32_t b = 0;
+        for (uint32_t i = t_offs[t]; i < t_offs[t + 1]; i++) b += bytes_go(t_insns[i] & 0xFFu);
+        tb[t] = (uint8_t)std::min(b, 255u);
+    }
+    CK(cudaMemcpyAsync(ctx->st_tins.p, t_insns, tin * 2, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->st_toffs.p, t_offs, ((size_t)n_targets + 1) * 4, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->st_tbytes.p, tb.data(), n_targets, cudaMemcpyHostToDevice, ctx->stream));
+    k_fingerprint<CsrSeqs><<<ctx->fp_blocks, 256, 0, ctx->stream>>>(
+        CsrSeqs{(const uint16_t*)ctx->st_tins.p, (const uint32_t*)ctx->st_toffs.p}, n_targets,
+        (uint64_t*)ctx->st_tout.p, nullptr);
+    CKL("k_fingerprint(stoke targets)");
+    // chains, entries, proofs
+    const uint64_t ecap = (uint64_t)n_chains * 16 + 1024;   // <= 16 shorter bests per chain and epoch
+    TRY(ensure(ctx, ctx->st_chains, (size_t)n_chains * sizeof(StokeChain)));
+    TRY(ensure(ctx, ctx->st_entries, ecap * sizeof(StokeEntry)));
+    TRY(ensure(ctx, ctx->st_vidx, ecap * 4));
+    TRY(ensure(ctx, ctx->fail, ecap * 4));
+    TRY(ensure(ctx, ctx->st_proven, (size_t)n_targets * 4));
+    TRY(ensure(ctx, ctx->st_cnt, sizeof(StokeCounters)));
+    TRY(ensure(ctx, ctx->st_pidx, ecap * 4));
+    CK(cudaMemsetAsync(ctx->st_chains.p, 0, (size_t)n_chains * sizeof(StokeChain), ctx->stream));
+    CK(cudaMemsetAsync(ctx->st_proven.p, 0, (size_t)n_targets * 4, ctx->stream));
+    StokeTargets tg{(const uint16_t*)ctx->st_tins.p, (const uint32_t*)ctx->st_toffs.p,
+                    (const uint64_t*)ctx->st_tout.p, (const uint8_t*)ctx->st_tbytes.p};
+    StokeParams prm;
+    prm.cost_mode = cfg->cost;
+    prm.dead = cfg->dead_flags;
+    prm.max_len = cfg->max_len;
+    prm.chains_per_target = cpt;
+    prm.seed = cfg->seed;
+    prm.stop_on_proof = cfg->stop_on_proof;
+    prm.proven = (const uint32_t*)ctx->st_proven.p;
+    if (cfg->cost == M6502_COST_REF) {
+        prm.t_start = 1.0f;
+        prm.decay = (float)(cfg->decay > 0.0 && cfg->decay < 1.0 ? cfg->decay : 0.9999);
+    } else {
+        double t0 = cfg->t_start > 0 ? cfg->t_start : 1.0, t1 = cfg->t_end > 0 ? cfg->t_end : 0.1;
+        prm.t_start = (float)t0;
+        prm.decay = (float)std::pow(t1 / t0, 1.0 / (double)steps);
+    }
+    std::vector<StokeEntry> h_entries;
+    std::vector<m6502_stoke_proof> found;
+    std::vector<double> first_ms(n_targets, -1.0);
+    std::vector<uint64_t> first_step(n_targets, 0);
+    m6502_stoke_stats st;
+    std::memset(&st, 0, sizeof st);
+    StokeCounters* sc = (StokeCounters*)ctx->st_cnt.p;
+    Counters* cnt = (Counters*)ctx->cnt.p;
+    uint64_t icap = std::max<uint64_t>(ctx->items.bytes / sizeof(Item), 1u << 16);
+    CK(cudaEventRecord(ctx->ev0, ctx->stream));
+    float ms_chains = 0, ms_verify = 0;
+    uint32_t proven_targets = 0;
+    for (uint64_t done = 0; done < steps;) {
+        const uint32_t e_steps = (uint32_t)std::min<uint64_t>(spe, steps - done);
+        prm.steps = e_steps;
+        CK(cudaMemsetAsync(sc, 0, sizeof(StokeCounters), ctx->stream));
+        CK(cudaEventRecord(ctx->sev[0], ctx->stream));
+        k_stoke_epoch<<<(n_chains + kWarpsPerBlock - 1) / kWarpsPerBlock, 256, 0, ctx->stream>>>(
+            (StokeChain*)ctx->st_chains.p, n_chains, tg, prm, (StokeEntry*)ctx->st_entries.p, ecap, sc);
+        CKL("k_stoke_epoch");
+        CK(cudaEventRecord(ctx->sev[1], ctx->stream));
+        k_stoke_vectors<<<ctx->sms * 8, 256, 0, ctx->stream>>>((StokeEntry*)ctx->st_entries.p, ecap, tg,
+                                                               cfg->dead_flags, (uint32_t*)ctx->st_vidx.p, sc);
+        CKL("k_stoke_vectors");
+        StokeSource src{(const StokeEntry*)ctx->st_entries.p, (const uint32_t*)ctx->st_vidx.p, tg, cfg->dead_flags};
+        for (int attempt = 0;; attempt++) {
+            TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
+            CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), ctx->stream));
+            ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg->sweep, 0};
+            k_exhaustive<StokeSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &sc->vec_ok, ecap, ea);
+            CKL("k_exhaustive(stoke)");
+            k_exh_items<StokeSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
+            CKL("k_exh_items(stoke)");
+            unsigned long long items = 0;
+            CK(cudaMemcpyAsync(&items, &cnt->items, sizeof items, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (items <= icap) break;
+            if (attempt >= 4) return set_err(ctx, M6502_E_NOMEM, "work-item queue kept overflowing");
+            icap = items + items / 4 + 1024;
+        }
+        k_stoke_collect<<<ctx->sms * 4, 256, 0, ctx->stream>>>((const StokeEntry*)ctx->st_entries.p,
+                                                               (const uint32_t*)ctx->st_vidx.p,
+                                                               (const uint32_t*)ctx->fail.p, sc,
+                                                               (StokeChain*)ctx->st_chains.p,
+                                                               (uint32_t*)ctx->st_proven.p,
+                                                               (uint32_t*)ctx->st_pidx.p, ecap);
+        CKL("k_stoke_collect");
+        CK(cudaEventRecord(ctx->sev[2], ctx->stream));
+        StokeCounters hc;
+        CK(cudaMemcpyAsync(&hc, sc, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        float e_ms = 0, a = 0, b = 0;
+        cudaEventElapsedTime(&e_ms, ctx->ev0, ctx->sev[2]);
+        cudaEventElapsedTime(&a, ctx->sev[0], ctx->sev[1]);
+        cudaEventElapsedTime(&b, ctx->sev[1], ctx->sev[2]);
+        ms_chains += a;
+        ms_verify += b;
+        done += e_steps;
+        st.epochs++;
+        st.steps += (uint64_t)e_steps * n_chains;   // chains that stopped still count their slot
+        st.accepted += hc.accepted;
+        st.candidates += std::min<uint64_t>(hc.entries, ecap);
+        st.undecided += hc.undecided;
+        if (hc.entries > ecap) return set_err(ctx, M6502_E_NOMEM, "STOKE entry buffer overflowed");
+        if (hc.proofs) {
+            std::vector<uint32_t> pidx(hc.proofs);
+            h_entries.resize(std::min<uint64_t>(hc.entries, ecap));
+            CK(cudaMemcpyAsync(pidx.data(), ctx->st_pidx.p, pidx.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaMemcpyAsync(h_entries.data(), ctx->st_entries.p, h_entries.size() * sizeof(StokeEntry),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            for (uint32_t e : pidx) {
+                const StokeEntry& en = h_entries[e];
+                m6502_stoke_proof pr;
+                std::memset(&pr, 0, sizeof pr);
+                pr.target = en.target; pr.chain = en.chain; pr.step = en.step; pr.ms = e_ms;
+                pr.cand_len = en.len; pr.dead_flags = en.dead_flags;
+                std::memcpy(pr.cand, en.ins, sizeof pr.cand);
+                found.push_back(pr);
+                if (first_ms[en.target] < 0) {
+                    first_ms[en.target] = e_ms;
+                    first_step[en.target] = en.step;
+                    proven_targets++;
+                } else if (en.step < first_step[en.target] && first_ms[en.target] == e_ms) {
+                    first_step[en.target] = en.step;
+                }
+            }
+            st.proofs += hc.proofs;
+        }
+        if (cfg->stop_on_proof && proven_targets == n_targets) break;
+    }
+    CK(cudaEventRecord(ctx->ev1, ctx->stream));
+    CK(cudaEventSynchronize(ctx->ev1));
+    float total = 0;
+    cudaEventElapsedTime(&total, ctx->ev0, ctx->ev1);
+    st.ms_device = total;
+    st.ms_chains = ms_chains;
+    st.ms_verify = ms_verify;
+    st.targets_proven = proven_targets;
+    // per-target summary: first proof, and the best proof (most Go bytes, then cycles saved)
+    for (uint32_t t = 0; t < n_targets; t++) {
+        m6502_stoke_result& r = results[t];
+        std::memset(&r, 0, sizeof r);
+        r.first_proof_ms = first_ms[t];
+        r.first_proof_step = first_step[t];
+    }
+    for (const m6502_stoke_proof& pr : found) {
+        m6502_stoke_result& r = results[pr.target];
+        const uint16_t* ts = t_insns + t_offs[pr.target];
+        int tn = (int)(t_offs[pr.target + 1] - t_offs[pr.target]);
+        int bs = 0, cs = 0;
+        for (int i = 0; i < tn; i++) { bs += (int)bytes_go(ts[i] & 0xFFu); cs += (int)cycles(ts[i] & 0xFFu); }
+        for (int i = 0; i < pr.cand_len; i++) { bs -= (int)bytes_go(pr.cand[i] & 0xFFu); cs -= (int)cycles(pr.cand[i] & 0xFFu); }
+        if (r.proofs == 0 || bs > r.bytes_saved || (bs == r.bytes_saved && cs > r.cycles_saved)) {
+            r.best_len = pr.cand_len;
+            std::memcpy(r.best, pr.cand, sizeof r.best);
+            r.bytes_saved = (int16_t)bs;
+            r.cycles_saved = (int16_t)cs;
+            r.dead_flags = pr.dead_flags;
+        }
+        r.proofs++;
+    }
+    if (stats) *stats = st;
+    if (n_proofs) *n_proofs = found.size();
+    if (proofs && cap) std::memcpy(proofs, found.data(), std::min<uint64_t>(cap, found.size()) * sizeof(m6502_stoke_proof));
+    if (found.size() > cap) return set_err(ctx, M6502_E_OVERFLOW, "proof buffer too small");
+    return M6502_OK;
+}
+
+}  // extern "C"

@@ -23,6 +23,8 @@ M6502_E_TOOBIG = -6
 STATIC_MAX_PAIRS = 1 << 20
 
 SEM_CUDA, SEM_GO = 0, 1
+COST_REF, COST_HAMMING = 0, 1
+PROPOSAL_UNIFORM = 0
 SWEEP_REFERENCE, SWEEP_FULL = 0, 1
 EXH_CONES, EXH_BRUTE = 0, 1
 CHECK_QC, CHECK_MID, CHECK_EXH, CHECK_ALL = 1, 2, 4, 7
@@ -69,6 +71,39 @@ class Stats(ctypes.Structure):
         return {n: getattr(self, n) for n, _ in self._fields_}
 
 
+class StokeCfg(ctypes.Structure):
+    _fields_ = [("chains_per_target", ctypes.c_uint32), ("steps_per_epoch", ctypes.c_uint32),
+                ("steps", ctypes.c_uint64), ("seed", ctypes.c_uint64), ("decay", ctypes.c_double),
+                ("t_start", ctypes.c_double), ("t_end", ctypes.c_double), ("cost", ctypes.c_uint32),
+                ("max_len", ctypes.c_uint32), ("sweep", ctypes.c_uint32), ("stop_on_proof", ctypes.c_uint32),
+                ("proposal", ctypes.c_uint32), ("dead_flags", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 3)]
+
+
+class StokeProof(ctypes.Structure):
+    _fields_ = [("target", ctypes.c_uint32), ("chain", ctypes.c_uint32), ("step", ctypes.c_uint64),
+                ("ms", ctypes.c_double), ("cand", ctypes.c_uint16 * 16), ("cand_len", ctypes.c_uint8),
+                ("dead_flags", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 6)]
+
+
+class StokeResult(ctypes.Structure):
+    _fields_ = [("first_proof_ms", ctypes.c_double), ("first_proof_step", ctypes.c_uint64),
+                ("proofs", ctypes.c_uint32), ("bytes_saved", ctypes.c_int16), ("cycles_saved", ctypes.c_int16),
+                ("best", ctypes.c_uint16 * 16), ("best_len", ctypes.c_uint8), ("dead_flags", ctypes.c_uint8),
+                ("reserved", ctypes.c_uint8 * 6)]
+
+
+class StokeStats(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in ("steps", "accepted", "candidates", "proofs", "undecided", "epochs",
+                                              "targets_proven")] + \
+               [(n, ctypes.c_double) for n in ("ms_device", "ms_chains", "ms_verify")]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
+
+
+assert ctypes.sizeof(StokeProof) == 64 and ctypes.sizeof(StokeResult) == 64
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -76,9 +111,9 @@ _lock = threading.Lock()
 SYMBOLS = (
     "m6502_version", "m6502_create", "m6502_destroy", "m6502_last_error", "m6502_stream",
     "m6502_check_pairs", "m6502_fingerprint", "m6502_exec_batch", "m6502_search", "m6502_enumerate",
-    "m6502_insn_table", "m6502_enumerate_targets", "m6502_disasm", "m6502_parse", "m6502_should_prune",
+    "m6502_insn_table", "m6502_enumerate_targets", "m6502_draw_targets", "m6502_disasm", "m6502_parse", "m6502_should_prune",
     "m6502_seq_bytes", "m6502_seq_cycles", "m6502_op_deps", "m6502_format_jsonl",
-    "m6502_exhaustive_static",
+    "m6502_exhaustive_static", "m6502_stoke_run",
 )
 
 
@@ -114,6 +149,8 @@ def lib():
         L.m6502_enumerate_targets.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, u16p,
                                               ctypes.c_uint64]
         L.m6502_enumerate_targets.restype = ctypes.c_uint64
+        L.m6502_draw_targets.argtypes = [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                                         ctypes.c_int, u16p, u32p]
         L.m6502_disasm.argtypes = [ctypes.c_uint16, ctypes.c_char_p, ctypes.c_int]
         L.m6502_parse.argtypes = [ctypes.c_char_p, u16p, ctypes.c_int]
         L.m6502_should_prune.argtypes = [u16p, ctypes.c_int]
@@ -122,6 +159,8 @@ def lib():
         L.m6502_op_deps.argtypes = [ctypes.c_int, u16p]
         L.m6502_format_jsonl.argtypes = [u16p, ctypes.c_int, P(Rule), ctypes.c_uint8,
                                          ctypes.c_char_p, ctypes.c_int]
+        L.m6502_stoke_run.argtypes = [vp, P(StokeCfg), u16p, u32p, ctypes.c_uint32, P(StokeResult),
+                                      P(StokeProof), ctypes.c_uint64, u64p, P(StokeStats)]
         L.m6502_exhaustive_static.argtypes = [ctypes.c_uint64, vp, vp, vp, vp, ctypes.c_uint8, ctypes.c_uint32,
                                               vp, vp]
         _lib = L

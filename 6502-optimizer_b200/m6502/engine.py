@@ -148,6 +148,43 @@ class Engine:
                              first, last)
 
 
+    # ---- STOKE (pkg/stoke) ----
+    def stoke(self, targets, chains_per_target=128, steps=1_000_000, steps_per_epoch=1000, seed=0,
+              cost=_lib.COST_REF, decay=0.9999, t_start=1.0, t_end=0.1, max_len=0, dead_flags=0,
+              sweep=_lib.SWEEP_REFERENCE, stop_on_proof=False, cap=1 << 16):
+        """Batched STOKE over targets (list of sequences).  Returns (results,
+        proofs, stats): results[i] is a dict per target (first_proof_ms < 0 when
+        unproven, best rewrite), proofs every proof found, in order."""
+        f, o = _csr(targets)
+        cfg = _lib.StokeCfg()
+        cfg.chains_per_target, cfg.steps_per_epoch, cfg.steps, cfg.seed = chains_per_target, steps_per_epoch, steps, seed
+        cfg.decay, cfg.t_start, cfg.t_end, cfg.cost = decay, t_start, t_end, cost
+        cfg.max_len, cfg.sweep, cfg.stop_on_proof, cfg.dead_flags = max_len, sweep, int(stop_on_proof), dead_flags
+        n = len(targets)
+        res = (_lib.StokeResult * max(n, 1))()
+        st = _lib.StokeStats()
+        n_out = ctypes.c_uint64(0)
+        while True:
+            prf = (_lib.StokeProof * max(cap, 1))()
+            with self._lock:
+                rc = self._L.m6502_stoke_run(self._ctx, ctypes.byref(cfg), _lib.ptr(f, ctypes.c_uint16),
+                                             _lib.ptr(o, ctypes.c_uint32), n, res, prf, cap, ctypes.byref(n_out),
+                                             ctypes.byref(st))
+            if rc == _lib.M6502_E_OVERFLOW:
+                cap = int(n_out.value)
+                continue
+            self._check(rc)
+            break
+        results = [{"first_proof_ms": r.first_proof_ms, "first_proof_step": r.first_proof_step,
+                    "proofs": r.proofs, "bytes_saved": r.bytes_saved, "cycles_saved": r.cycles_saved,
+                    "best": [int(x) for x in r.best[:r.best_len]], "dead_flags": r.dead_flags}
+                   for r in res[:n]]
+        proofs = [{"target": p.target, "chain": p.chain, "step": p.step, "ms": p.ms,
+                   "cand": [int(x) for x in p.cand[:p.cand_len]], "dead_flags": p.dead_flags}
+                  for p in prf[:n_out.value]]
+        return results, proofs, st.as_dict()
+
+
 _default = None
 _default_lock = threading.Lock()
 

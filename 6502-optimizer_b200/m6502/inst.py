@@ -108,3 +108,14 @@ def enumerate_targets(length, first=0, last=NUM_INSNS):
     out = np.zeros((max(n, 1), length), dtype=np.uint16)
     L.m6502_enumerate_targets(length, first, last, _lib.ptr(out, _lib.ctypes.c_uint16), n)
     return out[:n]
+
+
+def draw_targets(seed, min_len, max_len, n, reject_pruned=True):
+    """Seeded workload draw (m6502_draw_targets): list of n sequences."""
+    insns = np.zeros(max(n * max_len, 1), dtype=np.uint16)
+    offs = np.zeros(n + 1, dtype=np.uint32)
+    rc = _lib.lib().m6502_draw_targets(seed, min_len, max_len, n, int(reject_pruned),
+                                       _lib.ptr(insns, _lib.ctypes.c_uint16), _lib.ptr(offs, _lib.ctypes.c_uint32))
+    if rc != 0:
+        raise ValueError("bad draw arguments")
+    return [[int(x) for x in insns[offs[i]:offs[i + 1]]] for i in range(n)]

@@ -295,6 +295,44 @@ def run_engine(args):
         dist.destroy_process_group()
 
 
+def run_stoke(args):
+    """STOKE benchmark workload: 512 seeded targets of length 4..8 (seed 2),
+    128 chains each (65,536 chains), Hamming cost over the 32 MidCheck
+    vectors, temperature 1.0 -> 0.1; every shorter zero-cost best is proved on
+    the GPU.  Metric: median time-to-proof over the proved targets."""
+    import torch
+    import m6502
+    from m6502 import inst, _lib
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    targets = inst.draw_targets(2, 4, 8, 512, reject_pruned=False)
+    eng = m6502.Engine(device=local)
+    eng.stoke(targets[:8], chains_per_target=8, steps=2000, steps_per_epoch=1000, seed=1, cost=_lib.COST_HAMMING)
+    clocks = ClockSampler(local)
+    clocks.start()
+    res, proofs, st = eng.stoke(targets, chains_per_target=128, steps=args.stoke_steps,
+                                steps_per_epoch=args.stoke_epoch, seed=2, cost=_lib.COST_HAMMING,
+                                sweep=_lib.SWEEP_FULL, stop_on_proof=True)
+    clk = clocks.stop()
+    times = sorted(r["first_proof_ms"] for r in res if r["first_proof_ms"] >= 0)
+    median = statistics.median(times) if times else None
+    line = {"metric": "STOKE time-to-proof (median over proved targets)", "value": median, "unit": "ms",
+            "higher_is_better": False, "n_gpus": 1, "steps": args.stoke_steps, "warmup": 1,
+            "dtype": "u8", "data": "synthetic (512 seeded random targets, length 4-8, seed 2)",
+            "config": {"workload": "stoke-512x128", "targets": len(targets), "chains_per_target": 128,
+                       "steps_per_chain": args.stoke_steps, "steps_per_epoch": args.stoke_epoch,
+                       "cost": "hamming over 32 vectors + bytes + cycles/100", "temperature": "1.0 -> 0.1",
+                       "proposal": "uniform", "sweep": "full", "stop_on_proof": True},
+            "proved": len(times), "censored": len(targets) - len(times),
+            "proofs": st["proofs"], "candidates": st["candidates"], "undecided": st["undecided"],
+            "chain_steps_per_s": st["steps"] / (st["ms_device"] / 1e3) if st["ms_device"] else None,
+            "ms_device": st["ms_device"], "ms_chains": st["ms_chains"], "ms_verify": st["ms_verify"],
+            "p90_ms": times[int(0.9 * (len(times) - 1))] if times else None,
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}}
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -305,8 +343,13 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1500, help="targets in the CPU baseline sample")
     ap.add_argument("--ref-sample", type=int, default=600, help="targets per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["len2", "stoke"], default="len2")
+    ap.add_argument("--stoke-steps", type=int, default=1000000, help="steps per chain (STOKE workload)")
+    ap.add_argument("--stoke-epoch", type=int, default=2000, help="steps between proof rounds (STOKE workload)")
     args = ap.parse_args()
-    if args.impl == "reference":
+    if args.workload == "stoke":
+        run_stoke(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_engine(args)

@@ -211,6 +211,76 @@ int m6502_enumerate(m6502_ctx *ctx, const m6502_search_cfg *cfg, uint32_t tlen, 
                     uint32_t last, m6502_rule *out, uint64_t cap, uint64_t *n_out,
                     m6502_stats *stats);
 
+/* ---- STOKE ----
+ * Batched STOKE over many targets: chains_per_target MCMC chains per target
+ * (one warp each), replacing stoke.Run (pkg/stoke/search.go:32-176) with its
+ * Chain.Step (mcmc.go:51-81), Mutator (mutator.go:30-115) and Cost
+ * (cost.go:32-81).  Every shorter zero-cost best is checked on all 32 test
+ * vectors and proved by ExhaustiveCheck(Masked) on the device; a proof
+ * restarts its chain (search.go:151-154), or with stop_on_proof stops every
+ * chain of its target. */
+enum {
+    M6502_COST_REF = 0,     /* 1000 x mismatching QC vectors + bytes + cycles/100; T *= decay */
+    M6502_COST_HAMMING = 1  /* differing output bits over the 32 MidCheck vectors + bytes +
+                               cycles/100; T annealed geometrically t_start -> t_end */
+};
+enum { M6502_PROPOSAL_UNIFORM = 0 };
+
+typedef struct m6502_stoke_cfg {
+    uint32_t chains_per_target; /* 0 = 128 */
+    uint32_t steps_per_epoch;   /* steps between proof rounds (time resolution); 0 = 1000 */
+    uint64_t steps;             /* steps per chain; 0 = 1,000,000 */
+    uint64_t seed;              /* base seed of the chains' generators */
+    double decay;               /* COST_REF temperature factor per step; 0 = 0.9999 */
+    double t_start, t_end;      /* COST_HAMMING temperatures; 0 = 1.0 and 0.1 */
+    uint32_t cost;              /* M6502_COST_* */
+    uint32_t max_len;           /* longest candidate; 0 = max(len + 2, 10) (mcmc.go:30-33); <= 16 */
+    uint32_t sweep;             /* M6502_SWEEP_* of the proofs */
+    uint32_t stop_on_proof;     /* stop a target's chains at its first proof */
+    uint32_t proposal;          /* M6502_PROPOSAL_* */
+    uint8_t dead_flags;         /* stoke --dead-flags */
+    uint8_t reserved[3];
+} m6502_stoke_cfg;
+
+typedef struct m6502_stoke_proof {
+    uint32_t target, chain;
+    uint64_t step;              /* chain step that found the rewrite */
+    double ms;                  /* device time from the call's start to the proof round */
+    uint16_t cand[16];
+    uint8_t cand_len;
+    uint8_t dead_flags;         /* FlagDiff of a masked run (search.go:105-108), else 0 */
+    uint8_t reserved[6];
+} m6502_stoke_proof;            /* 64 bytes */
+
+typedef struct m6502_stoke_result {
+    double first_proof_ms;      /* time to the first proof of this target; < 0 if none */
+    uint64_t first_proof_step;
+    uint32_t proofs;            /* proofs found for this target */
+    int16_t bytes_saved, cycles_saved;   /* of the best proof (Go sizes) */
+    uint16_t best[16];
+    uint8_t best_len, dead_flags;
+    uint8_t reserved[6];
+} m6502_stoke_result;           /* 64 bytes */
+
+typedef struct m6502_stoke_stats {
+    uint64_t steps;             /* chain steps run (all chains) */
+    uint64_t accepted;          /* accepted moves */
+    uint64_t candidates;        /* shorter zero-cost bests sent to verification */
+    uint64_t proofs;            /* of those, proved equivalent */
+    uint64_t undecided;         /* sweeps beyond the cone cap */
+    uint64_t epochs;
+    uint64_t targets_proven;
+    double ms_device, ms_chains, ms_verify;
+} m6502_stoke_stats;
+
+/* n_targets targets (CSR, 1..14 instructions each).  results[n_targets] gets
+ * the per-target summary; proofs (capacity cap, may be NULL) every proof in
+ * the order found; *n_proofs the proof count (M6502_E_OVERFLOW if > cap). */
+int m6502_stoke_run(m6502_ctx *ctx, const m6502_stoke_cfg *cfg, const uint16_t *t_insns,
+                    const uint32_t *t_offs, uint32_t n_targets, m6502_stoke_result *results,
+                    m6502_stoke_proof *proofs, uint64_t cap, uint64_t *n_proofs,
+                    m6502_stoke_stats *stats);
+
 /* ---- host helpers (no GPU needed) ---- */
 /* The 2863 instructions in CUDA order (cuda/6502_search_v2.cu:741-752) or Go
  * order (pkg/search/enumerator.go:14-38). */
@@ -221,6 +291,14 @@ int m6502_insn_table(uint32_t semantics, uint16_t *out);
  * and returns the total count; out may be NULL to count only. */
 uint64_t m6502_enumerate_targets(uint32_t tlen, uint32_t first, uint32_t last, uint16_t *out,
                                  uint64_t cap);
+/* Seeded draw of n targets: splitmix64 from `seed`; each target's length
+ * uniform in [min_len, max_len] (drawn first when the range is not a single
+ * value), then each instruction uniform over the CUDA-order table (index by
+ * rejection sampling, no modulo bias); with reject_pruned, pruned draws are
+ * redrawn.  Writes CSR: insns (n * max_len capacity) and offs (n + 1).  The
+ * reference defines no workload draw; this one fixes the benchmark inputs. */
+int m6502_draw_targets(uint64_t seed, uint32_t min_len, uint32_t max_len, uint64_t n, int reject_pruned,
+                       uint16_t *insns, uint32_t *offs);
 /* Disassemble (pkg/inst/catalog.go:59-86); returns the text length. */
 int m6502_disasm(uint16_t insn, char *buf, int cap);
 /* parseAssembly (cmd/6502opt/main.go:302-322): "LDA #$42 : TAX" -> insns.

@@ -162,3 +162,14 @@ def test_format_jsonl_matches_oracle():
     line = json.loads(jsonl_line(t, r, 0xC3))
     assert line == {"source_asm": "LDA M : EOR M", "replacement_asm": "LDA #$00", "source_bytes": 4,
                     "replacement_bytes": 2, "bytes_saved": 2, "cycles_saved": 4, "dead_flags": "0xC3"}
+
+
+def test_draw_targets_matches_oracle_draw():
+    """The library's seeded draw equals the oracle's for fixed lengths (the
+    config-1 and length-3 workloads) and keeps lengths in range otherwise."""
+    for seed, length, n in ((0, 2, 256), (1, 3, 200)):
+        got = I.draw_targets(seed, length, length, n, reject_pruned=True)
+        assert got == oracle.draw_targets(seed, length, n).tolist()
+    var = I.draw_targets(2, 4, 8, 512, reject_pruned=False)
+    assert len(var) == 512 and all(4 <= len(s) <= 8 for s in var)
+    assert len({len(s) for s in var}) == 5

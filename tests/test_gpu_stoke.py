@@ -1,0 +1,80 @@
+"""Batched STOKE on the GPU (pkg/stoke restated): every rewrite the engine
+reports is re-proved by the CPU oracle, and rewrites the reference's examples
+make obvious are found."""
+import numpy as np
+import pytest
+
+import oracle
+from m6502 import _lib
+from m6502 import inst as I
+
+pytestmark = pytest.mark.gpu
+
+EASY = ["TXA : TAX", "CLC : CLC", "ROL A : AND #$FE", "LDA M : EOR M", "PHA : PLA : TAX",
+        "LDX #$05 : LDX #$07 : TXA", "SEC : CLC : INX"]
+
+
+def _go_bytes(seq):
+    return sum(oracle.lib().or_byte_size_go(x & 0xFF) for x in seq)
+
+
+def _oracle_sweep_ok(t, c):
+    """The CPU oracle re-proves pairs whose reference sweep has at most
+    512 x 32^4 states (a few seconds in C); wider ones are skipped."""
+    reads = 0
+    for x in list(t) + list(c):
+        reads |= int(oracle.lib().or_op_reads(x & 0xFF))
+    return bin(reads & 0xFC).count("1") <= 4
+
+
+@pytest.mark.parametrize("cost", [_lib.COST_REF, _lib.COST_HAMMING])
+def test_stoke_proofs_reprove_on_oracle(engine, cost):
+    targets = [I.parse_assembly(t) for t in EASY]
+    res, proofs, st = engine.stoke(targets, chains_per_target=32, steps=20000, steps_per_epoch=500, seed=7,
+                                   cost=cost, sweep=_lib.SWEEP_REFERENCE)
+    assert st["steps"] == 32 * len(targets) * 20000
+    assert 0 < st["accepted"] <= st["steps"]
+    assert st["proofs"] == len(proofs) > 0
+    for p in proofs:
+        t, c = targets[p["target"]], p["cand"]
+        assert _go_bytes(c) < _go_bytes(t)
+        assert oracle.quickcheck(t, c) and oracle.midcheck(t, c), (t, c)
+        assert oracle.exhaustive(t, c, 0, oracle.SWEEP_REFERENCE), (t, c)
+    # the two-instruction examples all have a one-instruction rewrite
+    for i, name in enumerate(EASY[:4]):
+        assert res[i]["first_proof_ms"] >= 0, name
+        assert res[i]["bytes_saved"] >= 1, name
+
+
+def test_stoke_masked_reports_flagdiff(engine):
+    """--dead-flags: proofs hold under the mask and carry FlagDiff
+    (pkg/stoke/search.go:104-108)."""
+    targets = [I.parse_assembly(t) for t in ("CMP #$10 : LDA #$00", "CLC : ADC #$01 : CLV")]
+    _, proofs, _ = engine.stoke(targets, chains_per_target=32, steps=20000, steps_per_epoch=500, seed=3,
+                                dead_flags=0xC3, sweep=_lib.SWEEP_REFERENCE)
+    assert proofs
+    for p in proofs:
+        t, c = targets[p["target"]], p["cand"]
+        assert oracle.exhaustive(t, c, 0xC3, oracle.SWEEP_REFERENCE)
+        assert p["dead_flags"] == oracle.flagdiff(t, c)
+
+
+def test_stoke_stop_on_proof_and_random_targets(engine):
+    """Seeded random targets of length 4..8 (the STOKE benchmark's draw):
+    stop_on_proof ends a proved target's chains; all proofs re-prove."""
+    rng = np.random.default_rng(2)
+    tab = oracle.insn_table()
+    targets = [[int(tab[k]) for k in rng.integers(0, 2863, size=int(rng.integers(4, 9)))] for _ in range(24)]
+    res, proofs, st = engine.stoke(targets, chains_per_target=16, steps=30000, steps_per_epoch=1000, seed=11,
+                                   cost=_lib.COST_HAMMING, stop_on_proof=True, sweep=_lib.SWEEP_REFERENCE)
+    proved = [i for i, r in enumerate(res) if r["first_proof_ms"] >= 0]
+    assert st["targets_proven"] == len(proved)
+    checked = 0
+    for p in proofs:
+        t, c = targets[p["target"]], p["cand"]
+        assert _go_bytes(c) < _go_bytes(t)
+        assert oracle.quickcheck(t, c) and oracle.midcheck(t, c)
+        if _oracle_sweep_ok(t, c):
+            assert oracle.exhaustive(t, c, 0, oracle.SWEEP_REFERENCE)
+            checked += 1
+    assert checked >= min(len(proofs), 1) or not proofs
