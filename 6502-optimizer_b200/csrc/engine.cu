@@ -31,6 +31,7 @@
 #include <string>
 #include <vector>
 
+#include "internal.h"
 #include "isa.cuh"
 #include "m6502.h"
 
@@ -1107,7 +1108,8 @@ struct m6502_ctx {
     std::vector<uint8_t> h_cmeta;
     DevBuf join_keys[256], join_idx[256];
     uint32_t join_n[256] = {};
-    DevBuf st_tins, st_toffs, st_tout, st_tbytes, st_chains, st_entries, st_vidx, st_proven, st_cnt, st_pidx;
+    DevBuf st_tins, st_toffs, st_tout, st_tbytes, st_chains, st_entries, st_vidx, st_proven, st_cnt, st_pidx,
+        st_mex, st_probs, st_traj;
 };
 
 namespace {
@@ -1399,6 +1401,12 @@ extern "C" {
 
 const char* m6502_version(void) { return "m6502-b200 1.0 (sm_100a)"; }
 
+}  // extern "C"
+
+int m6502_ctx_device(const m6502_ctx* ctx) { return ctx ? ctx->device : 0; }
+
+extern "C" {
+
 int m6502_create(m6502_ctx** out, const m6502_opts* opts) {
     if (!out) return M6502_E_INVAL;
     *out = nullptr;
@@ -1446,7 +1454,7 @@ void m6502_destroy(m6502_ctx* ctx) {
                       &ctx->pins, &ctx->poffs, &ctx->cins, &ctx->coffs, &ctx->pout, &ctx->pfd,
                       &ctx->enum_count, &ctx->st_tins, &ctx->st_toffs, &ctx->st_tout, &ctx->st_tbytes,
                       &ctx->st_chains, &ctx->st_entries, &ctx->st_vidx, &ctx->st_proven, &ctx->st_cnt,
-                      &ctx->st_pidx};
+                      &ctx->st_pidx, &ctx->st_mex, &ctx->st_probs, &ctx->st_traj};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);

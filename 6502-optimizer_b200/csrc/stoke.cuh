@@ -25,6 +25,7 @@ struct StokeChain {
     int32_t cost, best_cost;
     uint32_t target;
     uint32_t accepted;
+    uint32_t diff;          // MidCheck vectors on which the current candidate differs
     uint8_t len, best_len, status, pad;   // status: 0 (re)start, 1 running, 2 stopped
 };
 
@@ -36,7 +37,7 @@ struct StokeEntry {        // a shorter zero-cost best awaiting proof
 };
 
 struct StokeCounters {
-    unsigned long long entries, vec_ok, proofs, undecided, accepted;
+    unsigned long long entries, vec_ok, proofs, undecided, accepted, traj;
 };
 
 struct StokeTargets {
@@ -57,6 +58,10 @@ struct StokeParams {
     float t_start;
     const uint32_t* proven; // per target: 1 once proved (stop_on_proof)
     uint32_t stop_on_proof;
+    const float* cdf;       // PROPOSAL_MIXED: per chain 330 cumulative probabilities (3 heads)
+    float learned_frac;
+    m6502_mlp_example* traj;   // improving moves as labelled examples (optional)
+    uint64_t traj_cap;
 };
 
 __device__ __forceinline__ uint64_t sm_next(uint64_t& x) {
@@ -84,7 +89,7 @@ __device__ __forceinline__ uint16_t random_insn(uint64_t& rng) {
 // cycles / 100 (cost.go:32-81); COST_HAMMING: differing output bits over the
 // 32 vectors + bytes + cycles / 100.  `zero` is true when no vector differs.
 __device__ __forceinline__ int32_t stoke_cost(const uint16_t* seq, int len, uint64_t tv, uint64_t mask,
-                                              uint32_t mode, int lane, bool& zero) {
+                                              uint32_t mode, int lane, bool& zero, uint32_t& vmask) {
     St s = unpack(c_vec[lane]);
     for (int i = 0; i < len; i++) exec(s, seq[i]);
     const uint64_t x = (fp_of(s) ^ tv) & mask;
@@ -93,6 +98,7 @@ __device__ __forceinline__ int32_t stoke_cost(const uint16_t* seq, int len, uint
     b = __reduce_add_sync(kFull, b);
     c = __reduce_add_sync(kFull, c);
     int32_t base = (int32_t)(b + c / 100u);
+    vmask = __ballot_sync(kFull, x != 0);
     if (mode == M6502_COST_REF) {
         unsigned mism = __ballot_sync(kFull, x != 0) & 0xFFu;
         zero = mism == 0;
@@ -101,6 +107,54 @@ __device__ __forceinline__ int32_t stoke_cost(const uint16_t* seq, int len, uint
     uint32_t h = __reduce_add_sync(kFull, (uint32_t)__popcll(x));
     zero = h == 0;
     return (int32_t)h + base;
+}
+
+// Index drawn from one head of a chain's cumulative distribution (entries
+// [a, b) hold running sums); warp-uniform binary search.
+__device__ __forceinline__ int cdf_sample(const float* cdf, int a, int b, uint64_t& rng) {
+    const float base = a > 0 ? cdf[a - 1] : 0.0f;
+    const float r = base + sm_unit(rng) * (cdf[b - 1] - base);
+    int lo = a, hi = b - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (cdf[mid] > r) hi = mid; else lo = mid + 1;
+    }
+    return lo - a;
+}
+
+// The model's input for every chain: target, current candidate and its
+// vector mismatch mask (a chain about to (re)start uses the target itself).
+__global__ void k_stoke_examples(const StokeChain* __restrict__ chains, uint32_t n_chains, uint32_t cpt,
+                                 StokeTargets tg, m6502_mlp_example* __restrict__ ex) {
+    const int lane = threadIdx.x & 31;
+    for (uint32_t ci = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); ci < n_chains;
+         ci += gridDim.x * kWarpsPerBlock) {
+        const StokeChain& ch = chains[ci];
+        const uint32_t t = ci / cpt, t0 = tg.off[t], tlen = tg.off[t + 1] - t0;
+        const bool fresh = ch.status != 1;
+        m6502_mlp_example& x = ex[ci];
+        if (lane < 8) x.target[lane] = lane < (int)tlen ? tg.ins[t0 + lane] : 0;
+        if (lane < 16) x.cand[lane] = fresh ? (lane < (int)tlen ? tg.ins[t0 + lane] : 0) : ch.cur[lane];
+        if (lane == 0) {
+            x.diff = fresh ? 0u : ch.diff;
+            x.tlen = (uint8_t)min(tlen, 8u);
+            x.clen = fresh ? (uint8_t)tlen : ch.len;
+            x.pos = x.op = x.imm = 0;
+            x.weight = 0;
+        }
+    }
+}
+
+// Softmax outputs -> running sums per head (in place), one thread per chain.
+__global__ void k_cdf(float* __restrict__ p, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        float* r = p + (size_t)i * 330;
+        const int cut[4] = {0, 16, 74, 330};
+        for (int h = 0; h < 3; h++) {
+            float s = 0.0f;
+            for (int k = cut[h]; k < cut[h + 1]; k++) { s += r[k]; r[k] = s; }
+        }
+    }
 }
 
 // One epoch of every chain: warp per chain.
@@ -133,8 +187,9 @@ __global__ void __launch_bounds__(256) k_stoke_epoch(StokeChain* __restrict__ ch
     int32_t cost, best_cost;
     float temp;
     uint64_t rng, step = ch.step, since = ch.since;
-    uint32_t accepted = 0;
+    uint32_t accepted = 0, diff = 0;
     bool zero;
+    const float* cdf = prm.cdf ? prm.cdf + (size_t)ci * 330 : nullptr;
     if (status == 0) {   // NewChain (mcmc.go:28-49): start from the target
         if (lane < (int)tlen) { cur[lane] = tg.ins[t0 + lane]; best[lane] = cur[lane]; }
         __syncwarp();
@@ -142,13 +197,15 @@ __global__ void __launch_bounds__(256) k_stoke_epoch(StokeChain* __restrict__ ch
         rng = prm.seed + (uint64_t)ci * 0x9E3779B97F4A7C15ull + step;
         temp = prm.t_start;
         since = 0;
-        cost = best_cost = stoke_cost(cur, len, tv, mask, prm.cost_mode, lane, zero);
+        cost = best_cost = stoke_cost(cur, len, tv, mask, prm.cost_mode, lane, zero, diff);
+
     } else {
         if (lane < kMaxSeq) { cur[lane] = ch.cur[lane]; best[lane] = ch.best[lane]; }
         __syncwarp();
         len = ch.len; best_len = ch.best_len;
         cost = ch.cost; best_cost = ch.best_cost;
         temp = ch.temp; rng = ch.rng;
+        diff = ch.diff;
     }
     for (uint32_t it = 0; it < prm.steps; it++, step++, since++) {
         // Mutate (mutator.go:30-44): replace 40%, swap 20%, delete 20%,
@@ -169,7 +226,17 @@ __global__ void __launch_bounds__(256) k_stoke_epoch(StokeChain* __restrict__ ch
                 ins = (uint16_t)((cur[pos] & 0xFFu) | (sm_below(rng, 256) << 8));
             }
         }
-        if (kind == 0) { pos = (int)sm_below(rng, (uint32_t)len); ins = random_insn(rng); }
+        const bool learned = cdf && (kind == 0 || kind == 3) && sm_unit(rng) < prm.learned_frac;
+        if (learned) {   // position, opcode, operand from the model's distributions
+            const int lim = kind == 0 ? len : len + 1;
+            pos = cdf_sample(cdf, 0, 16, rng);
+            if (pos >= lim) pos = (int)sm_below(rng, (uint32_t)lim);
+            const uint32_t op = (uint32_t)cdf_sample(cdf, 16, 74, rng);
+            const uint32_t imm = has_imm(op) ? (uint32_t)cdf_sample(cdf, 74, 330, rng) : 0u;
+            ins = (uint16_t)(op | (imm << 8));
+            if (kind == 3) nlen = len + 1;
+        }
+        else if (kind == 0) { pos = (int)sm_below(rng, (uint32_t)len); ins = random_insn(rng); }
         else if (kind == 1) { if (len >= 2) pos = (int)sm_below(rng, (uint32_t)(len - 1)); }
         else if (kind == 2) { if (len > 1) { pos = (int)sm_below(rng, (uint32_t)len); nlen = len - 1; } }
         else if (kind == 3) { pos = (int)sm_below(rng, (uint32_t)(len + 1)); ins = random_insn(rng); nlen = len + 1; }
@@ -182,13 +249,30 @@ __global__ void __launch_bounds__(256) k_stoke_epoch(StokeChain* __restrict__ ch
             cand[lane] = v;
         }
         __syncwarp();
-        const int32_t ncost = stoke_cost(cand, nlen, tv, mask, prm.cost_mode, lane, zero);
+        uint32_t ndiff;
+        const int32_t ncost = stoke_cost(cand, nlen, tv, mask, prm.cost_mode, lane, zero, ndiff);
         // Metropolis accept (mcmc.go:51-81)
         const int32_t delta = ncost - cost;
         bool acc = delta <= 0;
         if (!acc && temp > 0.0f) acc = sm_unit(rng) < __expf(-(float)delta / temp);
+        if (acc && prm.traj && delta < 0 && (kind == 0 || kind == 3)) {   // an improving move: training example
+            unsigned long long e = 0;
+            if (lane == 0) e = atomicAdd(&sc->traj, 1ull);
+            e = __shfl_sync(kFull, e, 0);
+            if (e < prm.traj_cap) {
+                m6502_mlp_example& x = prm.traj[e];
+                if (lane < 8) x.target[lane] = lane < (int)tlen ? tg.ins[t0 + lane] : 0;
+                if (lane < 16) x.cand[lane] = lane < len ? cur[lane] : 0;
+                if (lane == 0) {
+                    x.diff = diff; x.tlen = (uint8_t)min(tlen, 8u); x.clen = (uint8_t)len;
+                    x.pos = (uint8_t)pos; x.op = (uint8_t)(ins & 0xFFu); x.imm = (uint8_t)(ins >> 8);
+                    x.weight = 1;
+                }
+            }
+        }
         if (acc) {
             uint16_t* tmp = cur; cur = cand; cand = tmp;
+            diff = ndiff;
             len = nlen;
             cost = ncost;
             accepted++;
@@ -222,7 +306,7 @@ __global__ void __launch_bounds__(256) k_stoke_epoch(StokeChain* __restrict__ ch
         ch.len = (uint8_t)len; ch.best_len = (uint8_t)best_len;
         ch.cost = cost; ch.best_cost = best_cost;
         ch.temp = temp; ch.rng = rng; ch.step = step; ch.since = since;
-        ch.target = t; ch.status = 1;
+        ch.target = t; ch.status = 1; ch.diff = diff;
         ch.accepted += accepted;
         atomicAdd(&sc->accepted, (unsigned long long)accepted);
     }
@@ -300,8 +384,8 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
     if (!cfg || !t_insns || !t_offs || (n_targets && !results)) return set_err(ctx, M6502_E_INVAL, "NULL argument");
     if (cfg->cost > M6502_COST_HAMMING || cfg->sweep > M6502_SWEEP_FULL || cfg->max_len > (uint32_t)kMaxSeq)
         return set_err(ctx, M6502_E_INVAL, "bad STOKE configuration");
-    if (cfg->proposal != M6502_PROPOSAL_UNIFORM)
-        return set_err(ctx, M6502_E_INVAL, "this build has the uniform proposal only");
+    if (cfg->proposal > M6502_PROPOSAL_MIXED || (cfg->proposal == M6502_PROPOSAL_MIXED && !cfg->model))
+        return set_err(ctx, M6502_E_INVAL, "PROPOSAL_MIXED needs a model");
     for (uint32_t t = 0; t < n_targets; t++) {
         uint32_t l = t_offs[t + 1] - t_offs[t];
         if (t_offs[t + 1] < t_offs[t] || l < 1 || l > (uint32_t)kMaxSeq - 2)
@@ -357,6 +441,22 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
     prm.seed = cfg->seed;
     prm.stop_on_proof = cfg->stop_on_proof;
     prm.proven = (const uint32_t*)ctx->st_proven.p;
+    prm.cdf = nullptr;
+    prm.learned_frac = cfg->learned_frac > 0 ? cfg->learned_frac : 0.5f;
+    prm.traj = nullptr;
+    prm.traj_cap = 0;
+    const bool mixed = cfg->proposal == M6502_PROPOSAL_MIXED;
+    if (mixed) {
+        TRY(ensure(ctx, ctx->st_mex, (size_t)n_chains * sizeof(m6502_mlp_example)));
+        TRY(ensure(ctx, ctx->st_probs, (size_t)n_chains * 330 * sizeof(float)));
+        prm.cdf = (const float*)ctx->st_probs.p;
+    }
+    uint64_t traj_total = 0;
+    if (cfg->trajectories && cfg->traj_cap) {
+        prm.traj_cap = std::min<uint64_t>(cfg->traj_cap, 1u << 20);
+        TRY(ensure(ctx, ctx->st_traj, prm.traj_cap * sizeof(m6502_mlp_example)));
+        prm.traj = (m6502_mlp_example*)ctx->st_traj.p;
+    }
     if (cfg->cost == M6502_COST_REF) {
         prm.t_start = 1.0f;
         prm.decay = (float)(cfg->decay > 0.0 && cfg->decay < 1.0 ? cfg->decay : 0.9999);
@@ -382,6 +482,16 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
         prm.steps = e_steps;
         CK(cudaMemsetAsync(sc, 0, sizeof(StokeCounters), ctx->stream));
         CK(cudaEventRecord(ctx->sev[0], ctx->stream));
+        if (mixed) {   // refresh the learned proposal of every chain
+            k_stoke_examples<<<(n_chains + kWarpsPerBlock - 1) / kWarpsPerBlock, 256, 0, ctx->stream>>>(
+                (const StokeChain*)ctx->st_chains.p, n_chains, cpt, tg, (m6502_mlp_example*)ctx->st_mex.p);
+            CKL("k_stoke_examples");
+            int mrc = m6502_mlp_forward_device(cfg->model, (const m6502_mlp_example*)ctx->st_mex.p, n_chains,
+                                               (float*)ctx->st_probs.p, ctx->stream);
+            if (mrc != M6502_OK) return set_err(ctx, mrc, "learned proposal forward pass failed");
+            k_cdf<<<(n_chains + 255) / 256, 256, 0, ctx->stream>>>((float*)ctx->st_probs.p, n_chains);
+            CKL("k_cdf");
+        }
         k_stoke_epoch<<<(n_chains + kWarpsPerBlock - 1) / kWarpsPerBlock, 256, 0, ctx->stream>>>(
             (StokeChain*)ctx->st_chains.p, n_chains, tg, prm, (StokeEntry*)ctx->st_entries.p, ecap, sc);
         CKL("k_stoke_epoch");
@@ -429,6 +539,15 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
         st.candidates += std::min<uint64_t>(hc.entries, ecap);
         st.undecided += hc.undecided;
         if (hc.entries > ecap) return set_err(ctx, M6502_E_NOMEM, "STOKE entry buffer overflowed");
+        if (prm.traj && hc.traj) {   // improving moves of this epoch -> the caller's buffer
+            const uint64_t have = std::min<uint64_t>(hc.traj, prm.traj_cap);
+            const uint64_t room = traj_total < cfg->traj_cap ? cfg->traj_cap - traj_total : 0;
+            const uint64_t take = std::min(have, room);
+            if (take)
+                CK(cudaMemcpyAsync(cfg->trajectories + traj_total, prm.traj, take * sizeof(m6502_mlp_example),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+            traj_total += hc.traj;
+        }
         if (hc.proofs) {
             std::vector<uint32_t> pidx(hc.proofs);
             h_entries.resize(std::min<uint64_t>(hc.entries, ecap));
@@ -487,6 +606,8 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
         }
         r.proofs++;
     }
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (cfg->traj_count) *cfg->traj_count = traj_total;
     if (stats) *stats = st;
     if (n_proofs) *n_proofs = found.size();
     if (proofs && cap) std::memcpy(proofs, found.data(), std::min<uint64_t>(cap, found.size()) * sizeof(m6502_stoke_proof));

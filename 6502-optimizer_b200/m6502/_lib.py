@@ -24,7 +24,7 @@ STATIC_MAX_PAIRS = 1 << 20
 
 SEM_CUDA, SEM_GO = 0, 1
 COST_REF, COST_HAMMING = 0, 1
-PROPOSAL_UNIFORM = 0
+PROPOSAL_UNIFORM, PROPOSAL_MIXED = 0, 1
 SWEEP_REFERENCE, SWEEP_FULL = 0, 1
 EXH_CONES, EXH_BRUTE = 0, 1
 CHECK_QC, CHECK_MID, CHECK_EXH, CHECK_ALL = 1, 2, 4, 7
@@ -76,7 +76,10 @@ class StokeCfg(ctypes.Structure):
                 ("steps", ctypes.c_uint64), ("seed", ctypes.c_uint64), ("decay", ctypes.c_double),
                 ("t_start", ctypes.c_double), ("t_end", ctypes.c_double), ("cost", ctypes.c_uint32),
                 ("max_len", ctypes.c_uint32), ("sweep", ctypes.c_uint32), ("stop_on_proof", ctypes.c_uint32),
-                ("proposal", ctypes.c_uint32), ("dead_flags", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 3)]
+                ("proposal", ctypes.c_uint32), ("dead_flags", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 3),
+                ("learned_frac", ctypes.c_float), ("reserved2", ctypes.c_uint32), ("model", ctypes.c_void_p),
+                ("trajectories", ctypes.c_void_p), ("traj_cap", ctypes.c_uint64),
+                ("traj_count", ctypes.POINTER(ctypes.c_uint64))]
 
 
 class StokeProof(ctypes.Structure):
@@ -104,6 +107,16 @@ class StokeStats(ctypes.Structure):
 assert ctypes.sizeof(StokeProof) == 64 and ctypes.sizeof(StokeResult) == 64
 
 
+class MlpExample(ctypes.Structure):
+    _fields_ = [("target", ctypes.c_uint16 * 8), ("cand", ctypes.c_uint16 * 16), ("diff", ctypes.c_uint32),
+                ("tlen", ctypes.c_uint8), ("clen", ctypes.c_uint8), ("pos", ctypes.c_uint8), ("op", ctypes.c_uint8),
+                ("imm", ctypes.c_uint8), ("weight", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 6)]
+
+
+assert ctypes.sizeof(MlpExample) == 64
+MLP_OUT = 330
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -113,7 +126,9 @@ SYMBOLS = (
     "m6502_check_pairs", "m6502_fingerprint", "m6502_exec_batch", "m6502_search", "m6502_enumerate",
     "m6502_insn_table", "m6502_enumerate_targets", "m6502_draw_targets", "m6502_disasm", "m6502_parse", "m6502_should_prune",
     "m6502_seq_bytes", "m6502_seq_cycles", "m6502_op_deps", "m6502_format_jsonl",
-    "m6502_exhaustive_static", "m6502_stoke_run",
+    "m6502_exhaustive_static", "m6502_stoke_run", "m6502_mlp_param_count", "m6502_mlp_create",
+    "m6502_mlp_destroy", "m6502_mlp_last_error", "m6502_mlp_params", "m6502_mlp_predict", "m6502_mlp_gradients",
+    "m6502_mlp_train", "m6502_gemm_bf16",
 )
 
 
@@ -161,6 +176,18 @@ def lib():
                                          ctypes.c_char_p, ctypes.c_int]
         L.m6502_stoke_run.argtypes = [vp, P(StokeCfg), u16p, u32p, ctypes.c_uint32, P(StokeResult),
                                       P(StokeProof), ctypes.c_uint64, u64p, P(StokeStats)]
+        L.m6502_mlp_param_count.restype = ctypes.c_uint64
+        L.m6502_mlp_create.argtypes = [vp, ctypes.c_uint64, P(vp)]
+        L.m6502_mlp_destroy.argtypes = [vp]
+        L.m6502_mlp_destroy.restype = None
+        L.m6502_mlp_last_error.argtypes = [vp]
+        L.m6502_mlp_last_error.restype = ctypes.c_char_p
+        L.m6502_mlp_params.argtypes = [vp, vp, vp]
+        L.m6502_mlp_predict.argtypes = [vp, P(MlpExample), ctypes.c_uint64, vp]
+        L.m6502_mlp_gradients.argtypes = [vp, P(MlpExample), ctypes.c_uint32, P(ctypes.c_float), vp]
+        L.m6502_mlp_train.argtypes = [vp, P(MlpExample), ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
+                                      ctypes.c_float, ctypes.c_uint64, vp]
+        L.m6502_gemm_bf16.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
         L.m6502_exhaustive_static.argtypes = [ctypes.c_uint64, vp, vp, vp, vp, ctypes.c_uint8, ctypes.c_uint32,
                                               vp, vp]
         _lib = L

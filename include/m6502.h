@@ -76,6 +76,8 @@ enum {
 };
 
 typedef struct m6502_ctx m6502_ctx;
+struct m6502_mlp;
+struct m6502_mlp_example;
 
 typedef struct m6502_opts {
     int32_t device;            /* CUDA device ordinal */
@@ -224,7 +226,11 @@ enum {
     M6502_COST_HAMMING = 1  /* differing output bits over the 32 MidCheck vectors + bytes +
                                cycles/100; T annealed geometrically t_start -> t_end */
 };
-enum { M6502_PROPOSAL_UNIFORM = 0 };
+enum {
+    M6502_PROPOSAL_UNIFORM = 0, /* mutator.go:30-115: uniform opcode / operand / position */
+    M6502_PROPOSAL_MIXED = 1    /* a share (learned_frac) of replace / insert moves drawn from
+                                   the learned model, refreshed at every proof round */
+};
 
 typedef struct m6502_stoke_cfg {
     uint32_t chains_per_target; /* 0 = 128 */
@@ -240,6 +246,13 @@ typedef struct m6502_stoke_cfg {
     uint32_t proposal;          /* M6502_PROPOSAL_* */
     uint8_t dead_flags;         /* stoke --dead-flags */
     uint8_t reserved[3];
+    float learned_frac;         /* PROPOSAL_MIXED: share of replace / insert moves from the model */
+    uint32_t reserved2;
+    struct m6502_mlp *model;    /* PROPOSAL_MIXED: the model (m6502_mlp_create) */
+    struct m6502_mlp_example *trajectories; /* optional HOST buffer: every accepted move that
+                                   lowered the cost (replace / insert) as a labelled example */
+    uint64_t traj_cap;
+    uint64_t *traj_count;       /* out: moves recorded (may exceed traj_cap) */
 } m6502_stoke_cfg;
 
 typedef struct m6502_stoke_proof {
@@ -280,6 +293,49 @@ int m6502_stoke_run(m6502_ctx *ctx, const m6502_stoke_cfg *cfg, const uint16_t *
                     const uint32_t *t_offs, uint32_t n_targets, m6502_stoke_result *results,
                     m6502_stoke_proof *proofs, uint64_t cap, uint64_t *n_proofs,
                     m6502_stoke_stats *stats);
+
+/* ---- learned proposal: a BF16 MLP on the tcgen05 tensor cores ----
+ * No counterpart in the reference: a small network that
+ * proposes STOKE moves.  Input: target and current candidate (embedded), the
+ * mask of MidCheck vectors on which they differ, their lengths.  Output:
+ * softmax over the position (16), opcode (58) and operand (256) of the next
+ * replace / insert move.  Trained on the device by this library's own forward
+ * and backward kernels.  ExhaustiveCheck alone decides equivalence: the model
+ * changes which candidates are tried, never a verdict. */
+typedef struct m6502_mlp m6502_mlp;
+#define M6502_MLP_OUT 330   /* probabilities per example: 16 + 58 + 256 */
+
+typedef struct m6502_mlp_example {
+    uint16_t target[8];     /* target instructions (tlen used) */
+    uint16_t cand[16];      /* current candidate (clen used) */
+    uint32_t diff;          /* bit v: candidate and target differ on MidCheck vector v */
+    uint8_t tlen, clen;     /* 1..8, 0..16 */
+    uint8_t pos, op, imm;   /* label: position, opcode and operand of the move */
+    uint8_t weight;         /* loss weight; 0 = unlabelled */
+    uint8_t reserved[6];
+} m6502_mlp_example;        /* 64 bytes */
+
+uint64_t m6502_mlp_param_count(void);
+int m6502_mlp_create(m6502_ctx *ctx, uint64_t seed, m6502_mlp **out);
+void m6502_mlp_destroy(m6502_mlp *mlp);
+const char *m6502_mlp_last_error(const m6502_mlp *mlp);
+/* Reads (out) and / or writes (in) all parameters, fp32, in the fixed order
+ * E_T[2863x128] P_T[8x128] E_C[2863x128] P_C[16x128] W1[512x320] b1[512]
+ * W2[512x512] b2 W3[512x512] b3 W4[384x512] b4[384] (W: rows = outputs). */
+int m6502_mlp_params(m6502_mlp *mlp, float *out, const float *in);
+/* probs: n x M6502_MLP_OUT. */
+int m6502_mlp_predict(m6502_mlp *mlp, const m6502_mlp_example *ex, uint64_t n, float *probs);
+/* Loss (weighted mean cross-entropy of the three heads; the operand head
+ * only for opcodes with an immediate) and its gradient for one batch of n
+ * <= 65,536 examples; grads: m6502_mlp_param_count() floats. */
+int m6502_mlp_gradients(m6502_mlp *mlp, const m6502_mlp_example *ex, uint32_t n, float *loss, float *grads);
+/* Adam on minibatches of `batch` (multiple of 128) examples sampled from ex. */
+int m6502_mlp_train(m6502_mlp *mlp, const m6502_mlp_example *ex, uint64_t n, uint32_t steps, uint32_t batch,
+                    float lr, uint64_t seed, float *loss_history);
+/* C[M x N] fp32 = A[M x K] . B[N x K]^T on the tensor cores; A, B bf16
+ * row-major DEVICE pointers, K a multiple of 64.  (The MLP's GEMM, exposed
+ * for testing.) */
+int m6502_gemm_bf16(m6502_ctx *ctx, int M, int N, int K, const void *A, const void *B, float *C);
 
 /* ---- host helpers (no GPU needed) ---- */
 /* The 2863 instructions in CUDA order (cuda/6502_search_v2.cu:741-752) or Go
