@@ -23,6 +23,10 @@
 //                   semantics: first candidate in Go order per target).
 #include <cuda_runtime.h>
 
+#include <cub/block/block_reduce.cuh>
+#include <cub/block/block_scan.cuh>
+#include <cub/device/device_radix_sort.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -132,6 +136,19 @@ uint32_t sweep_locs_of_reads(uint32_t reads) {
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ uint64_t fp_of(const St& s) {
     return pack(s) & ~((uint64_t)(~kPMask & 0xFFu) << 24);   // P & PMask
+}
+
+// Join key of a sequence: a 64-bit hash of its 8 QuickCheck outputs under
+// the run's mask.  Pairs passing QuickCheck have equal keys; equal keys are
+// re-checked vector by vector, so a hash collision costs only time.
+__host__ __device__ __forceinline__ uint64_t key_mix(uint64_t z) {
+    z ^= z >> 33; z *= 0xFF51AFD7ED558CCDull;
+    z ^= z >> 33; z *= 0xC4CEB9FE1A85EC53ull;
+    z ^= z >> 33;
+    return z;
+}
+__host__ __device__ __forceinline__ uint64_t key_step(uint64_t h, uint64_t masked_out, int v) {
+    return key_mix(h ^ (masked_out + (uint64_t)(v + 1) * 0x9E3779B97F4A7C15ull));
 }
 
 // Survivor record: target (index within the pass) and candidate code:
@@ -411,6 +428,82 @@ __device__ Groups make_groups(const Flow& fl, uint32_t dead, bool rep, bool brut
     return g;
 }
 
+// The same composition reading the dependency table from shared memory
+// (13 lanes read 13 different entries: constant memory would serialise).
+__device__ __forceinline__ uint32_t compose_s(uint32_t D, const uint16_t* seq, int n, int lane, uint32_t& written,
+                                              uint32_t& sweep, const uint16_t (*dep_tab)[NUM_LOCS]) {
+    for (int i = 0; i < n; i++) {
+        uint32_t op = seq[i] & 0xFFu;
+        uint32_t dep = (lane < NUM_LOCS) ? dep_tab[op][lane] : 0u;
+        uint32_t nd = 0;
+#pragma unroll
+        for (int l = 0; l < NUM_LOCS; l++) {
+            uint32_t x = __shfl_sync(kFull, D, l);
+            if (dep & (1u << l)) nd |= x;
+        }
+        D = nd;
+        written |= c_wr[op];
+        sweep |= c_sweep[op];
+    }
+    return D;
+}
+
+__device__ __forceinline__ Flow dataflow_s(const PairView& pv, int lane, const uint16_t (*dep_tab)[NUM_LOCS]) {
+    Flow fl;
+    uint32_t wt = 0, wc = 0, sw = 0;
+    uint32_t id = (lane < NUM_LOCS) ? (1u << lane) : 0u;
+    uint32_t dt = compose_s(id, pv.t, pv.tn, lane, wt, sw, dep_tab);
+    uint32_t dc = compose_s(id, pv.c, pv.cn, lane, wc, sw, dep_tab);
+    fl.k = __popc(sw);
+    fl.swept = sw | LB(L_A) | LB(L_C);
+    fl.written = wt | wc;
+    fl.cone = (dt | dc) & fl.swept;
+    return fl;
+}
+
+// Lane-distributed groups: lane o (< 13) keeps the cone of output o; the
+// maximal cones are found with shuffles and visited smallest first with warp
+// reductions, so no per-thread arrays (local memory) are needed.
+struct LaneGroups {
+    uint32_t my;        // this lane's cone (0 when its output is not compared)
+    uint32_t active;    // compared outputs (uniform)
+    uint32_t maxm;      // outputs whose cone is maximal (uniform)
+    uint32_t mybits;    // this lane's sweep bits when maximal
+};
+
+__device__ __forceinline__ LaneGroups lane_groups(const Flow& fl, uint32_t dead, bool rep, int lane) {
+    LaneGroups g;
+    uint32_t deadlocs = 0;
+    for (uint32_t l = L_C; l <= L_N; l++) if (dead & flag_bit(l)) deadlocs |= LB(l);
+    g.active = fl.written & ~deadlocs;
+    const bool act = lane < NUM_LOCS && ((g.active >> lane) & 1u);
+    g.my = act ? fl.cone : 0u;
+    bool ismax = act;
+#pragma unroll
+    for (int q = 0; q < NUM_LOCS; q++) {
+        const uint32_t cq = __shfl_sync(kFull, g.my, q);
+        if (((g.active >> q) & 1u) && q != lane && (cq & g.my) == g.my && (cq != g.my || q < lane)) ismax = false;
+    }
+    g.maxm = __ballot_sync(kFull, ismax);
+    g.mybits = ismax ? cone_bits(g.my, rep) : 0xFFu;
+    return g;
+}
+
+// Next group (smallest sweep first) of `remaining`: its output lane, bits,
+// cone and compare mask (outputs whose cone it contains).
+__device__ __forceinline__ void next_group(const LaneGroups& g, uint32_t remaining, int lane, int& o, uint32_t& bits,
+                                           uint32_t& cone, uint64_t& mask) {
+    const uint32_t key = ((remaining >> lane) & 1u) ? ((g.mybits << 5) | (uint32_t)lane) : 0xFFFFFFFFu;
+    const uint32_t kmin = __reduce_min_sync(kFull, key);
+    o = (int)(kmin & 31u);
+    bits = kmin >> 5;
+    cone = __shfl_sync(kFull, g.my, o);
+    const bool act = lane < NUM_LOCS && ((g.active >> lane) & 1u);
+    const uint64_t contrib = (act && (g.my & cone) == g.my) ? loc_mask64((uint32_t)lane) : 0ull;
+    const uint32_t lo = __reduce_or_sync(kFull, (uint32_t)contrib), hi = __reduce_or_sync(kFull, (uint32_t)(contrib >> 32));
+    mask = (uint64_t)lo | ((uint64_t)hi << 32);
+}
+
 struct ExhArgs {
     uint32_t* fail;              // per pair: 1 = not equivalent
     Item* items;
@@ -617,14 +710,15 @@ __global__ void __launch_bounds__(256) k_qc1(const uint64_t* __restrict__ tfp, c
 }
 
 // QC (+ MidCheck) of targets x all length-1 candidates as an exact join:
-// the non-pruned candidates sorted by masked vector-0 output (skeys/sidx,
-// built per dead-flags mask) sit in shared memory; a warp takes one target,
-// binary-searches its masked vector-0 output, and checks only the
-// candidates with an equal key -- the only ones a QuickCheck can pass, since
-// vector 0 is one of its 8 vectors.  Same survivors as k_qc1.
+// the non-pruned candidates sorted by the hash of their 8 masked QuickCheck
+// outputs (skeys/sidx, built per dead-flags mask) sit in shared memory; a
+// warp takes one target, binary-searches its own key and checks only the
+// candidates with an equal key -- a superset of those QuickCheck passes.
+// Lane v checks vector v from the candidate-major fingerprints (cfp_cm,
+// 256 contiguous bytes per candidate).  Same survivors as k_qc1.
 template <bool GO>
 __global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tfp, const uint8_t* __restrict__ tmeta,
-                                                  uint32_t nt, const uint64_t* __restrict__ cfp,
+                                                  uint32_t nt, const uint64_t* __restrict__ cfp_cm,
                                                   const uint8_t* __restrict__ cmeta, const uint64_t* __restrict__ skeys,
                                                   const uint16_t* __restrict__ sidx, uint32_t nsorted, uint32_t dead,
                                                   uint32_t stages, Surv* __restrict__ surv, uint64_t cap,
@@ -647,7 +741,9 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tf
     for (uint32_t t = blockIdx.x * kWarpsPerBlock + w; t < nt; t += gridDim.x * kWarpsPerBlock) {
         const uint64_t* trow = tfp + (uint64_t)t * 32;
         const uint64_t tv = trow[lane];   // lane v holds the target's output on vector v
-        const uint64_t key = __shfl_sync(kFull, tv, 0) & loose;
+        uint64_t key = 0x6502;
+#pragma unroll
+        for (int v = 0; v < 8; v++) key = key_step(key, __shfl_sync(kFull, tv, v) & loose, v);
         uint32_t lo = 0, hi = nsorted;            // lower bound of key
         while (lo < hi) {
             uint32_t mid = (lo + hi) >> 1;
@@ -662,7 +758,7 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tf
             const uint32_t cm = s_meta[c];
             const uint32_t cb = GO ? ((cm >> 2) & 3u) : (cm & 3u);
             if ((cm & 0x10u) || cb >= tb) continue;          // pruned or not shorter (uniform)
-            const uint64_t x = tv ^ cfp[(uint64_t)lane * kNumInsns + c];
+            const uint64_t x = tv ^ cfp_cm[(uint64_t)c * 32 + lane];   // one coalesced 256-byte row
             const unsigned lo_eq = __ballot_sync(kFull, (x & loose) == 0);
             const unsigned ex_eq = __ballot_sync(kFull, (x & exact) == 0);
             if ((lo_eq & 0xFFu) != 0xFFu) continue;          // QuickCheck fails
@@ -701,6 +797,9 @@ template <class Src>
 __global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long long* n_pairs_ptr,
                                                      uint64_t n_cap, ExhArgs a) {
     __shared__ uint16_t s_t[kWarpsPerBlock][kMaxSeq], s_c[kWarpsPerBlock][kMaxSeq];
+    __shared__ uint16_t s_dep[NUM_OPS][NUM_LOCS];
+    for (int i = threadIdx.x; i < NUM_OPS * NUM_LOCS; i += blockDim.x) (&s_dep[0][0])[i] = (&c_dep[0][0])[i];
+    __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t n = min((uint64_t)*n_pairs_ptr, n_cap);
     unsigned long long nstates = 0, probe_rej = 0;
@@ -729,38 +828,51 @@ __global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long
                 continue;
             }
         }
-        Flow fl = dataflow(pv, lane);
+        Flow fl = dataflow_s(pv, lane, s_dep);
         const bool rep = a.sweep == M6502_SWEEP_REFERENCE && fl.k >= 3;
-        Groups g = make_groups(fl, pv.dead, rep, a.brute != 0, lane);
-        bool too_big = false;
-        for (int i = 0; i < g.n; i++) too_big = too_big || g.bits[i] > kMaxConeBits;
+        LaneGroups lg;
+        if (a.brute) {   // one group: the whole product space, every output
+            lg.active = 0; lg.my = 0; lg.maxm = 1u; lg.mybits = 0;
+        } else {
+            lg = lane_groups(fl, pv.dead, rep, lane);
+        }
+        const uint32_t brute_bits = cone_bits(fl.swept, rep);
+        const bool too_big = a.brute ? brute_bits > kMaxConeBits
+                                     : __any_sync(kFull, ((lg.maxm >> lane) & 1u) && lg.mybits > kMaxConeBits);
         if (too_big) {
             if (lane == 0) a.fail[p] = 3u;   // undecided: sweep beyond the cap
             __syncwarp();
             continue;
         }
         bool ok = true;
-        uint32_t big = 0;   // groups left for the work queue
-        for (int i = 0; i < g.n && ok; i++) {
-            Fields f = make_fields(g.cone[i], fl.swept, rep);
-            uint64_t total = 1ull << g.bits[i];
-            uint64_t end = total <= kSmallSweep ? total : kProbe;
-            ok = sweep_states(pv, f, g.mask[i], 0, end, nullptr, &nstates, lane);
-            if (ok && end < total) big |= 1u << i;
+        uint32_t big = 0;   // groups (by output lane) left for the work queue
+        for (uint32_t rem = lg.maxm; rem && ok;) {
+            int o; uint32_t bits, cone; uint64_t mask;
+            if (a.brute) { o = 0; bits = brute_bits; cone = fl.swept; mask = cmp_mask(pv.dead); }
+            else next_group(lg, rem, lane, o, bits, cone, mask);
+            rem &= ~(1u << o);
+            Fields f = make_fields(cone, fl.swept, rep);
+            const uint64_t total = 1ull << bits;
+            const uint64_t end = total <= kSmallSweep ? total : kProbe;
+            ok = sweep_states(pv, f, mask, 0, end, nullptr, &nstates, lane);
+            if (ok && end < total) big |= 1u << o;
         }
         if (ok && big) {
-            for (int i = 0; i < g.n; i++) {
-                if (!(big & (1u << i))) continue;
-                uint64_t total = 1ull << g.bits[i];
-                uint64_t nitems = (total - kProbe + kChunk - 1) / kChunk;
+            for (uint32_t rem = big; rem;) {
+                int o; uint32_t bits, cone; uint64_t mask;
+                if (a.brute) { o = 0; bits = brute_bits; cone = fl.swept; mask = cmp_mask(pv.dead); }
+                else next_group(lg, rem, lane, o, bits, cone, mask);
+                rem &= ~(1u << o);
+                const uint64_t total = 1ull << bits;
+                const uint64_t nitems = (total - kProbe + kChunk - 1) / kChunk;
                 unsigned long long base = 0;
                 if (lane == 0) base = atomicAdd(&a.cnt->items, (unsigned long long)nitems);
                 base = __shfl_sync(kFull, base, 0);
                 for (uint64_t j = lane; j < nitems; j += 32) {
                     if (base + j >= a.item_cap) break;
                     Item it;
-                    it.pair = (uint32_t)p; it.cone = g.cone[i]; it.rep = rep ? 1 : 0; it.pad = 0;
-                    it.outmask = g.mask[i];
+                    it.pair = (uint32_t)p; it.cone = (uint16_t)cone; it.rep = rep ? 1 : 0; it.pad = 0;
+                    it.outmask = mask;
                     it.start = kProbe + j * kChunk;
                     it.count = min(kChunk, total - it.start);
                     a.items[base + j] = it;
@@ -777,6 +889,9 @@ __global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long
 template <class Src>
 __global__ void __launch_bounds__(256) k_exh_items(Src src, ExhArgs a) {
     __shared__ uint16_t s_t[kWarpsPerBlock][kMaxSeq], s_c[kWarpsPerBlock][kMaxSeq];
+    __shared__ uint16_t s_dep[NUM_OPS][NUM_LOCS];
+    for (int i = threadIdx.x; i < NUM_OPS * NUM_LOCS; i += blockDim.x) (&s_dep[0][0])[i] = (&c_dep[0][0])[i];
+    __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t n = min((uint64_t)a.cnt->items, a.item_cap);
     unsigned long long nstates = 0;
@@ -793,7 +908,7 @@ __global__ void __launch_bounds__(256) k_exh_items(Src src, ExhArgs a) {
         pv.t = s_t[w]; pv.c = s_c[w];
         src.load(it.pair, s_t[w], s_c[w], pv.tn, pv.cn, pv.dead, lane);
         __syncwarp();
-        Flow fl = dataflow(pv, lane);
+        Flow fl = dataflow_s(pv, lane, s_dep);
         Fields f = make_fields(it.cone, fl.swept, it.rep != 0);
         bool ok = sweep_states(pv, f, it.outmask, it.start, it.start + it.count, flag, &nstates, lane);
         if (!ok && lane == 0) *flag = 1u;
@@ -1105,11 +1220,14 @@ struct m6502_ctx {
         cins, coffs, pout, pfd, enum_count;
     std::vector<m6502_rule> staging;
     std::vector<uint64_t> h_cfp0;     // vector-0 outputs of the length-1 candidates (host copy)
+    std::vector<uint64_t> h_cfp8;     // QC-vector outputs [8][2863] (host copy)
+    DevBuf cfp1cm;                    // candidate-major fingerprints [2863][32]
     std::vector<uint8_t> h_cmeta;
     DevBuf join_keys[256], join_idx[256];
     uint32_t join_n[256] = {};
     DevBuf st_tins, st_toffs, st_tout, st_tbytes, st_chains, st_entries, st_vidx, st_proven, st_cnt, st_pidx,
         st_mex, st_probs, st_traj;
+    DevBuf st_keys, st_keys2, st_vals2, st_rep, st_ord, st_verdict, st_vlist, st_vpos, st_sort_tmp;
 };
 
 namespace {
@@ -1208,6 +1326,9 @@ int init_ctx(m6502_ctx* ctx) {
         meta[c] = (uint8_t)(bytes_cuda(op) | (bytes_go(op) << 2) | (should_prune(&one, 1) ? 0x10 : 0));
     }
     ctx->h_cfp0.assign(tr.begin(), tr.begin() + kNumInsns);
+    ctx->h_cfp8.assign(tr.begin(), tr.begin() + 8 * (size_t)kNumInsns);
+    TRY(ensure(ctx, ctx->cfp1cm, sizeof(uint64_t) * 32 * kNumInsns));
+    CK(cudaMemcpyAsync(ctx->cfp1cm.p, h.data(), h.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
     ctx->h_cmeta = meta;
     CK(cudaMemcpyAsync(ctx->cfp1.p, tr.data(), tr.size() * 8, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaMemcpyAsync(ctx->cmeta1.p, meta.data(), meta.size(), cudaMemcpyHostToDevice, ctx->stream));
@@ -1217,14 +1338,18 @@ int init_ctx(m6502_ctx* ctx) {
     return M6502_OK;
 }
 
-// Sorted (masked vector-0 output, candidate) table of the non-pruned
-// length-1 candidates for one dead-flags mask, built once per mask.
+// Sorted (QuickCheck key, candidate) table of the non-pruned length-1
+// candidates for one dead-flags mask, built once per mask.
 int join_table(m6502_ctx* ctx, uint32_t dead) {
     if (ctx->join_n[dead]) return M6502_OK;
     const uint64_t loose = cmp_mask(dead);
     std::vector<std::pair<uint64_t, uint16_t>> v;
-    for (int c = 0; c < kNumInsns; c++)
-        if (!(ctx->h_cmeta[c] & 0x10)) v.emplace_back(ctx->h_cfp0[c] & loose, (uint16_t)c);
+    for (int c = 0; c < kNumInsns; c++) {
+        if (ctx->h_cmeta[c] & 0x10) continue;
+        uint64_t key = 0x6502;
+        for (int q = 0; q < 8; q++) key = key_step(key, ctx->h_cfp8[(size_t)q * kNumInsns + c] & loose, q);
+        v.emplace_back(key, (uint16_t)c);
+    }
     std::sort(v.begin(), v.end());
     std::vector<uint64_t> keys(v.size());
     std::vector<uint16_t> idx(v.size());
@@ -1275,12 +1400,12 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             const uint16_t* ji = (const uint16_t*)ctx->join_idx[dead].p;
             if (go)
                 k_qc_join<true><<<jgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
-                                                                (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
+                                                                (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p,
                                                                 (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
                                                                 dead, stages, (Surv*)ctx->surv.p, scap, cnt);
             else
                 k_qc_join<false><<<jgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
-                                                                 (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
+                                                                 (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p,
                                                                  (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
                                                                  dead, stages, (Surv*)ctx->surv.p, scap, cnt);
         } else if (go)
@@ -1449,12 +1574,14 @@ void m6502_destroy(m6502_ctx* ctx) {
         if (ctx->join_keys[i].p) cudaFree(ctx->join_keys[i].p);
         if (ctx->join_idx[i].p) cudaFree(ctx->join_idx[i].p);
     }
-    DevBuf* bufs[] = {&ctx->cfp1, &ctx->cmeta1, &ctx->targets, &ctx->ids, &ctx->tfp, &ctx->tmeta,
+    DevBuf* bufs[] = {&ctx->cfp1cm, &ctx->cfp1, &ctx->cmeta1, &ctx->targets, &ctx->ids, &ctx->tfp, &ctx->tmeta,
                       &ctx->surv, &ctx->fail, &ctx->items, &ctx->rules, &ctx->cnt, &ctx->best,
                       &ctx->pins, &ctx->poffs, &ctx->cins, &ctx->coffs, &ctx->pout, &ctx->pfd,
                       &ctx->enum_count, &ctx->st_tins, &ctx->st_toffs, &ctx->st_tout, &ctx->st_tbytes,
                       &ctx->st_chains, &ctx->st_entries, &ctx->st_vidx, &ctx->st_proven, &ctx->st_cnt,
-                      &ctx->st_pidx, &ctx->st_mex, &ctx->st_probs, &ctx->st_traj};
+                      &ctx->st_pidx, &ctx->st_mex, &ctx->st_probs, &ctx->st_traj, &ctx->st_keys,
+                      &ctx->st_keys2, &ctx->st_vals2, &ctx->st_rep, &ctx->st_ord, &ctx->st_verdict,
+                      &ctx->st_vlist, &ctx->st_vpos, &ctx->st_sort_tmp};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);

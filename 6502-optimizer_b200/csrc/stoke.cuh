@@ -38,7 +38,29 @@ struct StokeEntry {        // a shorter zero-cost best awaiting proof
 
 struct StokeCounters {
     unsigned long long entries, vec_ok, proofs, undecided, accepted, traj;
+    unsigned long long reps;      // distinct (target, candidate) pairs among the vec_ok entries
+    unsigned long long max_ord;   // largest per-target ordinal of a distinct pair
+    unsigned long long round_n;   // pairs verified in the current round
+    unsigned long long verified;  // pairs verified this epoch (all rounds)
 };
+
+constexpr uint32_t kVerifyBatch = 8;   // distinct candidates per target per round under stop_on_proof
+
+// Sort key of an entry: target, length, then a 33-bit hash of the
+// instructions, so that identical (target, candidate) pairs are adjacent and
+// shorter candidates of a target come first.
+__device__ __forceinline__ uint64_t entry_key(const StokeEntry& e) {
+    uint64_t h = 0x5EED;
+    for (int i = 0; i < e.len; i++) h = key_mix(h ^ ((uint64_t)e.ins[i] + (uint64_t)(i + 1) * 0x9E3779B97F4A7C15ull));
+    return ((uint64_t)e.target << 38) | ((uint64_t)(e.len & 31u) << 33) | (h >> 31);
+}
+
+__device__ __forceinline__ bool same_candidate(const StokeEntry& a, const StokeEntry& b) {
+    if (a.target != b.target || a.len != b.len) return false;
+    for (int i = 0; i < a.len; i++)
+        if (a.ins[i] != b.ins[i]) return false;
+    return true;
+}
 
 struct StokeTargets {
     const uint16_t* ins;
@@ -314,9 +336,11 @@ __global__ void __launch_bounds__(256) k_stoke_epoch(StokeChain* __restrict__ ch
 
 // All 32 test vectors of each entry (a shorter zero-cost best): entries
 // that agree on every vector go on to ExhaustiveCheck (their indices are
-// compacted into vidx); FlagDiff over the QC vectors is recorded for masked runs.
+// compacted into vidx, with their sort keys); FlagDiff over the QC vectors is
+// recorded for masked runs.
 __global__ void k_stoke_vectors(StokeEntry* __restrict__ entries, uint64_t ecap, StokeTargets tg, uint32_t dead,
-                                uint32_t* __restrict__ vidx, StokeCounters* __restrict__ sc) {
+                                uint32_t* __restrict__ vidx, uint64_t* __restrict__ keys,
+                                StokeCounters* __restrict__ sc) {
     const int lane = threadIdx.x & 31;
     const uint64_t n = min((uint64_t)sc->entries, ecap);
     const uint64_t mask = cmp_mask(dead);
@@ -331,7 +355,11 @@ __global__ void k_stoke_vectors(StokeEntry* __restrict__ entries, uint64_t ecap,
         fd = __reduce_or_sync(kFull, fd);
         if (lane == 0) {
             en.dead_flags = (uint8_t)(dead ? fd : 0u);   // FlagDiff (verifier.go:591-604)
-            if (ok) vidx[atomicAdd(&sc->vec_ok, 1ull)] = (uint32_t)e;
+            if (ok) {
+                const unsigned long long k = atomicAdd(&sc->vec_ok, 1ull);
+                vidx[k] = (uint32_t)e;
+                keys[k] = entry_key(en);
+            }
         }
     }
 }
@@ -354,20 +382,104 @@ struct StokeSource {
     }
 };
 
-// Proven entries become proofs; their chains restart (search.go:151-154) and
-// their targets are marked proven.
-__global__ void k_stoke_collect(const StokeEntry* __restrict__ entries, const uint32_t* __restrict__ vidx,
-                                const uint32_t* __restrict__ fail, StokeCounters* __restrict__ sc,
-                                StokeChain* __restrict__ chains, uint32_t* __restrict__ proven,
+// Over the vec_ok entries sorted by key (one CTA, chunks of 1,024): rep[i] =
+// sorted position of the first entry with the same (target, candidate) --
+// the one that is verified for all of them -- and ord[i] = the ordinal of
+// that distinct candidate within its target (0 for the shortest).
+__global__ void __launch_bounds__(1024) k_stoke_dedupe(const uint64_t* __restrict__ keys,
+                                                       const uint32_t* __restrict__ vals,
+                                                       const StokeEntry* __restrict__ entries,
+                                                       uint32_t* __restrict__ rep, uint32_t* __restrict__ ord,
+                                                       StokeCounters* __restrict__ sc) {
+    using Scan = cub::BlockScan<uint32_t, 1024>;
+    using Reduce = cub::BlockReduce<uint32_t, 1024>;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ typename Reduce::TempStorage rtmp;
+    __shared__ uint32_t carry[3];   // running count of distinct pairs, last rep position, count at target start
+    const uint32_t n = (uint32_t)sc->vec_ok;
+    if (threadIdx.x == 0) carry[0] = carry[1] = carry[2] = 0;
+    __syncthreads();
+    uint32_t max_ord = 0;
+    for (uint32_t base = 0; base < n; base += 1024) {
+        const uint32_t i = base + threadIdx.x;
+        const bool valid = i < n;
+        bool is_rep = false, tstart = false;
+        if (valid) {
+            if (i == 0) is_rep = tstart = true;
+            else {
+                const uint64_t k = keys[i], kp = keys[i - 1];
+                tstart = (k >> 38) != (kp >> 38);
+                is_rep = tstart || k != kp || !same_candidate(entries[vals[i]], entries[vals[i - 1]]);
+            }
+        }
+        uint32_t r, rp, rs;
+        Scan(tmp).InclusiveSum(is_rep ? 1u : 0u, r);
+        __syncthreads();
+        r += carry[0];
+        Scan(tmp).InclusiveScan(is_rep ? i : 0u, rp, cub::Max());
+        __syncthreads();
+        rp = max(rp, carry[1]);
+        Scan(tmp).InclusiveScan(tstart ? r : 0u, rs, cub::Max());
+        __syncthreads();
+        rs = max(rs, carry[2]);
+        if (valid) {
+            rep[i] = rp;
+            ord[i] = r - rs;
+            max_ord = max(max_ord, r - rs);
+        }
+        __syncthreads();
+        if (threadIdx.x == 1023) { carry[0] = r; carry[1] = rp; carry[2] = rs; }
+        __syncthreads();
+    }
+    const uint32_t m = Reduce(rtmp).Reduce(max_ord, cub::Max());
+    if (threadIdx.x == 0) { sc->reps = carry[0]; sc->max_ord = m; }
+}
+
+// One verification round: the distinct pairs whose per-target ordinal lies
+// in [lo, hi), skipping targets already proved when stop_on_proof is set.
+__global__ void k_stoke_select(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
+                               const uint32_t* __restrict__ rep, const uint32_t* __restrict__ ord, uint32_t lo,
+                               uint32_t hi, uint32_t stop_on_proof, const uint32_t* __restrict__ proven,
+                               uint32_t* __restrict__ vlist, uint32_t* __restrict__ vpos,
+                               StokeCounters* __restrict__ sc) {
+    const uint32_t n = (uint32_t)sc->vec_ok;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (rep[i] != i || ord[i] < lo || ord[i] >= hi) continue;
+        if (stop_on_proof && proven[(uint32_t)(keys[i] >> 38)]) continue;
+        const unsigned long long p = atomicAdd(&sc->round_n, 1ull);
+        vlist[p] = vals[i];
+        vpos[p] = i;
+    }
+}
+
+// Verdicts of a round -> the sorted positions of the verified pairs; proved
+// targets are marked.
+__global__ void k_stoke_verdicts(const uint32_t* __restrict__ fail, const uint32_t* __restrict__ vpos,
+                                 const uint64_t* __restrict__ keys, uint32_t* __restrict__ verdict,
+                                 uint32_t* __restrict__ proven, StokeCounters* __restrict__ sc) {
+    const uint32_t n = (uint32_t)sc->round_n;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
+        const uint32_t i = vpos[p];
+        verdict[i] = fail[p];
+        if (fail[p] == 0) proven[(uint32_t)(keys[i] >> 38)] = 1;
+        if (fail[p] == 3) atomicAdd(&sc->undecided, 1ull);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->verified += n;
+}
+
+// Every vec_ok entry whose distinct pair was proved becomes a proof (as in
+// the reference, each chain's verified best is one result); its chain
+// restarts (search.go:151-154).
+__global__ void k_stoke_collect(const uint32_t* __restrict__ vals, const uint32_t* __restrict__ rep,
+                                const uint32_t* __restrict__ verdict, const StokeEntry* __restrict__ entries,
+                                StokeCounters* __restrict__ sc, StokeChain* __restrict__ chains,
                                 uint32_t* __restrict__ proof_idx, uint64_t pcap) {
-    const uint64_t n = sc->vec_ok;
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
-        if (fail[p] == 3) { atomicAdd(&sc->undecided, 1ull); continue; }
-        if (fail[p] != 0) continue;
-        const uint32_t e = vidx[p];
-        unsigned long long k = atomicAdd(&sc->proofs, 1ull);
+    const uint32_t n = (uint32_t)sc->vec_ok;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (verdict[rep[i]] != 0) continue;
+        const uint32_t e = vals[i];
+        const unsigned long long k = atomicAdd(&sc->proofs, 1ull);
         if (k < pcap) proof_idx[k] = e;
-        proven[entries[e].target] = 1;
         chains[entries[e].chain].status = 0;
     }
 }
@@ -429,6 +541,18 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
     TRY(ensure(ctx, ctx->st_proven, (size_t)n_targets * 4));
     TRY(ensure(ctx, ctx->st_cnt, sizeof(StokeCounters)));
     TRY(ensure(ctx, ctx->st_pidx, ecap * 4));
+    TRY(ensure(ctx, ctx->st_keys, ecap * 8));
+    TRY(ensure(ctx, ctx->st_keys2, ecap * 8));
+    TRY(ensure(ctx, ctx->st_vals2, ecap * 4));
+    TRY(ensure(ctx, ctx->st_rep, ecap * 4));
+    TRY(ensure(ctx, ctx->st_ord, ecap * 4));
+    TRY(ensure(ctx, ctx->st_verdict, ecap * 4));
+    TRY(ensure(ctx, ctx->st_vlist, ecap * 4));
+    TRY(ensure(ctx, ctx->st_vpos, ecap * 4));
+    size_t sort_bytes = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const uint64_t*)nullptr, (uint64_t*)nullptr,
+                                       (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)ecap, 0, 64, ctx->stream));
+    TRY(ensure(ctx, ctx->st_sort_tmp, sort_bytes + 256));
     CK(cudaMemsetAsync(ctx->st_chains.p, 0, (size_t)n_chains * sizeof(StokeChain), ctx->stream));
     CK(cudaMemsetAsync(ctx->st_proven.p, 0, (size_t)n_targets * 4, ctx->stream));
     StokeTargets tg{(const uint16_t*)ctx->st_tins.p, (const uint32_t*)ctx->st_toffs.p,
@@ -497,31 +621,73 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
         CKL("k_stoke_epoch");
         CK(cudaEventRecord(ctx->sev[1], ctx->stream));
         k_stoke_vectors<<<ctx->sms * 8, 256, 0, ctx->stream>>>((StokeEntry*)ctx->st_entries.p, ecap, tg,
-                                                               cfg->dead_flags, (uint32_t*)ctx->st_vidx.p, sc);
+                                                               cfg->dead_flags, (uint32_t*)ctx->st_vidx.p,
+                                                               (uint64_t*)ctx->st_keys.p, sc);
         CKL("k_stoke_vectors");
-        StokeSource src{(const StokeEntry*)ctx->st_entries.p, (const uint32_t*)ctx->st_vidx.p, tg, cfg->dead_flags};
-        for (int attempt = 0;; attempt++) {
-            TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
-            CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), ctx->stream));
-            ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg->sweep, 0};
-            k_exhaustive<StokeSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &sc->vec_ok, ecap, ea);
-            CKL("k_exhaustive(stoke)");
-            k_exh_items<StokeSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
-            CKL("k_exh_items(stoke)");
-            unsigned long long items = 0;
-            CK(cudaMemcpyAsync(&items, &cnt->items, sizeof items, cudaMemcpyDeviceToHost, ctx->stream));
+        // Identical (target, candidate) pairs are verified once: sort by key,
+        // pick one representative per pair, number the distinct candidates of
+        // each target.
+        StokeCounters hv;
+        CK(cudaMemcpyAsync(&hv, sc, sizeof hv, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        const uint32_t n_ok = (uint32_t)hv.vec_ok;
+        uint32_t max_ord = 0;
+        if (n_ok) {
+            size_t sort_bytes = ctx->st_sort_tmp.bytes;
+            CK(cub::DeviceRadixSort::SortPairs(ctx->st_sort_tmp.p, sort_bytes, (const uint64_t*)ctx->st_keys.p,
+                                               (uint64_t*)ctx->st_keys2.p, (const uint32_t*)ctx->st_vidx.p,
+                                               (uint32_t*)ctx->st_vals2.p, (int)n_ok, 0, 64, ctx->stream));
+            k_stoke_dedupe<<<1, 1024, 0, ctx->stream>>>((const uint64_t*)ctx->st_keys2.p,
+                                                        (const uint32_t*)ctx->st_vals2.p,
+                                                        (const StokeEntry*)ctx->st_entries.p, (uint32_t*)ctx->st_rep.p,
+                                                        (uint32_t*)ctx->st_ord.p, sc);
+            CKL("k_stoke_dedupe");
+            CK(cudaMemsetAsync(ctx->st_verdict.p, 0xFF, (size_t)n_ok * 4, ctx->stream));
+            CK(cudaMemcpyAsync(&hv, sc, sizeof hv, cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));
-            if (items <= icap) break;
-            if (attempt >= 4) return set_err(ctx, M6502_E_NOMEM, "work-item queue kept overflowing");
-            icap = items + items / 4 + 1024;
+            max_ord = (uint32_t)hv.max_ord;
         }
-        k_stoke_collect<<<ctx->sms * 4, 256, 0, ctx->stream>>>((const StokeEntry*)ctx->st_entries.p,
-                                                               (const uint32_t*)ctx->st_vidx.p,
-                                                               (const uint32_t*)ctx->fail.p, sc,
-                                                               (StokeChain*)ctx->st_chains.p,
-                                                               (uint32_t*)ctx->st_proven.p,
-                                                               (uint32_t*)ctx->st_pidx.p, ecap);
-        CKL("k_stoke_collect");
+        // Rounds of at most kVerifyBatch distinct candidates per target under
+        // stop_on_proof (a target proved in one round is skipped in the next);
+        // a single round of all of them otherwise.
+        const uint32_t batch = cfg->stop_on_proof ? kVerifyBatch : 0xFFFFFFFFu;
+        StokeSource src{(const StokeEntry*)ctx->st_entries.p, (const uint32_t*)ctx->st_vlist.p, tg, cfg->dead_flags};
+        for (uint32_t lo = 0; n_ok && lo <= max_ord; lo = (batch > 0xFFFFFFFFu - lo) ? 0xFFFFFFFFu : lo + batch) {
+            const uint32_t hi = batch > 0xFFFFFFFFu - lo ? 0xFFFFFFFFu : lo + batch;
+            CK(cudaMemsetAsync(&sc->round_n, 0, sizeof(unsigned long long), ctx->stream));
+            k_stoke_select<<<ctx->sms * 4, 256, 0, ctx->stream>>>(
+                (const uint64_t*)ctx->st_keys2.p, (const uint32_t*)ctx->st_vals2.p, (const uint32_t*)ctx->st_rep.p,
+                (const uint32_t*)ctx->st_ord.p, lo, hi, cfg->stop_on_proof, (const uint32_t*)ctx->st_proven.p,
+                (uint32_t*)ctx->st_vlist.p, (uint32_t*)ctx->st_vpos.p, sc);
+            CKL("k_stoke_select");
+            for (int attempt = 0;; attempt++) {
+                TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
+                CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), ctx->stream));
+                ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg->sweep, 0};
+                k_exhaustive<StokeSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &sc->round_n, ecap, ea);
+                CKL("k_exhaustive(stoke)");
+                k_exh_items<StokeSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
+                CKL("k_exh_items(stoke)");
+                unsigned long long items = 0;
+                CK(cudaMemcpyAsync(&items, &cnt->items, sizeof items, cudaMemcpyDeviceToHost, ctx->stream));
+                CK(cudaStreamSynchronize(ctx->stream));
+                if (items <= icap) break;
+                if (attempt >= 4) return set_err(ctx, M6502_E_NOMEM, "work-item queue kept overflowing");
+                icap = items + items / 4 + 1024;
+            }
+            k_stoke_verdicts<<<ctx->sms * 4, 256, 0, ctx->stream>>>(
+                (const uint32_t*)ctx->fail.p, (const uint32_t*)ctx->st_vpos.p, (const uint64_t*)ctx->st_keys2.p,
+                (uint32_t*)ctx->st_verdict.p, (uint32_t*)ctx->st_proven.p, sc);
+            CKL("k_stoke_verdicts");
+            if (hi == 0xFFFFFFFFu) break;
+        }
+        if (n_ok) {
+            k_stoke_collect<<<ctx->sms * 4, 256, 0, ctx->stream>>>(
+                (const uint32_t*)ctx->st_vals2.p, (const uint32_t*)ctx->st_rep.p, (const uint32_t*)ctx->st_verdict.p,
+                (const StokeEntry*)ctx->st_entries.p, sc, (StokeChain*)ctx->st_chains.p, (uint32_t*)ctx->st_pidx.p,
+                ecap);
+            CKL("k_stoke_collect");
+        }
         CK(cudaEventRecord(ctx->sev[2], ctx->stream));
         StokeCounters hc;
         CK(cudaMemcpyAsync(&hc, sc, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream));
@@ -538,6 +704,7 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
         st.accepted += hc.accepted;
         st.candidates += std::min<uint64_t>(hc.entries, ecap);
         st.undecided += hc.undecided;
+        st.verified += hc.verified;
         if (hc.entries > ecap) return set_err(ctx, M6502_E_NOMEM, "STOKE entry buffer overflowed");
         if (prm.traj && hc.traj) {   // improving moves of this epoch -> the caller's buffer
             const uint64_t have = std::min<uint64_t>(hc.traj, prm.traj_cap);
@@ -555,6 +722,13 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
             CK(cudaMemcpyAsync(h_entries.data(), ctx->st_entries.p, h_entries.size() * sizeof(StokeEntry),
                                cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));
+            // deterministic order within the epoch: target, step, chain
+            std::sort(pidx.begin(), pidx.end(), [&](uint32_t a, uint32_t b) {
+                const StokeEntry &x = h_entries[a], &y = h_entries[b];
+                if (x.target != y.target) return x.target < y.target;
+                if (x.step != y.step) return x.step < y.step;
+                return x.chain < y.chain;
+            });
             for (uint32_t e : pidx) {
                 const StokeEntry& en = h_entries[e];
                 m6502_stoke_proof pr;

@@ -98,7 +98,8 @@ class StokeResult(ctypes.Structure):
 class StokeStats(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("steps", "accepted", "candidates", "proofs", "undecided", "epochs",
                                               "targets_proven")] + \
-               [(n, ctypes.c_double) for n in ("ms_device", "ms_chains", "ms_verify")]
+               [(n, ctypes.c_double) for n in ("ms_device", "ms_chains", "ms_verify")] + \
+               [("verified", ctypes.c_uint64)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -324,7 +324,7 @@ def run_stoke(args):
                        "cost": "hamming over 32 vectors + bytes + cycles/100", "temperature": "1.0 -> 0.1",
                        "proposal": "uniform", "sweep": "full", "stop_on_proof": True},
             "proved": len(times), "censored": len(targets) - len(times),
-            "proofs": st["proofs"], "candidates": st["candidates"], "undecided": st["undecided"],
+            "proofs": st["proofs"], "candidates": st["candidates"], "verified": st["verified"], "undecided": st["undecided"],
             "chain_steps_per_s": st["steps"] / (st["ms_device"] / 1e3) if st["ms_device"] else None,
             "ms_device": st["ms_device"], "ms_chains": st["ms_chains"], "ms_verify": st["ms_verify"],
             "p90_ms": times[int(0.9 * (len(times) - 1))] if times else None,

@@ -284,6 +284,9 @@ typedef struct m6502_stoke_stats {
     uint64_t epochs;
     uint64_t targets_proven;
     double ms_device, ms_chains, ms_verify;
+    uint64_t verified;          /* distinct (target, candidate) pairs run through ExhaustiveCheck:
+                                   identical candidates are verified once, and under stop_on_proof
+                                   in rounds of 8 per target until one proves */
 } m6502_stoke_stats;
 
 /* n_targets targets (CSR, 1..14 instructions each).  results[n_targets] gets
@@ -295,7 +298,7 @@ int m6502_stoke_run(m6502_ctx *ctx, const m6502_stoke_cfg *cfg, const uint16_t *
                     m6502_stoke_stats *stats);
 
 /* ---- learned proposal: a BF16 MLP on the tcgen05 tensor cores ----
- * No counterpart in the reference (SURVEY row a-9): a small network that
+ * No counterpart in the reference: a small network that
  * proposes STOKE moves.  Input: target and current candidate (embedded), the
  * mask of MidCheck vectors on which they differ, their lengths.  Output:
  * softmax over the position (16), opcode (58) and operand (256) of the next

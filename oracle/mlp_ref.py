@@ -51,15 +51,16 @@ def features(ex, P):
     base = opbase()
     x = np.zeros((len(ex), IN))
     for r, e in enumerate(ex):
-        for p in range(e["tlen"]):
-            x[r, :EMB] += et[insn_index(e["target"][p], base)] + pt[p]
-        for p in range(e["clen"]):
-            x[r, EMB:2 * EMB] += ec[insn_index(e["cand"][p], base)] + pc[p]
+        t, c = e["target"][:POS_T], e.get("cand", [])[:POS_C]
+        for p in range(len(t)):
+            x[r, :EMB] += et[insn_index(t[p], base)] + pt[p]
+        for p in range(len(c)):
+            x[r, EMB:2 * EMB] += ec[insn_index(c[p], base)] + pc[p]
         for b in range(32):
             x[r, 256 + b] = (e["diff"] >> b) & 1
-        x[r, 288 + e["tlen"]] = 1 if e["tlen"] < 16 else 0
-        if e["clen"] < 16:
-            x[r, 304 + e["clen"]] = 1
+        x[r, 288 + len(t)] = 1
+        if len(c) < 16:
+            x[r, 304 + len(c)] = 1
     return bf16(x)
 
 
@@ -106,11 +107,12 @@ def loss_and_grads(ex, flat):
     g_et, g_pt = np.zeros(SHAPES[0]), np.zeros(SHAPES[1])
     g_ec, g_pc = np.zeros(SHAPES[2]), np.zeros(SHAPES[3])
     for r, e in enumerate(ex):
-        for p in range(e["tlen"]):
-            g_et[insn_index(e["target"][p], base)] += dx0[r, :EMB]
+        t, c = e["target"][:POS_T], e.get("cand", [])[:POS_C]
+        for p in range(len(t)):
+            g_et[insn_index(t[p], base)] += dx0[r, :EMB]
             g_pt[p] += dx0[r, :EMB]
-        for p in range(e["clen"]):
-            g_ec[insn_index(e["cand"][p], base)] += dx0[r, EMB:2 * EMB]
+        for p in range(len(c)):
+            g_ec[insn_index(c[p], base)] += dx0[r, EMB:2 * EMB]
             g_pc[p] += dx0[r, EMB:2 * EMB]
     grads[0], grads[1], grads[2], grads[3] = g_et, g_pt, g_ec, g_pc
     return loss, grads

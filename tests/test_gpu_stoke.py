@@ -78,3 +78,22 @@ def test_stoke_stop_on_proof_and_random_targets(engine):
             assert oracle.exhaustive(t, c, 0, oracle.SWEEP_REFERENCE)
             checked += 1
     assert checked >= min(len(proofs), 1) or not proofs
+
+
+def test_stoke_dedupe_deterministic(engine):
+    """Identical (target, candidate) pairs are verified once; every chain's
+    entry of a proved pair is still a proof.  Two runs with the same seed
+    report the same proofs in the same order."""
+    targets = [I.parse_assembly(s) for s in EASY]
+    kw = dict(chains_per_target=64, steps=8000, steps_per_epoch=1000, seed=5, cost=_lib.COST_HAMMING,
+              sweep=_lib.SWEEP_REFERENCE)
+    res1, p1, st1 = engine.stoke(targets, **kw)
+    res2, p2, st2 = engine.stoke(targets, **kw)
+    assert st1["proofs"] == len(p1) > 0
+    assert st1["verified"] < st1["candidates"]          # 64 chains per target find the same rewrites
+    keys = {(p["target"], tuple(p["cand"])) for p in p1}
+    assert st1["verified"] >= len(keys)
+    assert [(p["target"], p["chain"], p["step"], tuple(p["cand"])) for p in p1] == \
+           [(p["target"], p["chain"], p["step"], tuple(p["cand"])) for p in p2]
+    for k in ("proofs", "candidates", "verified", "undecided", "accepted"):
+        assert st1[k] == st2[k], k
