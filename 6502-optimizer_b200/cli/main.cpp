@@ -188,7 +188,9 @@ int cmd_enumerate(const Args& a) {
     cfg.semantics = go ? M6502_SEM_GO : M6502_SEM_CUDA;
     cfg.sweep = sweep == "reference" ? M6502_SWEEP_REFERENCE : M6502_SWEEP_FULL;
     cfg.stages = a.has("--no-exhaust") ? (M6502_CHECK_QC | M6502_CHECK_MID) : M6502_CHECK_ALL;
-    cfg.max_cand_len = 1;
+    // The Go search tries candidates of length 1..max-target - 1 (search.go:26-28);
+    // the CUDA pipeline only length 1 (6502_search_v2.cu:800-806).
+    cfg.max_cand_len = go ? (uint32_t)max_target - 1 : 1;
     cfg.dead_flags = dead;
     std::vector<OutRule> all;
     uint64_t total_rules = 0;
@@ -208,7 +210,9 @@ int cmd_enumerate(const Args& a) {
             if (rc != M6502_OK) die(ctx, rc, "m6502_enumerate");
             total_rules += n;
             std::sort(out.begin(), out.begin() + (long)n, [](const m6502_rule& x, const m6502_rule& y) {
-                return x.target != y.target ? x.target < y.target : x.cand[0] < y.cand[0];
+                if (x.target != y.target) return x.target < y.target;
+                if (x.cand_len != y.cand_len) return x.cand_len < y.cand_len;
+                return x.cand[0] != y.cand[0] ? x.cand[0] < y.cand[0] : x.cand[1] < y.cand[1];
             });
             for (uint64_t i = 0; i < n; i++) {
                 const m6502_rule& r = out[i];
@@ -276,7 +280,8 @@ int cmd_target(const Args& a) {
     m6502_search_cfg cfg{};
     cfg.semantics = M6502_SEM_GO;
     cfg.sweep = M6502_SWEEP_REFERENCE;
-    cfg.max_cand_len = maxc >= 1 ? 1 : 0;
+    if (maxc > 2) std::fprintf(stderr, "note: candidates are searched up to length 2 (--max-candidate %ld)\n", maxc);
+    cfg.max_cand_len = (uint32_t)std::max(0L, std::min(maxc, 2L));
     cfg.dead_flags = dead;
     m6502_rule out[4];
     uint64_t k = 0;

@@ -792,6 +792,133 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tf
     }
 }
 
+// ---- Length-2 candidates: an exact join over all 2,863^2 sequences ----
+//
+// Per dead-flags mask, every length-2 sequence (CUDA index c0 * 2863 + c1)
+// gets the key of its 8 masked QuickCheck outputs; the (key, index) table is
+// radix-sorted on the device once and cached.  A target's QuickCheck hits
+// among the 8.2 M candidates are then exactly the candidates with its key
+// that re-pass the 8 vectors -- found by one warp-wide search per target.
+
+// Keys of all length-2 sequences, thread per sequence.  Consecutive threads
+// share the first instruction and mostly the second's opcode, so the
+// dispatch stays warp-uniform.
+__global__ void k_cand2_keys(uint32_t dead, uint64_t* __restrict__ keys, uint32_t* __restrict__ idx) {
+    const uint64_t loose = cmp_mask(dead);
+    const uint32_t n = (uint32_t)kNumInsns * (uint32_t)kNumInsns;
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
+        const uint16_t i0 = c_tab[c / kNumInsns], i1 = c_tab[c % kNumInsns];
+        uint64_t key = 0x6502;
+        for (int v = 0; v < 8; v++) {
+            St s = unpack(c_vec[v]);
+            exec(s, i0);
+            exec(s, i1);
+            key = key_step(key, fp_of(s) & loose, v);
+        }
+        keys[c] = key;
+        idx[c] = c;
+    }
+}
+
+// First index of a sorted array with keys[i] >= key; the warp splits the
+// range 33 ways per step (one load per lane).
+__device__ __forceinline__ uint32_t warp_lower_bound(const uint64_t* __restrict__ keys, uint32_t n, uint64_t key,
+                                                     int lane) {
+    uint32_t lo = 0, hi = n;   // the answer lies in [lo, hi]
+    while (hi - lo > 32) {
+        const uint32_t piv = lo + (uint32_t)(((uint64_t)(hi - lo) * (uint64_t)(lane + 1)) / 33u);
+        const unsigned less = __ballot_sync(kFull, keys[piv] < key);
+        const int k = __popc(less);   // pivots ascend, so the lanes below k are exactly the ones below key
+        const uint32_t plo = __shfl_sync(kFull, piv, k > 0 ? k - 1 : 0);
+        const uint32_t phi = __shfl_sync(kFull, piv, k < 32 ? k : 31);
+        const uint32_t nlo = k > 0 ? plo + 1 : lo;
+        hi = k < 32 ? phi : hi;
+        lo = nlo;
+    }
+    const uint32_t i = lo + (uint32_t)lane;
+    return lo + (uint32_t)__popc(__ballot_sync(kFull, i < hi && keys[i] < key));
+}
+
+// QC (+ MidCheck) of targets x all length-2 candidates through the sorted
+// table.  Lane v executes the candidate on vector v.  The byte filter and
+// the pruner are applied per candidate in the equal range.  Go semantics:
+// `best` ([2][nt], the length-1 winners) skips the passes a target has
+// already settled (the worker stops at the first candidate length that
+// finds one, worker.go:122-176).
+template <bool GO>
+__global__ void __launch_bounds__(256) k_qc_join2(const uint64_t* __restrict__ tfp, const uint8_t* __restrict__ tmeta,
+                                                   uint32_t nt, const uint64_t* __restrict__ skeys,
+                                                   const uint32_t* __restrict__ sidx, uint32_t nsorted, uint32_t dead,
+                                                   uint32_t stages, const uint32_t* __restrict__ best,
+                                                   Surv* __restrict__ surv, uint64_t cap, Counters* __restrict__ cnt) {
+    __shared__ Surv s_stage[kWarpsPerBlock][kStage];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    Surv* stage = s_stage[w];
+    int nstage = 0;
+    const uint64_t loose = cmp_mask(dead), exact = cmp_mask(0);
+    unsigned long long nqc = 0, nmid = 0;
+    for (uint32_t t = blockIdx.x * kWarpsPerBlock + w; t < nt; t += gridDim.x * kWarpsPerBlock) {
+        bool need_u = true, need_m = dead != 0;
+        if (GO) {
+            need_u = best[t] == 0xFFFFFFFFu;
+            need_m = need_m && best[(uint64_t)nt + t] == 0xFFFFFFFFu;
+            if (!need_u && !need_m) continue;
+        }
+        const uint64_t tv = tfp[(uint64_t)t * 32 + lane];
+        uint64_t key = 0x6502;
+#pragma unroll
+        for (int v = 0; v < 8; v++) key = key_step(key, __shfl_sync(kFull, tv, v) & loose, v);
+        const uint32_t tb = GO ? (tmeta[t] >> 4) : (tmeta[t] & 15u);
+        for (uint32_t base = warp_lower_bound(skeys, nsorted, key, lane);; base += 32) {
+            const uint32_t i = base + (uint32_t)lane;
+            const bool eq = i < nsorted && skeys[i] == key;
+            const unsigned run = __ballot_sync(kFull, eq);
+            const uint32_t mine = eq ? sidx[i] : 0u;
+            for (unsigned r = run; r; r &= r - 1) {
+                const uint32_t c = __shfl_sync(kFull, mine, __ffs(r) - 1);
+                uint16_t seq[2] = {c_tab[c / kNumInsns], c_tab[c % kNumInsns]};
+                const uint32_t cb = GO ? bytes_go(seq[0] & 0xFFu) + bytes_go(seq[1] & 0xFFu)
+                                       : bytes_cuda(seq[0] & 0xFFu) + bytes_cuda(seq[1] & 0xFFu);
+                if (cb >= tb || should_prune(seq, 2)) continue;   // not shorter, or pruned (uniform)
+                St s = unpack(c_vec[lane]);
+                exec(s, seq[0]);
+                exec(s, seq[1]);
+                const uint64_t x = tv ^ fp_of(s);
+                const unsigned lo_eq = __ballot_sync(kFull, (x & loose) == 0);
+                const unsigned ex_eq = __ballot_sync(kFull, (x & exact) == 0);
+                if ((lo_eq & 0xFFu) != 0xFFu) continue;          // hash collision: QuickCheck fails
+                bool pass = false;
+                uint32_t code = c | kSurvLen2;
+                if (!GO) {
+                    nqc += lane == 0;
+                    const bool mid = !(stages & M6502_CHECK_MID) || lo_eq == kFull;
+                    if (mid) { nmid += lane == 0; pass = true; }
+                } else if ((ex_eq & 0xFFu) == 0xFFu) {           // processTask: unmasked QC passes
+                    if (need_u) { nqc += lane == 0; nmid += lane == 0; pass = true; }
+                } else if (need_m) {                             // processTaskMasked, FlagDiff != 0
+                    uint32_t fd = lane < 8 ? ((uint32_t)(x >> 24) & kPMask) : 0u;
+                    fd = __reduce_or_sync(kFull, fd);
+                    if (fd) {
+                        nqc += lane == 0; nmid += lane == 0; pass = true;
+                        code |= kSurvMasked | (fd_pack(fd) << 25);
+                    }
+                }
+                stage_push(pass && lane == 0, Surv{t, code}, stage, nstage, surv, cap, &cnt->surv, lane);
+            }
+            if (run != kFull) break;
+        }
+    }
+    stage_flush(stage, nstage, surv, cap, &cnt->surv, lane);
+    for (int o = 16; o; o >>= 1) {
+        nqc += __shfl_down_sync(kFull, nqc, o);
+        nmid += __shfl_down_sync(kFull, nmid, o);
+    }
+    if (lane == 0) {
+        if (nqc) atomicAdd(&cnt->qc, nqc);
+        if (nmid) atomicAdd(&cnt->mid, nmid);
+    }
+}
+
 // Exhaustive check, one pair per warp (persistent, device ticket).
 template <class Src>
 __global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long long* n_pairs_ptr,
@@ -1210,6 +1337,7 @@ struct m6502_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t sev[6] = {};   // stage boundaries of one pass
+    cudaEvent_t sev2[6] = {};  // stage boundaries of the length-2 candidate phase
     std::string err;
     std::mutex mu;
     int sms = 148;
@@ -1224,6 +1352,13 @@ struct m6502_ctx {
     DevBuf cfp1cm;                    // candidate-major fingerprints [2863][32]
     std::vector<uint8_t> h_cmeta;
     DevBuf join_keys[256], join_idx[256];
+    struct Cand2Table {            // sorted (key, index) of all length-2 sequences for one mask
+        uint32_t dead = 0xFFFFFFFFu;
+        DevBuf keys, idx;
+        uint64_t stamp = 0;
+    } cand2[4];                    // least recently used mask is rebuilt
+    uint64_t cand2_clock = 0;
+    DevBuf c2_keys_in, c2_idx_in, c2_sort_tmp;
     uint32_t join_n[256] = {};
     DevBuf st_tins, st_toffs, st_tout, st_tbytes, st_chains, st_entries, st_vidx, st_proven, st_cnt, st_pidx,
         st_mex, st_probs, st_traj;
@@ -1362,6 +1497,39 @@ int join_table(m6502_ctx* ctx, uint32_t dead) {
     return M6502_OK;
 }
 
+// The sorted length-2 candidate table for one dead-flags mask (cached).
+int cand2_table(m6502_ctx* ctx, uint32_t dead, m6502_ctx::Cand2Table** out) {
+    const uint32_t n = (uint32_t)kNumInsns * (uint32_t)kNumInsns;
+    m6502_ctx::Cand2Table* slot = nullptr;
+    for (auto& t : ctx->cand2)
+        if (t.dead == dead) slot = &t;
+    if (!slot) {
+        slot = &ctx->cand2[0];
+        for (auto& t : ctx->cand2)
+            if (t.stamp < slot->stamp) slot = &t;
+        slot->dead = 0xFFFFFFFFu;
+        TRY(ensure(ctx, slot->keys, (size_t)n * 8));
+        TRY(ensure(ctx, slot->idx, (size_t)n * 4));
+        TRY(ensure(ctx, ctx->c2_keys_in, (size_t)n * 8));
+        TRY(ensure(ctx, ctx->c2_idx_in, (size_t)n * 4));
+        size_t tb = 0;
+        CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, (const uint64_t*)nullptr, (uint64_t*)nullptr,
+                                           (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)n, 0, 64, ctx->stream));
+        TRY(ensure(ctx, ctx->c2_sort_tmp, tb));
+        k_cand2_keys<<<ctx->sms * 8, 256, 0, ctx->stream>>>(dead, (uint64_t*)ctx->c2_keys_in.p,
+                                                            (uint32_t*)ctx->c2_idx_in.p);
+        CKL("k_cand2_keys");
+        tb = ctx->c2_sort_tmp.bytes;
+        CK(cub::DeviceRadixSort::SortPairs(ctx->c2_sort_tmp.p, tb, (const uint64_t*)ctx->c2_keys_in.p,
+                                           (uint64_t*)slot->keys.p, (const uint32_t*)ctx->c2_idx_in.p,
+                                           (uint32_t*)slot->idx.p, (int)n, 0, 64, ctx->stream));
+        slot->dead = dead;
+    }
+    slot->stamp = ++ctx->cand2_clock;
+    *out = slot;
+    return M6502_OK;
+}
+
 struct PassOut {
     Counters c;
 };
@@ -1433,29 +1601,83 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             CKL("k_exh_items");
         }
         CK(cudaEventRecord(ctx->sev[4], ctx->stream));
+        // Passing survivors -> Go winners (best) or rules (CUDA semantics).
+        auto select_or_emit = [&]() -> int {
+            if (go) {
+                if (!exh) CK(cudaMemsetAsync(ctx->fail.p, 0, scap * sizeof(uint32_t), ctx->stream));
+                k_go_select<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
+                                                                   (const uint32_t*)ctx->fail.p, (uint32_t)nt,
+                                                                   (uint32_t*)ctx->best.p, cnt, d_targets, tlen,
+                                                                   cfg.sweep);
+                CKL("k_go_select");
+            } else {
+                k_emit_all<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
+                                                                  (const uint32_t*)ctx->fail.p, d_ids, dead,
+                                                                  (m6502_rule*)ctx->rules.p, rcap, cnt, exh ? 1 : 0,
+                                                                  d_targets, tlen, cfg.sweep);
+                CKL("k_emit_all");
+            }
+            return M6502_OK;
+        };
+        if (go) CK(cudaMemsetAsync(ctx->best.p, 0xFF, 2 * nt * sizeof(uint32_t), ctx->stream));
+        TRY(select_or_emit());
+        CK(cudaEventRecord(ctx->sev[5], ctx->stream));
+        const bool phase2 = cfg.max_cand_len >= 2;
+        Counters hc;
+        bool redo = false;
+        uint64_t surv1 = 0, items1 = 0;   // phase-1 survivors and work items
+        if (phase2) {
+            // Length-2 candidates (worker.go:122: candidate lengths 1..max).
+            CK(cudaMemcpyAsync(&hc, cnt, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (hc.surv > scap) { scap = hc.surv + hc.surv / 4 + 1024; redo = true; }
+            if (hc.items > icap) { icap = hc.items + hc.items / 4 + 1024; redo = true; }
+            if (hc.rules > rcap) { rcap = hc.rules + hc.rules / 4 + 1024; redo = true; }
+            if (redo) continue;
+            surv1 = hc.surv;
+            items1 = hc.items;
+            m6502_ctx::Cand2Table* c2 = nullptr;
+            TRY(cand2_table(ctx, dead, &c2));
+            // survivor, exhaustive-ticket and work-item counters restart for this phase
+            CK(cudaMemsetAsync(&cnt->surv, 0, 4 * sizeof(unsigned long long), ctx->stream));
+            CK(cudaEventRecord(ctx->sev2[0], ctx->stream));
+            const uint32_t jgrid2 =
+                (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8, (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
+            const uint32_t n2 = (uint32_t)kNumInsns * (uint32_t)kNumInsns;
+            if (go)
+                k_qc_join2<true><<<jgrid2, 256, 0, ctx->stream>>>(
+                    (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p, (uint32_t)nt, (const uint64_t*)c2->keys.p,
+                    (const uint32_t*)c2->idx.p, n2, dead, stages, (const uint32_t*)ctx->best.p, (Surv*)ctx->surv.p,
+                    scap, cnt);
+            else
+                k_qc_join2<false><<<jgrid2, 256, 0, ctx->stream>>>(
+                    (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p, (uint32_t)nt, (const uint64_t*)c2->keys.p,
+                    (const uint32_t*)c2->idx.p, n2, dead, stages, nullptr, (Surv*)ctx->surv.p, scap, cnt);
+            CKL("k_qc_join2");
+            CK(cudaEventRecord(ctx->sev2[1], ctx->stream));
+            if (exh) {
+                k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &cnt->surv, scap, ea);
+                CKL("k_exhaustive");
+            }
+            CK(cudaEventRecord(ctx->sev2[2], ctx->stream));
+            if (exh) {
+                k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
+                CKL("k_exh_items");
+            }
+            CK(cudaEventRecord(ctx->sev2[3], ctx->stream));
+            TRY(select_or_emit());
+            CK(cudaEventRecord(ctx->sev2[4], ctx->stream));
+        }
+        if (!phase2) CK(cudaEventRecord(ctx->sev2[4], ctx->stream));
         if (go) {
-            CK(cudaMemsetAsync(ctx->best.p, 0xFF, 2 * nt * sizeof(uint32_t), ctx->stream));
-            if (!exh) CK(cudaMemsetAsync(ctx->fail.p, 0, scap * sizeof(uint32_t), ctx->stream));
-            k_go_select<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
-                                                               (const uint32_t*)ctx->fail.p, (uint32_t)nt,
-                                                               (uint32_t*)ctx->best.p, cnt, d_targets, tlen, cfg.sweep);
-            CKL("k_go_select");
             k_go_emit<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const uint32_t*)ctx->best.p, (uint32_t)nt,
                                                              d_targets, tlen, d_ids,
                                                              (m6502_rule*)ctx->rules.p, rcap, cnt);
             CKL("k_go_emit");
-        } else {
-            k_emit_all<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
-                                                              (const uint32_t*)ctx->fail.p, d_ids, dead,
-                                                              (m6502_rule*)ctx->rules.p, rcap, cnt, exh ? 1 : 0,
-                                                              d_targets, tlen, cfg.sweep);
-            CKL("k_emit_all");
         }
-        CK(cudaEventRecord(ctx->sev[5], ctx->stream));
-        Counters hc;
+        CK(cudaEventRecord(ctx->sev2[5], ctx->stream));
         CK(cudaMemcpyAsync(&hc, cnt, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
-        bool redo = false;
         if (hc.surv > scap) { scap = hc.surv + hc.surv / 4 + 1024; redo = true; }
         if (hc.items > icap) { icap = hc.items + hc.items / 4 + 1024; redo = true; }
         if (hc.rules > rcap) { rcap = hc.rules + hc.rules / 4 + 1024; redo = true; }
@@ -1470,14 +1692,14 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             for (size_t i = old; i < ctx->staging.size(); i++) ctx->staging[i].target += base;
         if (st) {
             st->targets += nt;
-            st->pairs += nt * (uint64_t)kNumInsns;
+            st->pairs += nt * ((uint64_t)kNumInsns + (phase2 ? (uint64_t)kNumInsns * kNumInsns : 0u));
             st->qc_hits += hc.qc;
             st->mid_hits += hc.mid;
-            st->exh_checked += exh ? hc.surv : 0;
+            st->exh_checked += exh ? hc.surv + surv1 : 0;
             st->exh_passed += hc.exh_pass;
             st->rules += hc.rules;
             st->exh_states += hc.states;
-            st->exh_items += hc.items;
+            st->exh_items += hc.items + items1;
             st->exh_algo_ops += hc.algo;
             st->exh_probe_rejects += hc.probe_rejects;
             float ms[5];
@@ -1487,6 +1709,15 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             st->ms_exhaustive += ms[2];
             st->ms_exh_items += ms[3];
             st->ms_emit += ms[4];
+            cudaEventElapsedTime(&ms[4], ctx->sev2[4], ctx->sev2[5]);
+            st->ms_emit += ms[4];
+            if (phase2) {
+                for (int i = 0; i < 4; i++) cudaEventElapsedTime(&ms[i], ctx->sev2[i], ctx->sev2[i + 1]);
+                st->ms_qc += ms[0];
+                st->ms_exhaustive += ms[1];
+                st->ms_exh_items += ms[2];
+                st->ms_emit += ms[3];
+            }
             st->passes += 1;
         }
         return M6502_OK;
@@ -1499,7 +1730,8 @@ int check_cfg(m6502_ctx* ctx, const m6502_search_cfg* cfg) {
     if (cfg->semantics > M6502_SEM_GO) return set_err(ctx, M6502_E_INVAL, "bad semantics");
     if (cfg->sweep > M6502_SWEEP_FULL) return set_err(ctx, M6502_E_INVAL, "bad sweep");
     if (cfg->exh_mode > M6502_EXH_BRUTE) return set_err(ctx, M6502_E_INVAL, "bad exh_mode");
-    if (cfg->max_cand_len > 1) return set_err(ctx, M6502_E_INVAL, "max_cand_len > 1 is not supported by this build");
+    if (cfg->max_cand_len > 2)
+        return set_err(ctx, M6502_E_INVAL, "max_cand_len > 2: the length-3 candidate space (2.3e10) has no join table");
     return M6502_OK;
 }
 
@@ -1551,6 +1783,7 @@ int m6502_create(m6502_ctx** out, const m6502_opts* opts) {
     }
     bool ev_ok = true;
     for (cudaEvent_t& e : ctx->sev) ev_ok = ev_ok && cudaEventCreate(&e) == cudaSuccess;
+    for (cudaEvent_t& e : ctx->sev2) ev_ok = ev_ok && cudaEventCreate(&e) == cudaSuccess;
     if (!ev_ok) {
         delete ctx;
         return M6502_E_CUDA;
@@ -1581,9 +1814,15 @@ void m6502_destroy(m6502_ctx* ctx) {
                       &ctx->st_chains, &ctx->st_entries, &ctx->st_vidx, &ctx->st_proven, &ctx->st_cnt,
                       &ctx->st_pidx, &ctx->st_mex, &ctx->st_probs, &ctx->st_traj, &ctx->st_keys,
                       &ctx->st_keys2, &ctx->st_vals2, &ctx->st_rep, &ctx->st_ord, &ctx->st_verdict,
-                      &ctx->st_vlist, &ctx->st_vpos, &ctx->st_sort_tmp};
+                      &ctx->st_vlist, &ctx->st_vpos, &ctx->st_sort_tmp, &ctx->c2_keys_in, &ctx->c2_idx_in,
+                      &ctx->c2_sort_tmp};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->sev2) if (e) cudaEventDestroy(e);
+    for (auto& t : ctx->cand2) {
+        if (t.keys.p) cudaFree(t.keys.p);
+        if (t.idx.p) cudaFree(t.idx.p);
+    }
     if (ctx->ev0) cudaEventDestroy(ctx->ev0);
     if (ctx->ev1) cudaEventDestroy(ctx->ev1);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);

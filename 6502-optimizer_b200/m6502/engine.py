@@ -141,8 +141,11 @@ class Engine:
         return rules, st
 
     def enumerate(self, target_len=2, dead_flags=0, semantics=_lib.SEM_CUDA, sweep=_lib.SWEEP_FULL,
-                  exh_mode=_lib.EXH_CONES, stages=_lib.CHECK_ALL, first=0, last=2863, cap=1 << 21):
-        cfg = self._cfg(semantics, dead_flags, sweep, exh_mode, stages, 1)
+                  exh_mode=_lib.EXH_CONES, stages=_lib.CHECK_ALL, first=0, last=2863, cap=1 << 21,
+                  max_cand_len=1):
+        """All length-target_len targets whose first instruction has CUDA index in
+        [first, last), searched against candidates of length 1..max_cand_len."""
+        cfg = self._cfg(semantics, dead_flags, sweep, exh_mode, stages, max_cand_len)
         with self._lock:
             return self._run(self._L.m6502_enumerate, cap, self._ctx, ctypes.byref(cfg), target_len,
                              first, last)

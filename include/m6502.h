@@ -102,7 +102,11 @@ typedef struct m6502_search_cfg {
     uint32_t stages;       /* M6502_CHECK_* bits of the pipeline; 0 = all.  Without
                               EXH the MidCheck survivors are the rules
                               (cuda/6502_search_v2.cu --no-exhaust). */
-    uint32_t max_cand_len; /* candidate lengths searched: 1 (default) */
+    uint32_t max_cand_len; /* candidate lengths searched: 1..max_cand_len, at most 2
+                              (0 = 1).  Length 2: all 2,863^2 sequences through a
+                              sorted QuickCheck-key table per mask; Go semantics try
+                              length 2 only where length 1 found nothing
+                              (pkg/search/worker.go:122-176). */
     uint32_t flags;        /* M6502_TARGETS_ON_DEVICE */
     uint8_t dead_flags;    /* dead-flags mask of the run */
     uint8_t reserved[7];

@@ -53,3 +53,15 @@ def test_pair_verdicts():
         assert oracle.quickcheck(t, c, dead) == p["qc"], p
         assert oracle.midcheck(t, c, dead) == (p["qc"] and p["mid"]), p
         assert oracle.exhaustive(t, c, dead, oracle.SWEEP_REFERENCE) == p["exh"], p
+
+
+@pytest.mark.parametrize("mask", ["0x00", "0xC3"])
+def test_config3_fixture_reproduces(mask):
+    """The length-3 / length-2-candidate fixture is the oracle's own output:
+    the first 8 targets re-run here give the fixture's rules for them."""
+    cfg = READ("config3.json")
+    t = np.asarray(cfg["targets"], dtype=np.uint16)
+    assert (t == oracle.draw_targets(1, 3, 4096)[:len(t)]).all()
+    rules, _ = oracle.search_go(t[:8], dead=int(mask, 16), max_cand_len=2)
+    got = sorted([r[0], list(r[1]), r[2]] for r in rules)
+    assert got == [r for r in cfg["go"][mask]["rules"] if r[0] < 8]
