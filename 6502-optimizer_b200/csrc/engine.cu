@@ -89,6 +89,7 @@ __constant__ uint16_t c_sweep[NUM_OPS];       // swept locations implied by opRe
 __constant__ uint16_t c_tab[kNumInsns];       // instructions, CUDA order
 __constant__ uint16_t c_gotab[kNumInsns];     // instructions, Go order
 __constant__ uint32_t c_gorank[kNumInsns];    // Go-order rank of CUDA index i
+__constant__ uint16_t c_goidx[kNumInsns];     // CUDA index of Go rank r
 __constant__ uint32_t c_rep[32];
 
 // ---------------------------------------------------------------------------
@@ -163,6 +164,7 @@ __host__ __device__ __forceinline__ uint32_t fd_pack(uint32_t fd) { return (fd &
 
 struct Counters {
     unsigned long long qc, mid, surv, exh_ticket, items, item_ticket, rules, exh_pass, states, algo, probe_rejects;
+    unsigned long long round_n, max_ord;   // Go-order verification rounds
 };
 
 struct Item {   // one chunk of a large cone sweep
@@ -1101,6 +1103,14 @@ __global__ void k_emit_all(const Surv* __restrict__ surv, const unsigned long lo
     if (lane == 0 && algo) atomicAdd(&cnt->algo, algo);
 }
 
+// Go-order rank of a survivor's candidate; length-2 candidates (bit 28)
+// come after every length-1 candidate (worker.go:122: lengths ascending).
+__device__ __forceinline__ uint32_t go_rank_of(uint32_t code) {
+    const uint32_t idx = code & 0x7FFFFFu;
+    if (code & kSurvLen2) return (1u << 28) | (c_gorank[idx / kNumInsns] * kNumInsns + c_gorank[idx % kNumInsns]);
+    return c_gorank[idx];
+}
+
 // Go semantics: first passing candidate per target and pass, in Go order
 // (shorter candidates first, then Go enumeration order).
 __global__ void k_go_select(const Surv* __restrict__ surv, const unsigned long long* n_ptr, uint64_t n_cap,
@@ -1113,9 +1123,7 @@ __global__ void k_go_select(const Surv* __restrict__ surv, const unsigned long l
         if (fail[p]) continue;
         npass++;
         Surv s = surv[p];
-        uint32_t idx = s.c & 0x7FFFFFu, key;
-        if (s.c & kSurvLen2) key = (1u << 28) | (c_gorank[idx / kNumInsns] * kNumInsns + c_gorank[idx % kNumInsns]);
-        else key = c_gorank[idx];
+        const uint32_t idx = s.c & 0x7FFFFFu, key = go_rank_of(s.c);
         // keep FlagDiff beside the rank so the winner carries its own
         uint64_t pass = (s.c & kSurvMasked) ? 1 : 0;
         atomicMin(&best[pass * nt + s.t], key);
@@ -1158,6 +1166,65 @@ __global__ void k_go_emit(const uint32_t* __restrict__ best, uint32_t nt, const 
             unsigned long long idx = atomicAdd(&cnt->rules, 1ull);
             if (idx < rcap) rules[idx] = r;
         }
+    }
+}
+
+// ---- Go semantics: verification in Go order, in rounds ----
+//
+// The Go worker stops at the first candidate (in Go order) that passes
+// ExhaustiveCheck (worker.go:125-173).  The survivors of a pass are sorted by
+// (target, pass kind, Go rank); round r verifies, for every (target, kind)
+// not yet settled, the next block of its survivors (block sizes 64, 128,
+// 256, ...), and the smallest passing rank of a block settles it.  Only the
+// blocks up to the first pass are swept -- the work the Go worker does.
+
+// Sort key of a survivor: target << 30 | masked pass << 29 | go_rank_of.
+
+__global__ void k_go_keys(const Surv* __restrict__ surv, const unsigned long long* n_ptr, uint64_t* __restrict__ keys) {
+    const uint64_t n = *n_ptr;
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+        const Surv s = surv[p];
+        keys[p] = ((uint64_t)s.t << 30) | ((uint64_t)((s.c & kSurvMasked) ? 1u : 0u) << 29) | go_rank_of(s.c);
+    }
+}
+
+// Ordinal of each sorted survivor within its (target, kind) group.
+__global__ void k_go_ord(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ ord,
+                         Counters* __restrict__ cnt) {
+    unsigned long long mx = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t g = keys[i] >> 29;
+        uint64_t lo = 0, hi = i;   // first index of the group
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if ((keys[mid] >> 29) < g) lo = mid + 1; else hi = mid;
+        }
+        ord[i] = (uint32_t)min((unsigned long long)(i - lo), 0xFFFFFFFFull);
+        mx = max(mx, (unsigned long long)(i - lo));
+    }
+    for (int o = 16; o; o >>= 1) mx = max(mx, __shfl_down_sync(kFull, mx, o));
+    if ((threadIdx.x & 31) == 0 && mx) atomicMax(&cnt->max_ord, mx);
+}
+
+// The survivors of one round, rebuilt as Surv records from their keys.
+__global__ void k_go_round(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ ord, uint64_t n,
+                           uint32_t lo, uint32_t hi, const uint32_t* __restrict__ best, uint32_t nt,
+                           Surv* __restrict__ out, Counters* __restrict__ cnt) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t o = ord[i];
+        if (o < lo || o >= hi) continue;
+        const uint64_t k = keys[i];
+        const uint32_t t = (uint32_t)(k >> 30), kind = (uint32_t)(k >> 29) & 1u, rank = (uint32_t)k & 0x1FFFFFFFu;
+        if (best[(uint64_t)kind * nt + t] != 0xFFFFFFFFu) continue;   // settled by an earlier round
+        uint32_t code;
+        if (rank >> 28) {
+            const uint32_t r = rank & 0x0FFFFFFFu;
+            code = kSurvLen2 | ((uint32_t)c_goidx[r / kNumInsns] * kNumInsns + c_goidx[r % kNumInsns]);
+        } else {
+            code = c_goidx[rank];
+        }
+        if (kind) code |= kSurvMasked;
+        out[atomicAdd(&cnt->round_n, 1ull)] = Surv{t, code};
     }
 }
 
@@ -1351,6 +1418,7 @@ struct m6502_ctx {
     std::vector<uint64_t> h_cfp8;     // QC-vector outputs [8][2863] (host copy)
     DevBuf cfp1cm;                    // candidate-major fingerprints [2863][32]
     std::vector<uint8_t> h_cmeta;
+    DevBuf go_keys, go_keys2, go_ord, go_round, go_sort_tmp;   // Go-order verification rounds
     DevBuf join_keys[256], join_idx[256];
     struct Cand2Table {            // sorted (key, index) of all length-2 sequences for one mask
         uint32_t dead = 0xFFFFFFFFu;
@@ -1429,6 +1497,9 @@ int init_ctx(m6502_ctx* ctx) {
     CK(cudaMemcpyToSymbol(c_tab, tab, sizeof tab));
     CK(cudaMemcpyToSymbol(c_gotab, gotab, sizeof gotab));
     CK(cudaMemcpyToSymbol(c_gorank, gorank, sizeof gorank));
+    static uint16_t goidx[kNumInsns];
+    for (int i = 0; i < kNumInsns; i++) goidx[gorank[i]] = (uint16_t)i;
+    CK(cudaMemcpyToSymbol(c_goidx, goidx, sizeof goidx));
     CK(cudaMemcpyToSymbol(c_rep, rep, sizeof rep));
 
     int occ = 0;
@@ -1589,20 +1660,102 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
         CKL("k_qc1");
         CK(cudaEventRecord(ctx->sev[2], ctx->stream));
         const bool exh = (stages & M6502_CHECK_EXH) != 0;
+        const bool rounds = go && exh;   // Go semantics: verify in Go order, stop at the first pass
         SurvSource src{(const Surv*)ctx->surv.p, d_targets, tlen, dead, go ? 1 : 0};
         ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep, cfg.exh_mode == M6502_EXH_BRUTE};
-        if (exh) {
+        uint64_t round_checked = 0, round_items = 0;
+        bool grow = false;
+        // Go-order verification rounds over the survivors in ctx->surv; on
+        // return `best` holds the first passing candidate per target and pass.
+        auto go_rounds = [&]() -> int {
+            unsigned long long ns = 0;
+            CK(cudaMemcpyAsync(&ns, &cnt->surv, sizeof ns, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (ns > scap) { scap = ns + ns / 4 + 1024; grow = true; return M6502_OK; }
+            if (ns == 0) return M6502_OK;
+            TRY(ensure(ctx, ctx->go_keys, ns * 8));
+            TRY(ensure(ctx, ctx->go_keys2, ns * 8));
+            TRY(ensure(ctx, ctx->go_ord, ns * 4));
+            TRY(ensure(ctx, ctx->go_round, ns * sizeof(Surv)));
+            int end_bit = 30;
+            while (end_bit < 64 && (nt >> (end_bit - 30)) != 0) end_bit++;
+            size_t tb = 0;
+            CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, (const uint64_t*)nullptr, (uint64_t*)nullptr, (int)ns, 0,
+                                              end_bit, ctx->stream));
+            TRY(ensure(ctx, ctx->go_sort_tmp, tb));
+            k_go_keys<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv,
+                                                             (uint64_t*)ctx->go_keys.p);
+            CKL("k_go_keys");
+            tb = ctx->go_sort_tmp.bytes;
+            CK(cub::DeviceRadixSort::SortKeys(ctx->go_sort_tmp.p, tb, (const uint64_t*)ctx->go_keys.p,
+                                              (uint64_t*)ctx->go_keys2.p, (int)ns, 0, end_bit, ctx->stream));
+            CK(cudaMemsetAsync(&cnt->max_ord, 0, sizeof(unsigned long long), ctx->stream));
+            k_go_ord<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const uint64_t*)ctx->go_keys2.p, ns,
+                                                            (uint32_t*)ctx->go_ord.p, cnt);
+            CKL("k_go_ord");
+            unsigned long long max_ord = 0;
+            CK(cudaMemcpyAsync(&max_ord, &cnt->max_ord, sizeof max_ord, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            SurvSource rs{(const Surv*)ctx->go_round.p, d_targets, tlen, dead, 1};
+            uint64_t lo = 0, blk = 64;
+            while (lo <= max_ord) {
+                const uint64_t hi = lo + blk;
+                CK(cudaMemsetAsync(&cnt->round_n, 0, sizeof(unsigned long long), ctx->stream));
+                k_go_round<<<ctx->sms * 8, 256, 0, ctx->stream>>>(
+                    (const uint64_t*)ctx->go_keys2.p, (const uint32_t*)ctx->go_ord.p, ns, (uint32_t)lo,
+                    (uint32_t)std::min<uint64_t>(hi, 0xFFFFFFFFull), (const uint32_t*)ctx->best.p, (uint32_t)nt,
+                    (Surv*)ctx->go_round.p, cnt);
+                CKL("k_go_round");
+                unsigned long long cnts[2] = {0, 0};
+                for (int attempt = 0;; attempt++) {
+                    // exhaustive tickets, work items and item tickets restart each round
+                    CK(cudaMemsetAsync(&cnt->exh_ticket, 0, 3 * sizeof(unsigned long long), ctx->stream));
+                    ExhArgs ra{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep,
+                               cfg.exh_mode == M6502_EXH_BRUTE};
+                    k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(rs, &cnt->round_n, ns, ra);
+                    CKL("k_exhaustive");
+                    k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(rs, ra);
+                    CKL("k_exh_items");
+                    CK(cudaMemcpyAsync(&cnts[0], &cnt->items, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+                    CK(cudaMemcpyAsync(&cnts[1], &cnt->round_n, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                       ctx->stream));
+                    CK(cudaStreamSynchronize(ctx->stream));
+                    if (cnts[0] <= icap) break;
+                    if (attempt >= 4) return set_err(ctx, M6502_E_NOMEM, "work-item queue kept overflowing");
+                    icap = cnts[0] + cnts[0] / 4 + 1024;
+                    TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
+                }
+                k_go_select<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->go_round.p, &cnt->round_n, ns,
+                                                                   (const uint32_t*)ctx->fail.p, (uint32_t)nt,
+                                                                   (uint32_t*)ctx->best.p, cnt, d_targets, tlen,
+                                                                   cfg.sweep);
+                CKL("k_go_select");
+                round_checked += cnts[1];
+                round_items += cnts[0];
+                lo = hi;
+                blk = std::min<uint64_t>(blk * 2, 1ull << 22);
+            }
+            return M6502_OK;
+        };
+        if (go) CK(cudaMemsetAsync(ctx->best.p, 0xFF, 2 * nt * sizeof(uint32_t), ctx->stream));
+        if (exh && !rounds) {
             k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &cnt->surv, scap, ea);
             CKL("k_exhaustive");
         }
+        if (rounds) {
+            TRY(go_rounds());
+            if (grow) continue;
+        }
         CK(cudaEventRecord(ctx->sev[3], ctx->stream));
-        if (exh) {
+        if (exh && !rounds) {
             k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
             CKL("k_exh_items");
         }
         CK(cudaEventRecord(ctx->sev[4], ctx->stream));
         // Passing survivors -> Go winners (best) or rules (CUDA semantics).
         auto select_or_emit = [&]() -> int {
+            if (rounds) return M6502_OK;   // the rounds selected already
             if (go) {
                 if (!exh) CK(cudaMemsetAsync(ctx->fail.p, 0, scap * sizeof(uint32_t), ctx->stream));
                 k_go_select<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
@@ -1619,7 +1772,6 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             }
             return M6502_OK;
         };
-        if (go) CK(cudaMemsetAsync(ctx->best.p, 0xFF, 2 * nt * sizeof(uint32_t), ctx->stream));
         TRY(select_or_emit());
         CK(cudaEventRecord(ctx->sev[5], ctx->stream));
         const bool phase2 = cfg.max_cand_len >= 2;
@@ -1655,12 +1807,16 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
                     (const uint32_t*)c2->idx.p, n2, dead, stages, nullptr, (Surv*)ctx->surv.p, scap, cnt);
             CKL("k_qc_join2");
             CK(cudaEventRecord(ctx->sev2[1], ctx->stream));
-            if (exh) {
+            if (exh && !rounds) {
                 k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &cnt->surv, scap, ea);
                 CKL("k_exhaustive");
             }
+            if (rounds) {
+                TRY(go_rounds());
+                if (grow) continue;
+            }
             CK(cudaEventRecord(ctx->sev2[2], ctx->stream));
-            if (exh) {
+            if (exh && !rounds) {
                 k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
                 CKL("k_exh_items");
             }
@@ -1695,11 +1851,11 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             st->pairs += nt * ((uint64_t)kNumInsns + (phase2 ? (uint64_t)kNumInsns * kNumInsns : 0u));
             st->qc_hits += hc.qc;
             st->mid_hits += hc.mid;
-            st->exh_checked += exh ? hc.surv + surv1 : 0;
+            st->exh_checked += !exh ? 0 : rounds ? round_checked : hc.surv + surv1;
             st->exh_passed += hc.exh_pass;
             st->rules += hc.rules;
             st->exh_states += hc.states;
-            st->exh_items += hc.items + items1;
+            st->exh_items += rounds ? round_items : hc.items + items1;
             st->exh_algo_ops += hc.algo;
             st->exh_probe_rejects += hc.probe_rejects;
             float ms[5];
@@ -1815,7 +1971,8 @@ void m6502_destroy(m6502_ctx* ctx) {
                       &ctx->st_pidx, &ctx->st_mex, &ctx->st_probs, &ctx->st_traj, &ctx->st_keys,
                       &ctx->st_keys2, &ctx->st_vals2, &ctx->st_rep, &ctx->st_ord, &ctx->st_verdict,
                       &ctx->st_vlist, &ctx->st_vpos, &ctx->st_sort_tmp, &ctx->c2_keys_in, &ctx->c2_idx_in,
-                      &ctx->c2_sort_tmp};
+                      &ctx->c2_sort_tmp, &ctx->go_keys, &ctx->go_keys2, &ctx->go_ord, &ctx->go_round,
+                      &ctx->go_sort_tmp};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->sev2) if (e) cudaEventDestroy(e);

@@ -333,6 +333,116 @@ def run_stoke(args):
     eng.close()
 
 
+def go_checked_pairs(targets, rules, dead, nc2=True):
+    """Pairs the Go worker enumerates before it stops (worker.go:122-176:
+    every candidate of each length it tries up to and including the first
+    pass, per pass kind), from the rule set -- the work definition the
+    oracle's own counter uses, so the CPU and GPU rates compare like for like."""
+    from m6502 import inst, _lib
+    go_tab = inst.insn_table(_lib.SEM_GO)
+    rank = {int(x): i for i, x in enumerate(go_tab)}
+    n1, n2 = len(go_tab), len(go_tab) ** 2 if nc2 else 0
+    win = {}
+    for r in rules:
+        c = [int(x) for x in r["cand"][:r["cand_len"]]]
+        kind = 1 if (dead and int(r["dead_flags"])) else 0
+        rk = rank[c[0]] + 1 if len(c) == 1 else n1 + rank[c[0]] * n1 + rank[c[1]] + 1
+        win[(int(r["target"]), kind)] = rk
+    total = 0
+    for t in range(len(targets)):
+        for kind in range(2 if dead else 1):
+            total += win.get((t, kind), n1 + n2)
+    return total
+
+
+def run_len3(args):
+    """Batched length-3 workload: 4,096 seeded length-3 targets (seed 1), each
+    searched against all length-1 (2,863) and length-2 (8,196,769) candidates
+    under dead-flags masks 0x00, 0x01, 0xC3, 0xFF, Go-worker semantics (first
+    passing candidate per length in Go order), reference sweep.  One step =
+    the four masks.  Metric: pair-checks/s, counted as the Go worker counts
+    them (candidates enumerated up to the first pass)."""
+    import torch
+    import m6502
+    from m6502 import inst, _lib
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    masks = (0x00, 0x01, 0xC3, 0xFF)
+    targets = np.asarray(inst.draw_targets(1, 3, 3, 4096), dtype=np.uint16)
+    eng = m6502.Engine(device=local)
+    stream = torch.cuda.ExternalStream(eng.stream, device=local)
+    d_targets = torch.from_numpy(targets.view(np.int16)).to(f"cuda:{local}")
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step(device=True):
+        out = []
+        for m in masks:
+            if device:
+                out.append(eng.search(None, dead_flags=m, semantics=_lib.SEM_GO, sweep=_lib.SWEEP_REFERENCE,
+                                      max_cand_len=2, device_ptr=(d_targets.data_ptr(), len(targets), 3)))
+            else:
+                out.append(eng.search(targets, dead_flags=m, semantics=_lib.SEM_GO, sweep=_lib.SWEEP_REFERENCE,
+                                      max_cand_len=2))
+        return out
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, res = [], None
+    for _ in range(args.steps):
+        flush.fill_(1)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    e2e_ms = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        step(device=False)
+        torch.cuda.synchronize()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    clk = clocks.stop()
+    pairs = sum(go_checked_pairs(targets, rules, m) for m, (rules, _) in zip(masks, res))
+    all_pairs = sum(st["pairs"] for _, st in res)
+    t_ms = statistics.median(ms)
+    per_mask = {f"0x{m:02X}": {"rules": int(len(rules)), "qc_hits": st["qc_hits"], "exh_checked": st["exh_checked"],
+                               "exh_passed": st["exh_passed"], "ms": st["ms_device"]}
+                for m, (rules, st) in zip(masks, res)}
+    line = {"metric": "pair-checks/s", "value": pairs / (t_ms / 1e3), "unit": "pair-checks/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 1), "ms_per_step": t_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+            "data": "synthetic (4,096 seeded length-3 targets, seed 1)",
+            "config": {"workload": "len3-x-len1+len2-4masks", "targets": len(targets),
+                       "candidates": 2863 + 2863 * 2863, "masks": [f"0x{m:02X}" for m in masks],
+                       "semantics": "go worker (first pass per candidate length)", "sweep": "reference",
+                       "l2": "flushed between steps (512 MB write)"},
+            "pairs_go_counted": pairs, "pairs_decided": all_pairs, "per_mask": per_mask,
+            "e2e": {"value": pairs / (statistics.median(e2e_ms) / 1e3), "unit": "pair-checks/s",
+                    "h2d_bytes_per_step": int(targets.nbytes) * len(masks),
+                    "d2h_bytes_per_step": int(sum(len(r) for r, _ in res)) * 16},
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        nthreads = os.cpu_count() or 1
+        sample = targets[::64][:64]
+        t0 = time.perf_counter()
+        cpu_pairs = 0
+        for m in masks:
+            _, st = oracle.search_go(sample, dead=m, max_cand_len=2, nthreads=nthreads)
+            cpu_pairs += st["pairs"]
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": cpu_pairs / dt, "unit": "pair-checks/s", "cores": nthreads, "kind": "port",
+                                "sample": f"{len(sample)} targets (every 64th) x 4 masks, oracle Go worker, {dt:.1f} s"}
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__)
     ap.add_argument("--gpus", type=int, default=1)
@@ -343,12 +453,14 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1500, help="targets in the CPU baseline sample")
     ap.add_argument("--ref-sample", type=int, default=600, help="targets per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["len2", "stoke"], default="len2")
+    ap.add_argument("--workload", choices=["len2", "len3", "stoke"], default="len2")
     ap.add_argument("--stoke-steps", type=int, default=1000000, help="steps per chain (STOKE workload)")
     ap.add_argument("--stoke-epoch", type=int, default=2000, help="steps between proof rounds (STOKE workload)")
     args = ap.parse_args()
     if args.workload == "stoke":
         run_stoke(args)
+    elif args.workload == "len3":
+        run_len3(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
