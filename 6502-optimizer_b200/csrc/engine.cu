@@ -1891,12 +1891,16 @@ int check_cfg(m6502_ctx* ctx, const m6502_search_cfg* cfg) {
     return M6502_OK;
 }
 
+// Hands the staged rules to the caller; what does not fit stays staged for
+// m6502_fetch_rules.
 int finish(m6502_ctx* ctx, m6502_rule* out, uint64_t cap, uint64_t* n_out) {
-    uint64_t n = ctx->staging.size();
+    const uint64_t n = ctx->staging.size();
     if (n_out) *n_out = n;
-    if (out && cap) std::memcpy(out, ctx->staging.data(), std::min(n, cap) * sizeof(m6502_rule));
-    ctx->staging.clear();
-    if (n > cap) return set_err(ctx, M6502_E_OVERFLOW, "rule buffer too small");
+    const uint64_t k = out ? std::min(n, cap) : 0;
+    if (k) std::memcpy(out, ctx->staging.data(), k * sizeof(m6502_rule));
+    ctx->staging.erase(ctx->staging.begin(), ctx->staging.begin() + (long)k);
+    if (n > k) return set_err(ctx, M6502_E_OVERFLOW, "rule buffer too small: the rest stays staged");
+    ctx->staging.shrink_to_fit();
     return M6502_OK;
 }
 
@@ -2114,6 +2118,13 @@ int m6502_exec_batch(m6502_ctx* ctx, uint64_t n, const uint16_t* insns, const ui
     CK(cudaMemcpyAsync(states_out, d_out, n * 8, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     return M6502_OK;
+}
+
+int m6502_fetch_rules(m6502_ctx* ctx, m6502_rule* out, uint64_t cap, uint64_t* n_out) {
+    if (!ctx) return M6502_E_INVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (cap && !out) return set_err(ctx, M6502_E_INVAL, "NULL out");
+    return finish(ctx, out, cap, n_out);
 }
 
 int m6502_search(m6502_ctx* ctx, const m6502_search_cfg* cfg, const uint16_t* targets, uint64_t n,

@@ -124,7 +124,8 @@ _lock = threading.Lock()
 # Exported symbols (kept in step with include/m6502.h; the host tests check both).
 SYMBOLS = (
     "m6502_version", "m6502_create", "m6502_destroy", "m6502_last_error", "m6502_stream",
-    "m6502_check_pairs", "m6502_fingerprint", "m6502_exec_batch", "m6502_search", "m6502_enumerate",
+    "m6502_check_pairs", "m6502_fingerprint", "m6502_exec_batch", "m6502_search", "m6502_fetch_rules",
+    "m6502_enumerate",
     "m6502_insn_table", "m6502_enumerate_targets", "m6502_draw_targets", "m6502_disasm", "m6502_parse", "m6502_should_prune",
     "m6502_seq_bytes", "m6502_seq_cycles", "m6502_op_deps", "m6502_format_jsonl",
     "m6502_exhaustive_static", "m6502_stoke_run", "m6502_mlp_param_count", "m6502_mlp_create",
@@ -159,6 +160,7 @@ def lib():
         L.m6502_exec_batch.argtypes = [vp, ctypes.c_uint64, u16p, u32p, u64p, u64p]
         L.m6502_search.argtypes = [vp, P(SearchCfg), vp, ctypes.c_uint64, ctypes.c_uint32, vp,
                                    ctypes.c_uint64, u64p, P(Stats)]
+        L.m6502_fetch_rules.argtypes = [vp, vp, ctypes.c_uint64, u64p]
         L.m6502_enumerate.argtypes = [vp, P(SearchCfg), ctypes.c_uint32, ctypes.c_uint32,
                                       ctypes.c_uint32, vp, ctypes.c_uint64, u64p, P(Stats)]
         L.m6502_insn_table.argtypes = [ctypes.c_uint32, u16p]

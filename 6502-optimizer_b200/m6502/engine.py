@@ -106,14 +106,19 @@ class Engine:
     def _run(self, fn, cap, *args):
         st = _lib.Stats()
         n_out = ctypes.c_uint64(0)
-        while True:
-            out = np.zeros(max(cap, 1), dtype=_lib.RULE_DTYPE)
-            rc = fn(*args, out.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(n_out), ctypes.byref(st))
-            if rc == _lib.M6502_E_OVERFLOW:
-                cap = int(n_out.value)
-                continue
+        out = np.zeros(max(cap, 1), dtype=_lib.RULE_DTYPE)
+        rc = fn(*args, out.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(n_out), ctypes.byref(st))
+        if rc == _lib.M6502_E_OVERFLOW:   # the rest of the rules stay staged: fetch them, no re-run
+            n = int(n_out.value)
+            full = np.zeros(n, dtype=_lib.RULE_DTYPE)
+            full[:cap] = out[:cap]
+            rest = ctypes.c_uint64(0)
+            rc = self._L.m6502_fetch_rules(self._ctx, full[cap:].ctypes.data_as(ctypes.c_void_p), n - cap,
+                                           ctypes.byref(rest))
             self._check(rc)
-            return out[:n_out.value], st.as_dict()
+            return full, st.as_dict()
+        self._check(rc)
+        return out[:n_out.value], st.as_dict()
 
     def search(self, targets, dead_flags=0, semantics=_lib.SEM_CUDA, sweep=_lib.SWEEP_FULL,
                exh_mode=_lib.EXH_CONES, stages=_lib.CHECK_ALL, max_cand_len=1, cap=None,

@@ -379,10 +379,11 @@ def run_len3(args):
         for m in masks:
             if device:
                 out.append(eng.search(None, dead_flags=m, semantics=_lib.SEM_GO, sweep=_lib.SWEEP_REFERENCE,
-                                      max_cand_len=2, device_ptr=(d_targets.data_ptr(), len(targets), 3)))
+                                      max_cand_len=2, device_ptr=(d_targets.data_ptr(), len(targets), 3),
+                                      cap=2 * len(targets) + 16))
             else:
                 out.append(eng.search(targets, dead_flags=m, semantics=_lib.SEM_GO, sweep=_lib.SWEEP_REFERENCE,
-                                      max_cand_len=2))
+                                      max_cand_len=2, cap=2 * len(targets) + 16))
         return out
 
     for _ in range(max(args.warmup, 1)):
@@ -411,7 +412,10 @@ def run_len3(args):
     all_pairs = sum(st["pairs"] for _, st in res)
     t_ms = statistics.median(ms)
     per_mask = {f"0x{m:02X}": {"rules": int(len(rules)), "qc_hits": st["qc_hits"], "exh_checked": st["exh_checked"],
-                               "exh_passed": st["exh_passed"], "ms": st["ms_device"]}
+                               "exh_passed": st["exh_passed"], "exh_states": st["exh_states"],
+                               "exh_items": st["exh_items"], "ms": st["ms_device"], "ms_qc": st["ms_qc"],
+                               "ms_exhaustive": st["ms_exhaustive"], "ms_exh_items": st["ms_exh_items"],
+                               "ms_emit": st["ms_emit"]}
                 for m, (rules, st) in zip(masks, res)}
     line = {"metric": "pair-checks/s", "value": pairs / (t_ms / 1e3), "unit": "pair-checks/s",
             "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 1), "ms_per_step": t_ms,

@@ -202,12 +202,20 @@ int m6502_exhaustive_static(uint64_t n, const uint16_t *t_insns, const uint32_t 
  * 1..cfg->max_cand_len, through QC -> MidCheck -> ExhaustiveCheck on the
  * device.  Rules are written to out (capacity cap); *n_out gets the rule
  * count.  If cap is too small the call returns M6502_E_OVERFLOW with
- * *n_out = the number needed and out holding the first cap rules.  Rule
- * order is unspecified.  Replaces processTask/processTaskMasked
+ * *n_out = the number needed and out holding the first cap rules; the other
+ * rules stay staged in the context for m6502_fetch_rules (nothing is
+ * recomputed).  Rule order is unspecified.  Replaces processTask/processTaskMasked
  * (pkg/search/worker.go:119-245) and flush_batch (cuda/6502_search_v2.cu:848-977). */
 int m6502_search(m6502_ctx *ctx, const m6502_search_cfg *cfg, const uint16_t *targets,
                  uint64_t n, uint32_t tlen, m6502_rule *out, uint64_t cap, uint64_t *n_out,
                  m6502_stats *stats);
+
+/* The rules a search or enumeration left staged after M6502_E_OVERFLOW:
+ * copies up to cap of them to out and removes them from the context.
+ * *n_out = the number staged before the call; M6502_E_OVERFLOW again if
+ * more than cap were staged.  The next search or enumeration discards what
+ * is left. */
+int m6502_fetch_rules(m6502_ctx *ctx, m6502_rule *out, uint64_t cap, uint64_t *n_out);
 
 /* All pruned targets of length tlen (2 or 3) whose first instruction has
  * index in [first, last) of the CUDA-order table, searched as m6502_search

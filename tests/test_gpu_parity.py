@@ -215,3 +215,15 @@ def test_enumerate_slices_union_equals_whole(engine):
         assert 100 <= tid // 2863 < 160
         c = [int(r["cand"][0])]
         assert oracle.quickcheck(t, c) and oracle.midcheck(t, c) and oracle.exhaustive(t, c)
+
+
+def test_overflow_fetch_returns_every_rule(engine):
+    """A too-small rule buffer returns M6502_E_OVERFLOW; the rest of the run's
+    rules come from m6502_fetch_rules without re-running the search."""
+    targets = np.asarray(oracle.draw_targets(0, 2, 256), dtype=np.uint16)
+    full, st_full = engine.search(targets, sweep=_lib.SWEEP_REFERENCE, cap=1 << 16)
+    small, st_small = engine.search(targets, sweep=_lib.SWEEP_REFERENCE, cap=4)
+    key = lambda r: (int(r["target"]), tuple(int(x) for x in r["cand"][:r["cand_len"]]), int(r["dead_flags"]))
+    assert len(full) > 4
+    assert sorted(map(key, small)) == sorted(map(key, full))
+    assert st_small["passes"] == st_full["passes"]
