@@ -165,6 +165,7 @@ __host__ __device__ __forceinline__ uint32_t fd_pack(uint32_t fd) { return (fd &
 struct Counters {
     unsigned long long qc, mid, surv, exh_ticket, items, item_ticket, rules, exh_pass, states, algo, probe_rejects;
     unsigned long long round_n, max_ord;   // Go-order verification rounds
+    unsigned long long join_items;         // chunks of long length-2 equal ranges
 };
 
 struct Item {   // one chunk of a large cone sweep
@@ -847,78 +848,160 @@ __device__ __forceinline__ uint32_t warp_lower_bound(const uint64_t* __restrict_
 // `best` ([2][nt], the length-1 winners) skips the passes a target has
 // already settled (the worker stops at the first candidate length that
 // finds one, worker.go:122-176).
+//
+// Equal ranges are very uneven (a flags-only target under mask 0xFF matches
+// hundreds of thousands of flags-only candidates), so a range longer than
+// kJoinChunk is cut into work items that every warp drains.
+constexpr uint32_t kJoinChunk = 1024;
+
+struct JoinItem {   // candidates [lo, hi) of one target's equal range
+    uint32_t t, lo, hi, exact;
+};
+
+struct Join2Args {
+    const uint64_t* tfp;
+    const uint8_t* tmeta;
+    uint32_t nt;
+    const uint64_t* lkeys;   // the run mask's table
+    const uint32_t* lidx;
+    const uint64_t* ekeys;   // the unmasked table (Go semantics, unmasked pass only)
+    const uint32_t* eidx;
+    uint32_t nsorted;
+    uint32_t dead;
+    uint32_t stages;
+    const uint32_t* best;    // Go semantics: settled passes
+    Surv* surv;
+    uint64_t cap;
+    JoinItem* items;
+    uint64_t item_cap;
+    Counters* cnt;
+};
+
+// Which passes a target still needs (Go semantics; both for CUDA).
 template <bool GO>
-__global__ void __launch_bounds__(256) k_qc_join2(const uint64_t* __restrict__ tfp, const uint8_t* __restrict__ tmeta,
-                                                   uint32_t nt, const uint64_t* __restrict__ skeys,
-                                                   const uint32_t* __restrict__ sidx, uint32_t nsorted, uint32_t dead,
-                                                   uint32_t stages, const uint32_t* __restrict__ best,
-                                                   Surv* __restrict__ surv, uint64_t cap, Counters* __restrict__ cnt) {
-    __shared__ Surv s_stage[kWarpsPerBlock][kStage];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    Surv* stage = s_stage[w];
-    int nstage = 0;
-    const uint64_t loose = cmp_mask(dead), exact = cmp_mask(0);
-    unsigned long long nqc = 0, nmid = 0;
-    for (uint32_t t = blockIdx.x * kWarpsPerBlock + w; t < nt; t += gridDim.x * kWarpsPerBlock) {
-        bool need_u = true, need_m = dead != 0;
-        if (GO) {
-            need_u = best[t] == 0xFFFFFFFFu;
-            need_m = need_m && best[(uint64_t)nt + t] == 0xFFFFFFFFu;
-            if (!need_u && !need_m) continue;
-        }
-        const uint64_t tv = tfp[(uint64_t)t * 32 + lane];
-        uint64_t key = 0x6502;
-#pragma unroll
-        for (int v = 0; v < 8; v++) key = key_step(key, __shfl_sync(kFull, tv, v) & loose, v);
-        const uint32_t tb = GO ? (tmeta[t] >> 4) : (tmeta[t] & 15u);
-        for (uint32_t base = warp_lower_bound(skeys, nsorted, key, lane);; base += 32) {
-            const uint32_t i = base + (uint32_t)lane;
-            const bool eq = i < nsorted && skeys[i] == key;
-            const unsigned run = __ballot_sync(kFull, eq);
-            const uint32_t mine = eq ? sidx[i] : 0u;
-            for (unsigned r = run; r; r &= r - 1) {
-                const uint32_t c = __shfl_sync(kFull, mine, __ffs(r) - 1);
-                uint16_t seq[2] = {c_tab[c / kNumInsns], c_tab[c % kNumInsns]};
-                const uint32_t cb = GO ? bytes_go(seq[0] & 0xFFu) + bytes_go(seq[1] & 0xFFu)
-                                       : bytes_cuda(seq[0] & 0xFFu) + bytes_cuda(seq[1] & 0xFFu);
-                if (cb >= tb || should_prune(seq, 2)) continue;   // not shorter, or pruned (uniform)
-                St s = unpack(c_vec[lane]);
-                exec(s, seq[0]);
-                exec(s, seq[1]);
-                const uint64_t x = tv ^ fp_of(s);
-                const unsigned lo_eq = __ballot_sync(kFull, (x & loose) == 0);
-                const unsigned ex_eq = __ballot_sync(kFull, (x & exact) == 0);
-                if ((lo_eq & 0xFFu) != 0xFFu) continue;          // hash collision: QuickCheck fails
-                bool pass = false;
-                uint32_t code = c | kSurvLen2;
-                if (!GO) {
-                    nqc += lane == 0;
-                    const bool mid = !(stages & M6502_CHECK_MID) || lo_eq == kFull;
-                    if (mid) { nmid += lane == 0; pass = true; }
-                } else if ((ex_eq & 0xFFu) == 0xFFu) {           // processTask: unmasked QC passes
-                    if (need_u) { nqc += lane == 0; nmid += lane == 0; pass = true; }
-                } else if (need_m) {                             // processTaskMasked, FlagDiff != 0
-                    uint32_t fd = lane < 8 ? ((uint32_t)(x >> 24) & kPMask) : 0u;
-                    fd = __reduce_or_sync(kFull, fd);
-                    if (fd) {
-                        nqc += lane == 0; nmid += lane == 0; pass = true;
-                        code |= kSurvMasked | (fd_pack(fd) << 25);
-                    }
+__device__ __forceinline__ void open_passes(const Join2Args& a, uint32_t t, bool& need_u, bool& need_m) {
+    need_u = true;
+    need_m = a.dead != 0;
+    if (GO) {
+        need_u = a.best[t] == 0xFFFFFFFFu;
+        need_m = need_m && a.best[(uint64_t)a.nt + t] == 0xFFFFFFFFu;
+    }
+}
+
+template <bool GO>
+__device__ __forceinline__ void join2_range(const Join2Args& a, uint32_t t, uint32_t lo, uint32_t hi, bool use_exact,
+                                            uint64_t tv, bool need_u, bool need_m, Surv* stage, int& nstage,
+                                            unsigned long long& nqc, unsigned long long& nmid, int lane) {
+    const uint64_t loose = cmp_mask(a.dead), exact = cmp_mask(0);
+    const uint32_t* sidx = use_exact ? a.eidx : a.lidx;
+    const uint32_t tb = GO ? (a.tmeta[t] >> 4) : (a.tmeta[t] & 15u);
+    for (uint32_t base = lo; base < hi; base += 32) {
+        const uint32_t i = base + (uint32_t)lane;
+        const unsigned run = __ballot_sync(kFull, i < hi);
+        const uint32_t mine = i < hi ? sidx[i] : 0u;
+        for (unsigned r = run; r; r &= r - 1) {
+            const uint32_t c = __shfl_sync(kFull, mine, __ffs(r) - 1);
+            uint16_t seq[2] = {c_tab[c / kNumInsns], c_tab[c % kNumInsns]};
+            const uint32_t cb = GO ? bytes_go(seq[0] & 0xFFu) + bytes_go(seq[1] & 0xFFu)
+                                   : bytes_cuda(seq[0] & 0xFFu) + bytes_cuda(seq[1] & 0xFFu);
+            if (cb >= tb || should_prune(seq, 2)) continue;   // not shorter, or pruned (uniform)
+            St s = unpack(c_vec[lane]);
+            exec(s, seq[0]);
+            exec(s, seq[1]);
+            const uint64_t x = tv ^ fp_of(s);
+            const unsigned lo_eq = __ballot_sync(kFull, (x & loose) == 0);
+            const unsigned ex_eq = __ballot_sync(kFull, (x & exact) == 0);
+            if ((lo_eq & 0xFFu) != 0xFFu) continue;          // hash collision: QuickCheck fails
+            bool pass = false;
+            uint32_t code = c | kSurvLen2;
+            if (!GO) {
+                nqc += lane == 0;
+                const bool mid = !(a.stages & M6502_CHECK_MID) || lo_eq == kFull;
+                if (mid) { nmid += lane == 0; pass = true; }
+            } else if ((ex_eq & 0xFFu) == 0xFFu) {           // processTask: unmasked QC passes
+                if (need_u) { nqc += lane == 0; nmid += lane == 0; pass = true; }
+            } else if (need_m) {                             // processTaskMasked, FlagDiff != 0
+                uint32_t fd = lane < 8 ? ((uint32_t)(x >> 24) & kPMask) : 0u;
+                fd = __reduce_or_sync(kFull, fd);
+                if (fd) {
+                    nqc += lane == 0; nmid += lane == 0; pass = true;
+                    code |= kSurvMasked | (fd_pack(fd) << 25);
                 }
-                stage_push(pass && lane == 0, Surv{t, code}, stage, nstage, surv, cap, &cnt->surv, lane);
             }
-            if (run != kFull) break;
+            stage_push(pass && lane == 0, Surv{t, code}, stage, nstage, a.surv, a.cap, &a.cnt->surv, lane);
         }
     }
-    stage_flush(stage, nstage, surv, cap, &cnt->surv, lane);
+}
+
+__device__ __forceinline__ void join_counts(Counters* cnt, unsigned long long nqc, unsigned long long nmid) {
     for (int o = 16; o; o >>= 1) {
         nqc += __shfl_down_sync(kFull, nqc, o);
         nmid += __shfl_down_sync(kFull, nmid, o);
     }
-    if (lane == 0) {
+    if ((threadIdx.x & 31) == 0) {
         if (nqc) atomicAdd(&cnt->qc, nqc);
         if (nmid) atomicAdd(&cnt->mid, nmid);
     }
+}
+
+template <bool GO>
+__global__ void __launch_bounds__(256) k_qc_join2(Join2Args a) {
+    __shared__ Surv s_stage[kWarpsPerBlock][kStage];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    Surv* stage = s_stage[w];
+    int nstage = 0;
+    const uint64_t loose = cmp_mask(a.dead), exact = cmp_mask(0);
+    unsigned long long nqc = 0, nmid = 0;
+    for (uint32_t t = blockIdx.x * kWarpsPerBlock + w; t < a.nt; t += gridDim.x * kWarpsPerBlock) {
+        bool need_u, need_m;
+        open_passes<GO>(a, t, need_u, need_m);
+        if (!need_u && !need_m) continue;
+        const uint64_t tv = a.tfp[(uint64_t)t * 32 + lane];
+        // Only the unmasked pass open: its candidates are the exact-key range
+        // of the unmasked table, a subset of the masked key's range.
+        const bool use_exact = GO && !need_m;
+        const uint64_t* skeys = use_exact ? a.ekeys : a.lkeys;
+        const uint64_t km = use_exact ? exact : loose;
+        uint64_t key = 0x6502;
+#pragma unroll
+        for (int v = 0; v < 8; v++) key = key_step(key, __shfl_sync(kFull, tv, v) & km, v);
+        const uint32_t lo = warp_lower_bound(skeys, a.nsorted, key, lane);
+        const uint32_t hi = key == ~0ull ? a.nsorted : warp_lower_bound(skeys, a.nsorted, key + 1, lane);
+        if (hi - lo <= kJoinChunk) {
+            join2_range<GO>(a, t, lo, hi, use_exact, tv, need_u, need_m, stage, nstage, nqc, nmid, lane);
+            continue;
+        }
+        const uint32_t nitems = (hi - lo + kJoinChunk - 1) / kJoinChunk;
+        unsigned long long b = 0;
+        if (lane == 0) b = atomicAdd(&a.cnt->join_items, (unsigned long long)nitems);
+        b = __shfl_sync(kFull, b, 0);
+        for (uint32_t j = lane; j < nitems; j += 32)
+            if (b + j < a.item_cap)
+                a.items[b + j] = JoinItem{t, lo + j * kJoinChunk, min(hi, lo + (j + 1) * kJoinChunk),
+                                          use_exact ? 1u : 0u};
+    }
+    stage_flush(stage, nstage, a.surv, a.cap, &a.cnt->surv, lane);
+    join_counts(a.cnt, nqc, nmid);
+}
+
+// The chunks of the long equal ranges, a warp per chunk.
+template <bool GO>
+__global__ void __launch_bounds__(256) k_qc_join2_items(Join2Args a) {
+    __shared__ Surv s_stage[kWarpsPerBlock][kStage];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    Surv* stage = s_stage[w];
+    int nstage = 0;
+    unsigned long long nqc = 0, nmid = 0;
+    const uint64_t n = min((uint64_t)a.cnt->join_items, a.item_cap);
+    for (uint64_t q = (uint64_t)blockIdx.x * kWarpsPerBlock + w; q < n; q += (uint64_t)gridDim.x * kWarpsPerBlock) {
+        const JoinItem it = a.items[q];
+        bool need_u, need_m;
+        open_passes<GO>(a, it.t, need_u, need_m);
+        const uint64_t tv = a.tfp[(uint64_t)it.t * 32 + lane];
+        join2_range<GO>(a, it.t, it.lo, it.hi, it.exact != 0, tv, need_u, need_m, stage, nstage, nqc, nmid, lane);
+    }
+    stage_flush(stage, nstage, a.surv, a.cap, &a.cnt->surv, lane);
+    join_counts(a.cnt, nqc, nmid);
 }
 
 // Exhaustive check, one pair per warp (persistent, device ticket).
@@ -1419,6 +1502,7 @@ struct m6502_ctx {
     DevBuf cfp1cm;                    // candidate-major fingerprints [2863][32]
     std::vector<uint8_t> h_cmeta;
     DevBuf go_keys, go_keys2, go_ord, go_round, go_sort_tmp;   // Go-order verification rounds
+    DevBuf jitems;                                             // chunks of long length-2 equal ranges
     DevBuf join_keys[256], join_idx[256];
     struct Cand2Table {            // sorted (key, index) of all length-2 sequences for one mask
         uint32_t dead = 0xFFFFFFFFu;
@@ -1617,6 +1701,7 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
     uint64_t scap = std::max<uint64_t>(ctx->surv.bytes / sizeof(Surv), nt * 4 + 4096);
     uint64_t icap = std::max<uint64_t>(ctx->items.bytes / sizeof(Item), 1u << 16);
     uint64_t rcap = std::max<uint64_t>(ctx->rules.bytes / sizeof(m6502_rule), nt / 2 + 4096);
+    uint64_t jcap = std::max<uint64_t>(ctx->jitems.bytes / sizeof(JoinItem), 1u << 16);
     for (int attempt = 0; attempt < 6; attempt++) {
         TRY(ensure(ctx, ctx->surv, scap * sizeof(Surv)));
         TRY(ensure(ctx, ctx->fail, scap * sizeof(uint32_t)));
@@ -1788,23 +1873,29 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             if (redo) continue;
             surv1 = hc.surv;
             items1 = hc.items;
-            m6502_ctx::Cand2Table* c2 = nullptr;
+            m6502_ctx::Cand2Table *c2 = nullptr, *c2e = nullptr;
+            if (go && dead) TRY(cand2_table(ctx, 0, &c2e));   // unmasked table for targets with only that pass open
             TRY(cand2_table(ctx, dead, &c2));
+            if (!c2e) c2e = c2;
             // survivor, exhaustive-ticket and work-item counters restart for this phase
             CK(cudaMemsetAsync(&cnt->surv, 0, 4 * sizeof(unsigned long long), ctx->stream));
             CK(cudaEventRecord(ctx->sev2[0], ctx->stream));
             const uint32_t jgrid2 =
                 (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8, (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
             const uint32_t n2 = (uint32_t)kNumInsns * (uint32_t)kNumInsns;
-            if (go)
-                k_qc_join2<true><<<jgrid2, 256, 0, ctx->stream>>>(
-                    (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p, (uint32_t)nt, (const uint64_t*)c2->keys.p,
-                    (const uint32_t*)c2->idx.p, n2, dead, stages, (const uint32_t*)ctx->best.p, (Surv*)ctx->surv.p,
-                    scap, cnt);
-            else
-                k_qc_join2<false><<<jgrid2, 256, 0, ctx->stream>>>(
-                    (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p, (uint32_t)nt, (const uint64_t*)c2->keys.p,
-                    (const uint32_t*)c2->idx.p, n2, dead, stages, nullptr, (Surv*)ctx->surv.p, scap, cnt);
+            TRY(ensure(ctx, ctx->jitems, jcap * sizeof(JoinItem)));
+            CK(cudaMemsetAsync(&cnt->join_items, 0, sizeof(unsigned long long), ctx->stream));
+            Join2Args ja{(const uint64_t*)ctx->tfp.p, (const uint8_t*)ctx->tmeta.p, (uint32_t)nt,
+                         (const uint64_t*)c2->keys.p, (const uint32_t*)c2->idx.p, (const uint64_t*)c2e->keys.p,
+                         (const uint32_t*)c2e->idx.p, n2, dead, stages, go ? (const uint32_t*)ctx->best.p : nullptr,
+                         (Surv*)ctx->surv.p, scap, (JoinItem*)ctx->jitems.p, jcap, cnt};
+            if (go) {
+                k_qc_join2<true><<<jgrid2, 256, 0, ctx->stream>>>(ja);
+                k_qc_join2_items<true><<<ctx->sms * 8, 256, 0, ctx->stream>>>(ja);
+            } else {
+                k_qc_join2<false><<<jgrid2, 256, 0, ctx->stream>>>(ja);
+                k_qc_join2_items<false><<<ctx->sms * 8, 256, 0, ctx->stream>>>(ja);
+            }
             CKL("k_qc_join2");
             CK(cudaEventRecord(ctx->sev2[1], ctx->stream));
             if (exh && !rounds) {
@@ -1837,6 +1928,7 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
         if (hc.surv > scap) { scap = hc.surv + hc.surv / 4 + 1024; redo = true; }
         if (hc.items > icap) { icap = hc.items + hc.items / 4 + 1024; redo = true; }
         if (hc.rules > rcap) { rcap = hc.rules + hc.rules / 4 + 1024; redo = true; }
+        if (hc.join_items > jcap) { jcap = hc.join_items + hc.join_items / 4 + 1024; redo = true; }
         if (redo) continue;
         size_t old = ctx->staging.size();
         ctx->staging.resize(old + hc.rules);
@@ -1976,7 +2068,7 @@ void m6502_destroy(m6502_ctx* ctx) {
                       &ctx->st_keys2, &ctx->st_vals2, &ctx->st_rep, &ctx->st_ord, &ctx->st_verdict,
                       &ctx->st_vlist, &ctx->st_vpos, &ctx->st_sort_tmp, &ctx->c2_keys_in, &ctx->c2_idx_in,
                       &ctx->c2_sort_tmp, &ctx->go_keys, &ctx->go_keys2, &ctx->go_ord, &ctx->go_round,
-                      &ctx->go_sort_tmp};
+                      &ctx->go_sort_tmp, &ctx->jitems};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->sev2) if (e) cudaEventDestroy(e);

@@ -1,10 +1,20 @@
 // mlp.cu -- the learned STOKE proposal: a BF16 MLP trained and run on the
 // 5th-generation tensor cores.
 //
-// Input (320 features per example): sum of target-instruction and
-// target-position embeddings (128), the same for the current candidate
-// (128), the 32-bit mask of MidCheck vectors on which candidate and target
-// differ, and one-hot target / candidate lengths (16 + 16).  Three hidden
+// Input (448 features per example):
+//   [0, 128)    target: sum over positions p of E_T[op] + E_T[58 + imm]
+//               (operand row only for opcodes that take one) + P_T[p]
+//   [128, 256)  the same for the current candidate (E_C, P_C)
+//   [256, 288)  the 32-bit mask of MidCheck vectors on which they differ
+//   [288, 320)  one-hot target and candidate lengths (16 + 16)
+//   [320, 368)  per candidate position p < 16: cand[p] != target[p],
+//               cand[p] == target[p + 1], cand[p] == target[p - 1]
+//               (a changed, deleted or inserted instruction)
+//   [368, 434)  at the first position where the candidate departs from the
+//               target: the target's opcode one-hot (58) and operand bits (8)
+//   [434, 448)  zero
+// The instruction embedding is factored into opcode and operand rows, so an
+// operand value seen with one opcode informs the others.  Three hidden
 // layers of 512 (ReLU), then one linear layer to 384 logits holding three
 // softmax heads: position (16), opcode (58), operand (256).  All four dense
 // layers, forward and backward, are tcgen05 GEMMs (tc_gemm.cuh) with bf16
@@ -27,16 +37,18 @@
 
 namespace {
 
-constexpr int kEmb = 128, kIn = 320, kHid = 512, kOut = 384;
+constexpr int kEmb = 128, kIn = 448, kHid = 512, kOut = 384;
 constexpr int kPosT = 8, kPosC = 16;
 constexpr int kHeadPos = 0, kHeadOp = 16, kHeadImm = 74, kHeadEnd = 330;
-constexpr int kInsns = 2863;
+constexpr int kVocab = (int)m6502::NUM_OPS + 256;   // opcode rows, then operand rows
+constexpr int kFtDiff = 256, kFtTlen = 288, kFtClen = 304, kFtMis = 320, kFtDel = 336, kFtIns = 352,
+              kFtCopyOp = 368, kFtCopyImm = 426, kFtEnd = 434;
 constexpr int kMaxBatch = 1 << 16;   // largest batch of one device pass
 
 // Parameter tensors in their fixed order.
 struct Shape { int rows, cols; };
 constexpr Shape kShapes[] = {
-    {kInsns, kEmb}, {kPosT, kEmb}, {kInsns, kEmb}, {kPosC, kEmb},   // E_T, P_T, E_C, P_C
+    {kVocab, kEmb}, {kPosT, kEmb}, {kVocab, kEmb}, {kPosC, kEmb},   // E_T, P_T, E_C, P_C
     {kHid, kIn}, {1, kHid}, {kHid, kHid}, {1, kHid}, {kHid, kHid}, {1, kHid},   // W1 b1 W2 b2 W3 b3
     {kOut, kHid}, {1, kOut}};                                                   // W4 b4
 constexpr int kNumTensors = 12;
@@ -49,12 +61,23 @@ size_t param_count() {
     return n;
 }
 
-__constant__ uint32_t c_opbase[m6502::NUM_OPS];   // CUDA-order index of each opcode's first instruction
-
-__device__ __forceinline__ int insn_index(uint16_t insn) {
+// Embedding rows of an instruction: its opcode, and its operand (or -1).
+__device__ __forceinline__ bool insn_rows(uint16_t insn, int& op_row, int& imm_row) {
     const uint32_t op = insn & 0xFFu;
-    if (op >= m6502::NUM_OPS) return -1;
-    return (int)(c_opbase[op] + (m6502::has_imm(op) ? (insn >> 8) : 0u));
+    if (op >= m6502::NUM_OPS) return false;
+    op_row = (int)op;
+    imm_row = m6502::has_imm(op) ? (int)m6502::NUM_OPS + (int)(insn >> 8) : -1;
+    return true;
+}
+
+// First position where the candidate departs from the target (a different
+// instruction, or the candidate ends), or -1 if it does not before the
+// target ends.
+__device__ __forceinline__ int first_departure(const m6502_mlp_example& e) {
+    const int tl = min((int)e.tlen, kPosT);
+    for (int p = 0; p < tl; p++)
+        if (p >= (int)e.clen || e.cand[p] != e.target[p]) return p;
+    return -1;
 }
 
 // Features: warp per example, lane owns 4 of the 128 embedding dims.
@@ -69,26 +92,50 @@ __global__ void k_features(const m6502_mlp_example* __restrict__ ex, int n, int 
             continue;
         }
         const m6502_mlp_example e = ex[r];
+        const int tl = min((int)e.tlen, kPosT), cl = min((int)e.clen, kPosC);
         float at[4] = {0, 0, 0, 0}, ac[4] = {0, 0, 0, 0};
-        for (int p = 0; p < e.tlen && p < kPosT; p++) {
-            const int ix = insn_index(e.target[p]);
-            if (ix < 0) continue;
-            for (int j = 0; j < 4; j++) at[j] += et[(size_t)ix * kEmb + lane * 4 + j] + pt[p * kEmb + lane * 4 + j];
+        for (int p = 0; p < tl; p++) {
+            int o, m;
+            if (!insn_rows(e.target[p], o, m)) continue;
+            for (int j = 0; j < 4; j++) {
+                const int d = lane * 4 + j;
+                at[j] += et[(size_t)o * kEmb + d] + (m >= 0 ? et[(size_t)m * kEmb + d] : 0.0f) + pt[p * kEmb + d];
+            }
         }
-        for (int p = 0; p < e.clen && p < kPosC; p++) {
-            const int ix = insn_index(e.cand[p]);
-            if (ix < 0) continue;
-            for (int j = 0; j < 4; j++) ac[j] += ec[(size_t)ix * kEmb + lane * 4 + j] + pc[p * kEmb + lane * 4 + j];
+        for (int p = 0; p < cl; p++) {
+            int o, m;
+            if (!insn_rows(e.cand[p], o, m)) continue;
+            for (int j = 0; j < 4; j++) {
+                const int d = lane * 4 + j;
+                ac[j] += ec[(size_t)o * kEmb + d] + (m >= 0 ? ec[(size_t)m * kEmb + d] : 0.0f) + pc[p * kEmb + d];
+            }
         }
         for (int j = 0; j < 4; j++) {
             xr[lane * 4 + j] = __float2bfloat16(at[j]);
             xr[kEmb + lane * 4 + j] = __float2bfloat16(ac[j]);
         }
-        xr[256 + lane] = __float2bfloat16((e.diff >> lane) & 1u ? 1.0f : 0.0f);
+        xr[kFtDiff + lane] = __float2bfloat16((e.diff >> lane) & 1u ? 1.0f : 0.0f);
         if (lane < 16) {
-            xr[288 + lane] = __float2bfloat16(lane == e.tlen ? 1.0f : 0.0f);
-            xr[304 + lane] = __float2bfloat16(lane == e.clen ? 1.0f : 0.0f);
+            const int p = lane;
+            xr[kFtTlen + p] = __float2bfloat16(p == (int)e.tlen ? 1.0f : 0.0f);
+            xr[kFtClen + p] = __float2bfloat16(p == (int)e.clen ? 1.0f : 0.0f);
+            const bool in_c = p < cl;
+            const bool mis = in_c && p < tl && e.cand[p] != e.target[p];
+            const bool del = in_c && p + 1 < tl && e.cand[p] == e.target[p + 1];
+            const bool ins = in_c && p >= 1 && p - 1 < tl && e.cand[p] == e.target[p - 1];
+            xr[kFtMis + p] = __float2bfloat16(mis ? 1.0f : 0.0f);
+            xr[kFtDel + p] = __float2bfloat16(del ? 1.0f : 0.0f);
+            xr[kFtIns + p] = __float2bfloat16(ins ? 1.0f : 0.0f);
         }
+        const int q = first_departure(e);
+        const uint32_t qop = q >= 0 ? (e.target[q] & 0xFFu) : 0xFFu, qimm = q >= 0 ? (uint32_t)(e.target[q] >> 8) : 0u;
+        for (int k = lane; k < (int)m6502::NUM_OPS; k += 32)
+            xr[kFtCopyOp + k] = __float2bfloat16((uint32_t)k == qop ? 1.0f : 0.0f);
+        if (lane < 8) {
+            const bool bit = qop < m6502::NUM_OPS && m6502::has_imm(qop) && ((qimm >> lane) & 1u);
+            xr[kFtCopyImm + lane] = __float2bfloat16(bit ? 1.0f : 0.0f);
+        }
+        for (int d = kFtEnd + lane; d < kIn; d += 32) xr[d] = __float2bfloat16(0.0f);
     }
 }
 
@@ -180,18 +227,20 @@ __global__ void k_embed_grad(const float* __restrict__ dx, const m6502_mlp_examp
         const m6502_mlp_example e = ex[r];
         const float* d = dx + (size_t)r * kIn;
         for (int p = 0; p < e.tlen && p < kPosT; p++) {
-            const int ix = insn_index(e.target[p]);
-            if (ix < 0) continue;
+            int o, m;
+            if (!insn_rows(e.target[p], o, m)) continue;
             for (int j = lane; j < kEmb; j += 32) {
-                atomicAdd(&get[(size_t)ix * kEmb + j], d[j]);
+                atomicAdd(&get[(size_t)o * kEmb + j], d[j]);
+                if (m >= 0) atomicAdd(&get[(size_t)m * kEmb + j], d[j]);
                 atomicAdd(&gpt[p * kEmb + j], d[j]);
             }
         }
         for (int p = 0; p < e.clen && p < kPosC; p++) {
-            const int ix = insn_index(e.cand[p]);
-            if (ix < 0) continue;
+            int o, m;
+            if (!insn_rows(e.cand[p], o, m)) continue;
             for (int j = lane; j < kEmb; j += 32) {
-                atomicAdd(&gec[(size_t)ix * kEmb + j], d[kEmb + j]);
+                atomicAdd(&gec[(size_t)o * kEmb + j], d[kEmb + j]);
+                if (m >= 0) atomicAdd(&gec[(size_t)m * kEmb + j], d[kEmb + j]);
                 atomicAdd(&gpc[p * kEmb + j], d[kEmb + j]);
             }
         }
@@ -413,11 +462,7 @@ int m6502_mlp_create(m6502_ctx* ctx, uint64_t seed, m6502_mlp** out) {
     mlp->device = m6502_ctx_device(ctx);
     mlp->stream = (cudaStream_t)m6502_stream(ctx);
     if (cudaSetDevice(mlp->device) != cudaSuccess) { delete mlp; return M6502_E_CUDA; }
-    uint32_t base[m6502::NUM_OPS];
-    uint32_t k = 0;
-    for (uint32_t op = 0; op < m6502::NUM_OPS; op++) { base[op] = k; k += m6502::has_imm(op) ? 256 : 1; }
-    if (cudaMemcpyToSymbol(c_opbase, base, sizeof base) != cudaSuccess ||
-        cudaFuncSetAttribute(tcg::k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, tcg::kSmemBytes) != cudaSuccess) {
+    if (cudaFuncSetAttribute(tcg::k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, tcg::kSmemBytes) != cudaSuccess) {
         delete mlp;
         return M6502_E_CUDA;
     }

@@ -51,29 +51,59 @@ def collect_trajectories(engine, targets, steps=20000, chains=32, seed=1, cap=1 
     return rows, st
 
 
-def move_log_likelihood(probs, rows):
+def move_log_likelihood(probs, rows, mix=None):
     """Mean log-likelihood per move under the model and under the uniform
     proposal (position uniform over the candidate, opcode 1/58, operand 1/256
-    when the opcode takes one)."""
+    when the opcode takes one).  With mix = f the model's probabilities are
+    those of the proposal STOKE draws from: f x model + (1 - f) x uniform."""
     lm, lu = 0.0, 0.0
     for p, r in zip(probs, rows):
-        pp = max(float(p[r["pos"]]), 1e-12)
-        po = max(float(p[16 + r["op"]]), 1e-12)
-        lm += math.log(pp) + math.log(po)
-        lu += -math.log(max(len(r["cand"]), 1)) - math.log(58)
+        n = max(len(r["cand"]), 1)
+        up, uo, ui = 1.0 / n, 1.0 / 58, 1.0 / 256
+        pp, po = float(p[r["pos"]]), float(p[16 + r["op"]])
+        if mix is not None:
+            pp, po = mix * pp + (1 - mix) * up, mix * po + (1 - mix) * uo
+        lm += math.log(max(pp, 1e-12)) + math.log(max(po, 1e-12))
+        lu += math.log(up) + math.log(uo)
         if HasImmediate(r["op"]):
-            lm += math.log(max(float(p[74 + r["imm"]]), 1e-12))
-            lu += -math.log(256)
+            pi = float(p[74 + r["imm"]])
+            if mix is not None:
+                pi = mix * pi + (1 - mix) * ui
+            lm += math.log(max(pi, 1e-12))
+            lu += math.log(ui)
     return lm / len(rows), lu / len(rows)
 
 
-def train_proposal(engine, train_targets, steps=1500, batch=1024, lr=1e-3, traj_steps=20000, seed=0,
-                   rule_limit=100000):
-    """Builds the training set and trains a fresh model; returns (mlp, info)."""
-    rows = examples_from_rules(engine, limit=rule_limit, seed=seed)
-    traj, st = collect_trajectories(engine, train_targets, steps=traj_steps, seed=seed + 1)
+def train_proposal(engine, train_targets, val_targets=None, steps=3000, chunk=500, batch=1024, lr=1e-3,
+                   traj_steps=8000, seed=0, rule_limit=50000, mix=0.5):
+    """Builds the training set (length-2 rules + improving moves of uniform
+    STOKE on train_targets) and trains a fresh model in chunks of `chunk`
+    steps.  With val_targets, the parameters kept are those of the chunk whose
+    mixed-proposal log-likelihood on the validation targets' improving moves
+    is highest (early stopping).  Returns (mlp, info)."""
+    rows = examples_from_rules(engine, limit=rule_limit, seed=seed) if rule_limit else []
+    traj, _ = collect_trajectories(engine, train_targets, steps=traj_steps, seed=seed + 1)
+    val = []
+    if val_targets is not None:
+        val, _ = collect_trajectories(engine, val_targets, steps=traj_steps // 2, chains=16, seed=seed + 3)
+        val = val[:4000]
     data = rows + traj
     mlp = MLP(engine, seed=seed)
-    hist = mlp.train(data, steps=steps, batch=batch, lr=lr, seed=seed + 2)
-    return mlp, {"rule_examples": len(rows), "trajectory_examples": len(traj), "loss_first": float(hist[:10].mean()),
-                 "loss_last": float(hist[-10:].mean())}
+    hist, best, best_ll, best_step, done = [], None, -float("inf"), 0, 0
+    while done < steps:
+        k = min(chunk, steps - done)
+        hist.append(mlp.train(data, steps=k, batch=batch, lr=lr, seed=seed + 2 + done))
+        done += k
+        if val:
+            ll, _ = move_log_likelihood(mlp.predict(val), val, mix=mix)
+            if ll > best_ll:
+                best_ll, best, best_step = ll, mlp.params(), done
+    if best is not None:
+        mlp.set_params(best)
+    hist = np.concatenate(hist)
+    info = {"rule_examples": len(rows), "trajectory_examples": len(traj), "validation_moves": len(val),
+            "loss_first": float(hist[:10].mean()), "loss_last": float(hist[-10:].mean()),
+            "best_step": best_step if val else steps, "val_ll_mixed": best_ll if val else None}
+    if val:
+        info["val_ll_uniform"] = move_log_likelihood(np.zeros((len(val), 330)), val)[1]
+    return mlp, info

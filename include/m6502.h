@@ -335,8 +335,9 @@ int m6502_mlp_create(m6502_ctx *ctx, uint64_t seed, m6502_mlp **out);
 void m6502_mlp_destroy(m6502_mlp *mlp);
 const char *m6502_mlp_last_error(const m6502_mlp *mlp);
 /* Reads (out) and / or writes (in) all parameters, fp32, in the fixed order
- * E_T[2863x128] P_T[8x128] E_C[2863x128] P_C[16x128] W1[512x320] b1[512]
- * W2[512x512] b2 W3[512x512] b3 W4[384x512] b4[384] (W: rows = outputs). */
+ * E_T[314x128] P_T[8x128] E_C[314x128] P_C[16x128] W1[512x448] b1[512]
+ * W2[512x512] b2 W3[512x512] b3 W4[384x512] b4[384] (W: rows = outputs;
+ * E rows 0..57 are opcodes, 58..313 operand values). */
 int m6502_mlp_params(m6502_mlp *mlp, float *out, const float *in);
 /* probs: n x M6502_MLP_OUT. */
 int m6502_mlp_predict(m6502_mlp *mlp, const m6502_mlp_example *ex, uint64_t n, float *probs);

@@ -8,12 +8,14 @@ kernels' arithmetic rather than the storage format.
 """
 import numpy as np
 
-EMB, IN, HID, OUT = 128, 320, 512, 384
+EMB, IN, HID, OUT = 128, 448, 512, 384
 POS_T, POS_C = 8, 16
 H_POS, H_OP, H_IMM, H_END = 0, 16, 74, 330
-SHAPES = [(2863, EMB), (POS_T, EMB), (2863, EMB), (POS_C, EMB), (HID, IN), (1, HID), (HID, HID), (1, HID),
+VOCAB = 58 + 256   # opcode rows, then operand rows
+SHAPES = [(VOCAB, EMB), (POS_T, EMB), (VOCAB, EMB), (POS_C, EMB), (HID, IN), (1, HID), (HID, HID), (1, HID),
           (HID, HID), (1, HID), (OUT, HID), (1, OUT)]
 IMM_OPS = set(range(26, 37))
+F_DIFF, F_TLEN, F_CLEN, F_MIS, F_DEL, F_INS, F_COPY_OP, F_COPY_IMM = 256, 288, 304, 320, 336, 352, 368, 426
 
 
 def bf16(x):
@@ -33,34 +35,50 @@ def unpack(flat):
     return out
 
 
-def opbase():
-    base, k = [], 0
-    for op in range(58):
-        base.append(k)
-        k += 256 if op in IMM_OPS else 1
-    return base
-
-
-def insn_index(insn, base):
+def rows_of(insn):
+    """Embedding rows of an instruction: its opcode and, for the opcodes that
+    take one, its operand (58 + value)."""
     op = insn & 0xFF
-    return base[op] + ((insn >> 8) if op in IMM_OPS else 0)
+    return [op, 58 + (insn >> 8)] if op in IMM_OPS else [op]
+
+
+def first_departure(t, c):
+    for p in range(len(t)):
+        if p >= len(c) or c[p] != t[p]:
+            return p
+    return -1
 
 
 def features(ex, P):
     et, pt, ec, pc = P[0], P[1], P[2], P[3]
-    base = opbase()
     x = np.zeros((len(ex), IN))
     for r, e in enumerate(ex):
-        t, c = e["target"][:POS_T], e.get("cand", [])[:POS_C]
+        t, c = list(e["target"][:POS_T]), list(e.get("cand", [])[:POS_C])
         for p in range(len(t)):
-            x[r, :EMB] += et[insn_index(t[p], base)] + pt[p]
+            for k in rows_of(t[p]):
+                x[r, :EMB] += et[k]
+            x[r, :EMB] += pt[p]
         for p in range(len(c)):
-            x[r, EMB:2 * EMB] += ec[insn_index(c[p], base)] + pc[p]
+            for k in rows_of(c[p]):
+                x[r, EMB:2 * EMB] += ec[k]
+            x[r, EMB:2 * EMB] += pc[p]
         for b in range(32):
-            x[r, 256 + b] = (e["diff"] >> b) & 1
-        x[r, 288 + len(t)] = 1
+            x[r, F_DIFF + b] = (e["diff"] >> b) & 1
+        if len(t) < 16:
+            x[r, F_TLEN + len(t)] = 1
         if len(c) < 16:
-            x[r, 304 + len(c)] = 1
+            x[r, F_CLEN + len(c)] = 1
+        for p in range(len(c)):
+            x[r, F_MIS + p] = p < len(t) and c[p] != t[p]
+            x[r, F_DEL + p] = p + 1 < len(t) and c[p] == t[p + 1]
+            x[r, F_INS + p] = 1 <= p <= len(t) and c[p] == t[p - 1]
+        q = first_departure(t, c)
+        if q >= 0:
+            op, imm = t[q] & 0xFF, t[q] >> 8
+            x[r, F_COPY_OP + op] = 1
+            if op in IMM_OPS:
+                for b in range(8):
+                    x[r, F_COPY_IMM + b] = (imm >> b) & 1
     return bf16(x)
 
 
@@ -103,16 +121,17 @@ def loss_and_grads(ex, flat):
             dout = bf16(d * (acts[l] > 0))
         else:
             dx0 = d
-    base = opbase()
     g_et, g_pt = np.zeros(SHAPES[0]), np.zeros(SHAPES[1])
     g_ec, g_pc = np.zeros(SHAPES[2]), np.zeros(SHAPES[3])
     for r, e in enumerate(ex):
         t, c = e["target"][:POS_T], e.get("cand", [])[:POS_C]
         for p in range(len(t)):
-            g_et[insn_index(t[p], base)] += dx0[r, :EMB]
+            for k in rows_of(t[p]):
+                g_et[k] += dx0[r, :EMB]
             g_pt[p] += dx0[r, :EMB]
         for p in range(len(c)):
-            g_ec[insn_index(c[p], base)] += dx0[r, EMB:2 * EMB]
+            for k in rows_of(c[p]):
+                g_ec[k] += dx0[r, EMB:2 * EMB]
             g_pc[p] += dx0[r, EMB:2 * EMB]
     grads[0], grads[1], grads[2], grads[3] = g_et, g_pt, g_ec, g_pc
     return loss, grads
