@@ -167,7 +167,7 @@ def run_engine(args):
     import m6502
     from m6502 import inst, _lib
 
-    all_targets = inst.enumerate_targets(2)
+    all_targets = inst.enumerate_targets(2, args.first_op, args.last_op)
     shard = np.ascontiguousarray(all_targets[rank::world])
     n = len(shard)
     eng = m6502.Engine(device=local)
@@ -246,9 +246,9 @@ def run_engine(args):
                   "exhaustive_ms": avg("ms_exhaustive"), "exh_items_ms": avg("ms_exh_items"),
                   "emit_ms": avg("ms_emit")}
         dominant = max(("k_exhaustive", avg("ms_exhaustive")), ("k_exh_items", avg("ms_exh_items")),
-                       ("k_qc1", qc_ms), key=lambda kv: kv[1])[0]
+                       ("k_qc_join", qc_ms), key=lambda kv: kv[1])[0]
         traffic = load_traffic().get(dominant)
-        if dominant == "k_qc1":
+        if dominant == "k_qc_join":
             achieved, alg = qc_achieved, "13 ops/pair + 31x13 ops per QC hit (QC+MidCheck)"
         else:
             achieved, alg = exh_achieved, "accepted pairs x 2^(9+8k) states x (10 ops/instruction + 3)"
@@ -257,7 +257,9 @@ def run_engine(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u8",
             "data": "synthetic (exhaustive enumeration of all length-2 targets)",
-            "config": {"workload": WORKLOAD, "targets": total_targets, "candidates": PAIRS_PER_TARGET,
+            "config": {"workload": WORKLOAD if (args.first_op, args.last_op) == (0, 2863)
+                       else f"len2-enumerate-first-ops-{args.first_op}-{args.last_op}",
+                       "targets": total_targets, "candidates": PAIRS_PER_TARGET,
                        "pairs_per_step": pairs_per_step, "dead_flags": "0x00",
                        "sweep": args.sweep, "semantics": "cuda-pipeline", "exh_mode": "cones",
                        "parallelism": f"strided target shards x{world}",
@@ -458,6 +460,10 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=600, help="targets per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", choices=["len2", "len3", "stoke"], default="len2")
+    ap.add_argument("--first-op", type=int, default=0,
+                    help="length-2 workload: first instructions [first-op, last-op) of the CUDA-order table "
+                         "(a subset, for small profiler captures)")
+    ap.add_argument("--last-op", type=int, default=2863)
     ap.add_argument("--stoke-steps", type=int, default=1000000, help="steps per chain (STOKE workload)")
     ap.add_argument("--stoke-epoch", type=int, default=2000, help="steps between proof rounds (STOKE workload)")
     args = ap.parse_args()
