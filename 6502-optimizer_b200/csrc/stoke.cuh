@@ -601,8 +601,10 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     float ms_chains = 0, ms_verify = 0;
     uint32_t proven_targets = 0;
+    uint32_t epoch_len = cfg->first_epoch ? std::min(cfg->first_epoch, spe) : spe;
     for (uint64_t done = 0; done < steps;) {
-        const uint32_t e_steps = (uint32_t)std::min<uint64_t>(spe, steps - done);
+        const uint32_t e_steps = (uint32_t)std::min<uint64_t>(epoch_len, steps - done);
+        epoch_len = (uint32_t)std::min<uint64_t>((uint64_t)epoch_len * 2, spe);
         prm.steps = e_steps;
         CK(cudaMemsetAsync(sc, 0, sizeof(StokeCounters), ctx->stream));
         CK(cudaEventRecord(ctx->sev[0], ctx->stream));

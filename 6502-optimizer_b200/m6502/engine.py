@@ -159,8 +159,8 @@ class Engine:
     # ---- STOKE (pkg/stoke) ----
     def stoke(self, targets, chains_per_target=128, steps=1_000_000, steps_per_epoch=1000, seed=0,
               cost=_lib.COST_REF, decay=0.9999, t_start=1.0, t_end=0.1, max_len=0, dead_flags=0,
-              sweep=_lib.SWEEP_REFERENCE, stop_on_proof=False, cap=1 << 16, model=None, learned_frac=0.5,
-              trajectories=None):
+              sweep=_lib.SWEEP_REFERENCE, stop_on_proof=False, cap=1 << 18, model=None, learned_frac=0.5,
+              trajectories=None, first_epoch=0):
         """Batched STOKE over targets (list of sequences).  Returns (results,
         proofs, stats): results[i] is a dict per target (first_proof_ms < 0 when
         unproven, best rewrite), proofs every proof found, in order."""
@@ -169,6 +169,7 @@ class Engine:
         cfg.chains_per_target, cfg.steps_per_epoch, cfg.steps, cfg.seed = chains_per_target, steps_per_epoch, steps, seed
         cfg.decay, cfg.t_start, cfg.t_end, cfg.cost = decay, t_start, t_end, cost
         cfg.max_len, cfg.sweep, cfg.stop_on_proof, cfg.dead_flags = max_len, sweep, int(stop_on_proof), dead_flags
+        cfg.first_epoch = first_epoch
         if model is not None:
             cfg.proposal, cfg.model, cfg.learned_frac = _lib.PROPOSAL_MIXED, model.handle, learned_frac
         if trajectories is not None:   # (ctypes array of MlpExample, capacity, c_uint64 count)

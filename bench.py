@@ -8,6 +8,9 @@ MidCheck -> full ExhaustiveCheck, dead-flags 0x00, CUDA-pipeline semantics.
 The metric is pair-checks/s of the whole job.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+  python bench.py --workload len3            # 4,096 length-3 targets x length-1+2 candidates x 4 masks
+  python bench.py --workload stoke           # STOKE time-to-proof, uniform proposal
+  python bench.py --workload stoke-learned   # the same with the trained 50/50 mixed proposal
 
 With N > 1 (torchrun) the target list is split strided across ranks (no
 collective on the data path; the fixed job is shared, "scaling": "strong").
@@ -297,40 +300,80 @@ def run_engine(args):
         dist.destroy_process_group()
 
 
+def stoke_once(eng, targets, args, model=None):
+    """One STOKE run over the 512-target set; returns the per-target summary
+    and the stats.  Same seeds for every proposal."""
+    from m6502 import _lib
+    kw = dict(chains_per_target=128, steps=args.stoke_steps, steps_per_epoch=args.stoke_epoch,
+              first_epoch=args.stoke_first_epoch, seed=2, cost=_lib.COST_HAMMING, sweep=_lib.SWEEP_FULL,
+              stop_on_proof=True)
+    if model is not None:
+        kw.update(model=model, learned_frac=0.5)
+    res, proofs, st = eng.stoke(targets, **kw)
+    times = sorted(r["first_proof_ms"] for r in res if r["first_proof_ms"] >= 0)
+    steps = sorted(r["first_proof_step"] for r in res if r["first_proof_ms"] >= 0)
+    summary = {"median_ms": statistics.median(times) if times else None,
+               "p90_ms": times[int(0.9 * (len(times) - 1))] if times else None,
+               "median_steps": statistics.median(steps) if steps else None,
+               "proved": len(times), "censored": len(targets) - len(times),
+               "proofs": st["proofs"], "candidates": st["candidates"], "verified": st["verified"],
+               "undecided": st["undecided"], "epochs": st["epochs"],
+               "chain_steps_per_s": st["steps"] / (st["ms_device"] / 1e3) if st["ms_device"] else None,
+               "ms_device": st["ms_device"], "ms_chains": st["ms_chains"], "ms_verify": st["ms_verify"]}
+    return res, summary
+
+
 def run_stoke(args):
-    """STOKE benchmark workload: 512 seeded targets of length 4..8 (seed 2),
+    """STOKE benchmark workloads on 512 seeded targets of length 4..8 (seed 2),
     128 chains each (65,536 chains), Hamming cost over the 32 MidCheck
     vectors, temperature 1.0 -> 0.1; every shorter zero-cost best is proved on
-    the GPU.  Metric: median time-to-proof over the proved targets."""
+    the GPU (full sweep).  Metric: median time-to-proof over the proved
+    targets.  `stoke`: the uniform proposal.  `stoke-learned`: the 50/50
+    mixed proposal of a model trained first on the GPU (training targets
+    seed 20, validation seed 22, disjoint draws), reported beside a uniform
+    run with the same seeds."""
     import torch
     import m6502
     from m6502 import inst, _lib
+    from m6502.proposal import train_proposal
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     targets = inst.draw_targets(2, 4, 8, 512, reject_pruned=False)
     eng = m6502.Engine(device=local)
     eng.stoke(targets[:8], chains_per_target=8, steps=2000, steps_per_epoch=1000, seed=1, cost=_lib.COST_HAMMING)
+    learned = args.workload == "stoke-learned"
+    model, train_info, train_s = None, None, None
+    if learned:
+        t0 = time.perf_counter()
+        model, train_info = train_proposal(eng, inst.draw_targets(20, 4, 8, 2048, reject_pruned=False),
+                                           inst.draw_targets(22, 4, 8, 64, reject_pruned=False),
+                                           steps=3000, chunk=500)
+        train_s = time.perf_counter() - t0
     clocks = ClockSampler(local)
     clocks.start()
-    res, proofs, st = eng.stoke(targets, chains_per_target=128, steps=args.stoke_steps,
-                                steps_per_epoch=args.stoke_epoch, seed=2, cost=_lib.COST_HAMMING,
-                                sweep=_lib.SWEEP_FULL, stop_on_proof=True)
+    _, uni = stoke_once(eng, targets, args)
+    lrn = stoke_once(eng, targets, args, model)[1] if learned else None
     clk = clocks.stop()
-    times = sorted(r["first_proof_ms"] for r in res if r["first_proof_ms"] >= 0)
-    median = statistics.median(times) if times else None
-    line = {"metric": "STOKE time-to-proof (median over proved targets)", "value": median, "unit": "ms",
+    main = lrn if learned else uni
+    line = {"metric": "STOKE time-to-proof (median over proved targets)", "value": main["median_ms"], "unit": "ms",
             "higher_is_better": False, "n_gpus": 1, "steps": args.stoke_steps, "warmup": 1,
             "dtype": "u8", "data": "synthetic (512 seeded random targets, length 4-8, seed 2)",
-            "config": {"workload": "stoke-512x128", "targets": len(targets), "chains_per_target": 128,
-                       "steps_per_chain": args.stoke_steps, "steps_per_epoch": args.stoke_epoch,
+            "config": {"workload": "stoke-512x128" + ("-learned" if learned else ""), "targets": len(targets),
+                       "chains_per_target": 128, "steps_per_chain": args.stoke_steps,
+                       "steps_per_epoch": args.stoke_epoch, "first_epoch": args.stoke_first_epoch,
                        "cost": "hamming over 32 vectors + bytes + cycles/100", "temperature": "1.0 -> 0.1",
-                       "proposal": "uniform", "sweep": "full", "stop_on_proof": True},
-            "proved": len(times), "censored": len(targets) - len(times),
-            "proofs": st["proofs"], "candidates": st["candidates"], "verified": st["verified"], "undecided": st["undecided"],
-            "chain_steps_per_s": st["steps"] / (st["ms_device"] / 1e3) if st["ms_device"] else None,
-            "ms_device": st["ms_device"], "ms_chains": st["ms_chains"], "ms_verify": st["ms_verify"],
-            "p90_ms": times[int(0.9 * (len(times) - 1))] if times else None,
+                       "proposal": "mixed 50/50 learned + uniform" if learned else "uniform",
+                       "sweep": "full", "stop_on_proof": True},
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}}
+    line.update(main)
+    if learned:
+        line["uniform"] = uni
+        line["train"] = dict(train_info, seconds=train_s)
+        if uni["median_ms"] and main["median_ms"]:
+            line["speedup_median_ms"] = uni["median_ms"] / main["median_ms"]
+        if uni["median_steps"] and main["median_steps"]:
+            line["speedup_median_steps"] = uni["median_steps"] / main["median_steps"]
+        model.close()
     print(json.dumps(line), flush=True)
     eng.close()
 
@@ -459,15 +502,17 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1500, help="targets in the CPU baseline sample")
     ap.add_argument("--ref-sample", type=int, default=600, help="targets per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["len2", "len3", "stoke"], default="len2")
+    ap.add_argument("--workload", choices=["len2", "len3", "stoke", "stoke-learned"], default="len2")
     ap.add_argument("--first-op", type=int, default=0,
                     help="length-2 workload: first instructions [first-op, last-op) of the CUDA-order table "
                          "(a subset, for small profiler captures)")
     ap.add_argument("--last-op", type=int, default=2863)
     ap.add_argument("--stoke-steps", type=int, default=1000000, help="steps per chain (STOKE workload)")
     ap.add_argument("--stoke-epoch", type=int, default=2000, help="steps between proof rounds (STOKE workload)")
+    ap.add_argument("--stoke-first-epoch", type=int, default=64,
+                    help="steps of the first STOKE epoch; epochs double up to --stoke-epoch")
     args = ap.parse_args()
-    if args.workload == "stoke":
+    if args.workload in ("stoke", "stoke-learned"):
         run_stoke(args)
     elif args.workload == "len3":
         run_len3(args)

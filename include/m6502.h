@@ -259,7 +259,8 @@ typedef struct m6502_stoke_cfg {
     uint8_t dead_flags;         /* stoke --dead-flags */
     uint8_t reserved[3];
     float learned_frac;         /* PROPOSAL_MIXED: share of replace / insert moves from the model */
-    uint32_t reserved2;
+    uint32_t first_epoch;       /* steps of the first epoch; each next epoch doubles, up to
+                                   steps_per_epoch (finer time-to-proof early on); 0 = steps_per_epoch */
     struct m6502_mlp *model;    /* PROPOSAL_MIXED: the model (m6502_mlp_create) */
     struct m6502_mlp_example *trajectories; /* optional HOST buffer: every accepted move that
                                    lowered the cost (replace / insert) as a labelled example */
