@@ -48,12 +48,14 @@ constexpr int kMaxSeq = 16;          // longest sequence the pairwise API takes
 constexpr int kWarpsPerBlock = 8;    // 256-thread CTAs
 constexpr uint64_t kSmallSweep = 1ull << 13;  // sweep in-warp up to this many states
 constexpr uint64_t kProbe = 1ull << 12;       // in-warp probe of a large cone
-constexpr uint64_t kChunk = 1ull << 15;       // states per work item
+constexpr uint64_t kChunk = 1ull << 13;       // states per work item (at least)
+constexpr uint64_t kMaxItemsPerCone = 1ull << 16;   // larger cones get larger items
 // Largest cone a pair may need swept (2^34 states, about 0.1 s of the whole
 // GPU).  Pairs of long sequences that read many registers can need far
 // more; they get the verdict "undecided" instead of an endless sweep.
 constexpr uint32_t kMaxConeBits = 34;
 constexpr unsigned kTicketBatch = 4;           // pairs a warp takes per ticket atomic
+constexpr int kMaxAsyncPasses = 64;            // passes of one search queued without a host round trip
 
 // Test vectors: TestVectors + MidCheckVectors of pkg/search/verifier.go:18-67
 // (A, X, Y, P, S, M, S0, S1).  Vectors 0..7 are QuickCheck's.
@@ -720,7 +722,7 @@ __global__ void __launch_bounds__(256) k_qc1(const uint64_t* __restrict__ tfp, c
 // Lane v checks vector v from the candidate-major fingerprints (cfp_cm,
 // 256 contiguous bytes per candidate).  Same survivors as k_qc1.
 template <bool GO>
-__global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tfp, const uint8_t* __restrict__ tmeta,
+__global__ void __launch_bounds__(256) k_qc_join(const uint16_t* __restrict__ targets, uint32_t tlen,
                                                   uint32_t nt, const uint64_t* __restrict__ cfp_cm,
                                                   const uint8_t* __restrict__ cmeta, const uint64_t* __restrict__ skeys,
                                                   const uint16_t* __restrict__ sidx, uint32_t nsorted, uint32_t dead,
@@ -742,8 +744,17 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tf
     const uint64_t loose = cmp_mask(dead), exact = cmp_mask(0);
     unsigned long long nqc = 0, nmid = 0;
     for (uint32_t t = blockIdx.x * kWarpsPerBlock + w; t < nt; t += gridDim.x * kWarpsPerBlock) {
-        const uint64_t* trow = tfp + (uint64_t)t * 32;
-        const uint64_t tv = trow[lane];   // lane v holds the target's output on vector v
+        // The target's outputs, computed here rather than stored: lane v runs
+        // it on vector v (its instructions are warp-uniform loads).
+        const uint16_t* ts = targets + (uint64_t)t * tlen;
+        St st = unpack(c_vec[lane]);
+        uint32_t tb = 0;
+        for (uint32_t i = 0; i < tlen; i++) {
+            const uint16_t insn = ts[i];
+            exec(st, insn);
+            tb += GO ? bytes_go(insn & 0xFFu) : bytes_cuda(insn & 0xFFu);
+        }
+        const uint64_t tv = fp_of(st);   // lane v holds the target's output on vector v
         uint64_t key = 0x6502;
 #pragma unroll
         for (int v = 0; v < 8; v++) key = key_step(key, __shfl_sync(kFull, tv, v) & loose, v);
@@ -755,7 +766,6 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint64_t* __restrict__ tf
         uint32_t end = lo;
         while (end < nsorted && s_key[end] == key) end++;
         if (lo == end) continue;
-        const uint32_t tb = GO ? (tmeta[t] >> 4) : (tmeta[t] & 15u);
         for (uint32_t i = lo; i < end; i++) {
             const uint32_t c = s_idx[i];
             const uint32_t cm = s_meta[c];
@@ -1006,7 +1016,7 @@ __global__ void __launch_bounds__(256) k_qc_join2_items(Join2Args a) {
 
 // Exhaustive check, one pair per warp (persistent, device ticket).
 template <class Src>
-__global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long long* n_pairs_ptr,
+__global__ void __launch_bounds__(256, 4) k_exhaustive(Src src, const unsigned long long* n_pairs_ptr,
                                                      uint64_t n_cap, ExhArgs a) {
     __shared__ uint16_t s_t[kWarpsPerBlock][kMaxSeq], s_c[kWarpsPerBlock][kMaxSeq];
     __shared__ uint16_t s_dep[NUM_OPS][NUM_LOCS];
@@ -1076,7 +1086,8 @@ __global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long
                 else next_group(lg, rem, lane, o, bits, cone, mask);
                 rem &= ~(1u << o);
                 const uint64_t total = 1ull << bits;
-                const uint64_t nitems = (total - kProbe + kChunk - 1) / kChunk;
+                const uint64_t chunk = max(kChunk, (total + kMaxItemsPerCone - 1) / kMaxItemsPerCone);
+                const uint64_t nitems = (total - kProbe + chunk - 1) / chunk;
                 unsigned long long base = 0;
                 if (lane == 0) base = atomicAdd(&a.cnt->items, (unsigned long long)nitems);
                 base = __shfl_sync(kFull, base, 0);
@@ -1085,8 +1096,8 @@ __global__ void __launch_bounds__(256) k_exhaustive(Src src, const unsigned long
                     Item it;
                     it.pair = (uint32_t)p; it.cone = (uint16_t)cone; it.rep = rep ? 1 : 0; it.pad = 0;
                     it.outmask = mask;
-                    it.start = kProbe + j * kChunk;
-                    it.count = min(kChunk, total - it.start);
+                    it.start = kProbe + j * chunk;
+                    it.count = min(chunk, total - it.start);
                     a.items[base + j] = it;
                 }
             }
@@ -1144,10 +1155,10 @@ __device__ __forceinline__ unsigned long long algo_ops(const uint16_t* t, uint32
 
 // CUDA semantics: every passing survivor is a rule.
 __global__ void k_emit_all(const Surv* __restrict__ surv, const unsigned long long* n_ptr, uint64_t n_cap,
-                           const uint32_t* __restrict__ fail, const uint64_t* __restrict__ ids,
+                           const uint32_t* __restrict__ fail, const uint64_t* __restrict__ ids, uint64_t base,
                            uint32_t run_dead, m6502_rule* __restrict__ rules, uint64_t rcap,
-                           Counters* cnt, int check_exh, const uint16_t* __restrict__ targets,
-                           uint32_t tlen, uint32_t sweep_mode) {
+                           unsigned long long* rule_ctr, Counters* cnt, int check_exh,
+                           const uint16_t* __restrict__ targets, uint32_t tlen, uint32_t sweep_mode) {
     const uint64_t n = min((uint64_t)*n_ptr, n_cap);
     const int lane = threadIdx.x & 31;
     unsigned long long npass = 0, algo = 0;
@@ -1159,7 +1170,7 @@ __global__ void k_emit_all(const Surv* __restrict__ surv, const unsigned long lo
         if (pass) {
             Surv s = surv[p];
             uint32_t idx = s.c & 0x7FFFFFu;
-            r.target = ids ? ids[s.t] : s.t;
+            r.target = ids ? ids[s.t] : base + s.t;
             r.dead_flags = (uint8_t)run_dead;
             if (s.c & kSurvLen2) { r.cand_len = 2; r.cand[0] = c_tab[idx / kNumInsns]; r.cand[1] = c_tab[idx % kNumInsns]; }
             else { r.cand_len = 1; r.cand[0] = c_tab[idx]; }
@@ -1170,7 +1181,7 @@ __global__ void k_emit_all(const Surv* __restrict__ surv, const unsigned long lo
         if (vote) {
             int leader = __ffs(vote) - 1;
             unsigned long long b = 0;
-            if (lane == leader) b = atomicAdd(&cnt->rules, (unsigned long long)__popc(vote));
+            if (lane == leader) b = atomicAdd(rule_ctr, (unsigned long long)__popc(vote));
             b = __shfl_sync(kFull, b, leader);
             if (pass) {
                 unsigned long long idx = b + __popc(vote & ((1u << lane) - 1u));
@@ -1488,6 +1499,8 @@ struct m6502_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t sev[6] = {};   // stage boundaries of one pass
     cudaEvent_t sev2[6] = {};  // stage boundaries of the length-2 candidate phase
+    cudaEvent_t aev[6 * kMaxAsyncPasses] = {};   // stage boundaries of the queued passes
+    DevBuf cnt_slots;          // Counters of the queued passes
     std::string err;
     std::mutex mu;
     int sms = 148;
@@ -1696,8 +1709,10 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
     const bool go = cfg.semantics == M6502_SEM_GO;
     const uint32_t stages = cfg.stages ? cfg.stages : M6502_CHECK_ALL;
     const uint32_t dead = cfg.dead_flags;
-    TRY(ensure(ctx, ctx->tfp, nt * 32 * sizeof(uint64_t)));
-    TRY(ensure(ctx, ctx->tmeta, nt));
+    if ((cfg.flags & M6502_QC_SCAN) || cfg.max_cand_len >= 2) {   // stored target fingerprints
+        TRY(ensure(ctx, ctx->tfp, nt * 32 * sizeof(uint64_t)));
+        TRY(ensure(ctx, ctx->tmeta, nt));
+    }
     uint64_t scap = std::max<uint64_t>(ctx->surv.bytes / sizeof(Surv), nt * 4 + 4096);
     uint64_t icap = std::max<uint64_t>(ctx->items.bytes / sizeof(Item), 1u << 16);
     uint64_t rcap = std::max<uint64_t>(ctx->rules.bytes / sizeof(m6502_rule), nt / 2 + 4096);
@@ -1711,11 +1726,13 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
         Counters* cnt = (Counters*)ctx->cnt.p;
         CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), ctx->stream));
         CK(cudaEventRecord(ctx->sev[0], ctx->stream));
-        k_fingerprint<FixedSeqs><<<ctx->fp_blocks, 256, 0, ctx->stream>>>(
-            FixedSeqs{d_targets, tlen}, nt, (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p);
-        CKL("k_fingerprint(targets)");
-        CK(cudaEventRecord(ctx->sev[1], ctx->stream));
         const bool scan = (cfg.flags & M6502_QC_SCAN) != 0;
+        if (scan || cfg.max_cand_len >= 2) {   // the join computes its targets' outputs itself
+            k_fingerprint<FixedSeqs><<<ctx->fp_blocks, 256, 0, ctx->stream>>>(
+                FixedSeqs{d_targets, tlen}, nt, (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p);
+            CKL("k_fingerprint(targets)");
+        }
+        CK(cudaEventRecord(ctx->sev[1], ctx->stream));
         uint32_t qgrid = (uint32_t)std::min<uint64_t>(ctx->qc_blocks, (nt + kQcTile - 1) / kQcTile);
         if (!scan) {
             TRY(join_table(ctx, dead));
@@ -1723,12 +1740,12 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             const uint64_t* jk = (const uint64_t*)ctx->join_keys[dead].p;
             const uint16_t* ji = (const uint16_t*)ctx->join_idx[dead].p;
             if (go)
-                k_qc_join<true><<<jgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
+                k_qc_join<true><<<jgrid, 256, 0, ctx->stream>>>(d_targets, tlen,
                                                                 (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p,
                                                                 (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
                                                                 dead, stages, (Surv*)ctx->surv.p, scap, cnt);
             else
-                k_qc_join<false><<<jgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
+                k_qc_join<false><<<jgrid, 256, 0, ctx->stream>>>(d_targets, tlen,
                                                                  (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p,
                                                                  (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
                                                                  dead, stages, (Surv*)ctx->surv.p, scap, cnt);
@@ -1850,9 +1867,9 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
                 CKL("k_go_select");
             } else {
                 k_emit_all<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
-                                                                  (const uint32_t*)ctx->fail.p, d_ids, dead,
-                                                                  (m6502_rule*)ctx->rules.p, rcap, cnt, exh ? 1 : 0,
-                                                                  d_targets, tlen, cfg.sweep);
+                                                                  (const uint32_t*)ctx->fail.p, d_ids, 0, dead,
+                                                                  (m6502_rule*)ctx->rules.p, rcap, &cnt->rules, cnt,
+                                                                  exh ? 1 : 0, d_targets, tlen, cfg.sweep);
                 CKL("k_emit_all");
             }
             return M6502_OK;
@@ -1973,6 +1990,144 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
     return set_err(ctx, M6502_E_NOMEM, "device buffers kept overflowing");
 }
 
+// CUDA semantics with length-1 candidates: every pass of a search is
+// queued on the stream with no host round trip in between.  Each pass has
+// its own counters (survivors, work items) and stage events; all passes
+// append their rules to one device buffer through one counter, with the
+// global target index.  One synchronisation at the end reads every pass's
+// counters; if any buffer overflowed, the whole search is re-run with larger
+// buffers (nothing is dropped).  Returns M6502_E_INVAL when the search does
+// not fit this path.
+int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* targets, uint64_t n, uint32_t tlen,
+                 bool on_dev, m6502_stats* st) {
+    const uint64_t P = ctx->pass_targets;
+    const uint64_t npass = (n + P - 1) / P;
+    if (npass == 0 || npass > (uint64_t)kMaxAsyncPasses) return set_err(ctx, M6502_E_INVAL, "too many passes");
+    const uint32_t stages = cfg.stages ? cfg.stages : M6502_CHECK_ALL;
+    const uint32_t dead = cfg.dead_flags;
+    const bool exh = (stages & M6502_CHECK_EXH) != 0;
+    const bool scan = (cfg.flags & M6502_QC_SCAN) != 0;
+    const uint64_t pmax = std::min(P, n);
+    uint64_t scap = std::max<uint64_t>(ctx->surv.bytes / sizeof(Surv), pmax * 4 + 4096);
+    uint64_t icap = std::max<uint64_t>(ctx->items.bytes / sizeof(Item), 1u << 16);
+    uint64_t rcap = std::max<uint64_t>(ctx->rules.bytes / sizeof(m6502_rule), n / 2 + 4096);
+    if (scan) {
+        TRY(ensure(ctx, ctx->tfp, pmax * 32 * sizeof(uint64_t)));
+        TRY(ensure(ctx, ctx->tmeta, pmax));
+    }
+    if (!on_dev) TRY(ensure(ctx, ctx->targets, pmax * tlen * 2));
+    if (!scan) TRY(join_table(ctx, dead));
+    TRY(ensure(ctx, ctx->cnt_slots, npass * sizeof(Counters)));
+    Counters* slots = (Counters*)ctx->cnt_slots.p;
+    for (int attempt = 0; attempt < 6; attempt++) {
+        TRY(ensure(ctx, ctx->surv, scap * sizeof(Surv)));
+        TRY(ensure(ctx, ctx->fail, scap * sizeof(uint32_t)));
+        TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
+        TRY(ensure(ctx, ctx->rules, rcap * sizeof(m6502_rule)));
+        CK(cudaMemsetAsync(slots, 0, npass * sizeof(Counters), ctx->stream));
+        for (uint64_t p = 0; p < npass; p++) {
+            const uint64_t b = p * P, nt = std::min(P, n - b);
+            const uint16_t* d_t;
+            if (on_dev) {
+                d_t = targets + b * tlen;
+            } else {   // stream order keeps the previous pass's kernels ahead of this copy
+                CK(cudaMemcpyAsync(ctx->targets.p, targets + b * tlen, nt * tlen * 2, cudaMemcpyHostToDevice,
+                                   ctx->stream));
+                d_t = (const uint16_t*)ctx->targets.p;
+            }
+            Counters* cnt = slots + p;
+            cudaEvent_t* ev = ctx->aev + 6 * p;
+            CK(cudaEventRecord(ev[0], ctx->stream));
+            if (scan) {
+                k_fingerprint<FixedSeqs><<<ctx->fp_blocks, 256, 0, ctx->stream>>>(
+                    FixedSeqs{d_t, tlen}, nt, (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p);
+                CKL("k_fingerprint(targets)");
+            }
+            CK(cudaEventRecord(ev[1], ctx->stream));
+            if (scan) {
+                const uint32_t qgrid = (uint32_t)std::min<uint64_t>(ctx->qc_blocks, (nt + kQcTile - 1) / kQcTile);
+                k_qc1<false><<<qgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
+                                                             (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
+                                                             (uint8_t*)ctx->cmeta1.p, dead, stages,
+                                                             (Surv*)ctx->surv.p, scap, cnt);
+                CKL("k_qc1");
+            } else {
+                const uint32_t jgrid = (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8,
+                                                                    (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
+                k_qc_join<false><<<jgrid, 256, 0, ctx->stream>>>(
+                    d_t, tlen, (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p, (uint8_t*)ctx->cmeta1.p,
+                    (const uint64_t*)ctx->join_keys[dead].p, (const uint16_t*)ctx->join_idx[dead].p,
+                    ctx->join_n[dead], dead, stages, (Surv*)ctx->surv.p, scap, cnt);
+                CKL("k_qc_join");
+            }
+            CK(cudaEventRecord(ev[2], ctx->stream));
+            SurvSource src{(const Surv*)ctx->surv.p, d_t, tlen, dead, 0};
+            ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep,
+                       cfg.exh_mode == M6502_EXH_BRUTE};
+            if (exh) {
+                k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &cnt->surv, scap, ea);
+                CKL("k_exhaustive");
+            }
+            CK(cudaEventRecord(ev[3], ctx->stream));
+            if (exh) {
+                k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
+                CKL("k_exh_items");
+            }
+            CK(cudaEventRecord(ev[4], ctx->stream));
+            k_emit_all<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
+                                                              (const uint32_t*)ctx->fail.p, nullptr, b, dead,
+                                                              (m6502_rule*)ctx->rules.p, rcap, &slots[0].rules, cnt,
+                                                              exh ? 1 : 0, d_t, tlen, cfg.sweep);
+            CKL("k_emit_all");
+            CK(cudaEventRecord(ev[5], ctx->stream));
+        }
+        std::vector<Counters> hc(npass);
+        CK(cudaMemcpyAsync(hc.data(), slots, npass * sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        bool redo = false;
+        for (const Counters& c : hc) {
+            if (c.surv > scap) { scap = std::max<uint64_t>(scap, c.surv + c.surv / 4 + 1024); redo = true; }
+            if (c.items > icap) { icap = std::max<uint64_t>(icap, c.items + c.items / 4 + 1024); redo = true; }
+        }
+        const uint64_t nrules = hc[0].rules;
+        if (nrules > rcap) { rcap = nrules + nrules / 4 + 1024; redo = true; }
+        if (redo) continue;
+        const size_t old = ctx->staging.size();
+        ctx->staging.resize(old + nrules);
+        if (nrules)
+            CK(cudaMemcpyAsync(ctx->staging.data() + old, ctx->rules.p, nrules * sizeof(m6502_rule),
+                               cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        if (st) {
+            for (uint64_t p = 0; p < npass; p++) {
+                const Counters& c = hc[p];
+                const uint64_t nt = std::min(P, n - p * P);
+                st->targets += nt;
+                st->pairs += nt * (uint64_t)kNumInsns;
+                st->qc_hits += c.qc;
+                st->mid_hits += c.mid;
+                st->exh_checked += exh ? c.surv : 0;
+                st->exh_passed += c.exh_pass;
+                st->exh_states += c.states;
+                st->exh_items += c.items;
+                st->exh_algo_ops += c.algo;
+                st->exh_probe_rejects += c.probe_rejects;
+                float ms[5];
+                for (int i = 0; i < 5; i++) cudaEventElapsedTime(&ms[i], ctx->aev[6 * p + i], ctx->aev[6 * p + i + 1]);
+                st->ms_fingerprint += ms[0];
+                st->ms_qc += ms[1];
+                st->ms_exhaustive += ms[2];
+                st->ms_exh_items += ms[3];
+                st->ms_emit += ms[4];
+                st->passes += 1;
+            }
+            st->rules += nrules;
+        }
+        return M6502_OK;
+    }
+    return set_err(ctx, M6502_E_NOMEM, "device buffers kept overflowing");
+}
+
 int check_cfg(m6502_ctx* ctx, const m6502_search_cfg* cfg) {
     if (!cfg) return set_err(ctx, M6502_E_INVAL, "cfg is NULL");
     if (cfg->semantics > M6502_SEM_GO) return set_err(ctx, M6502_E_INVAL, "bad semantics");
@@ -2036,6 +2191,7 @@ int m6502_create(m6502_ctx** out, const m6502_opts* opts) {
     bool ev_ok = true;
     for (cudaEvent_t& e : ctx->sev) ev_ok = ev_ok && cudaEventCreate(&e) == cudaSuccess;
     for (cudaEvent_t& e : ctx->sev2) ev_ok = ev_ok && cudaEventCreate(&e) == cudaSuccess;
+    for (cudaEvent_t& e : ctx->aev) ev_ok = ev_ok && cudaEventCreate(&e) == cudaSuccess;
     if (!ev_ok) {
         delete ctx;
         return M6502_E_CUDA;
@@ -2068,10 +2224,11 @@ void m6502_destroy(m6502_ctx* ctx) {
                       &ctx->st_keys2, &ctx->st_vals2, &ctx->st_rep, &ctx->st_ord, &ctx->st_verdict,
                       &ctx->st_vlist, &ctx->st_vpos, &ctx->st_sort_tmp, &ctx->c2_keys_in, &ctx->c2_idx_in,
                       &ctx->c2_sort_tmp, &ctx->go_keys, &ctx->go_keys2, &ctx->go_ord, &ctx->go_round,
-                      &ctx->go_sort_tmp, &ctx->jitems};
+                      &ctx->go_sort_tmp, &ctx->jitems, &ctx->cnt_slots};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->sev2) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : ctx->aev) if (e) cudaEventDestroy(e);
     for (auto& t : ctx->cand2) {
         if (t.keys.p) cudaFree(t.keys.p);
         if (t.idx.p) cudaFree(t.idx.p);
@@ -2234,7 +2391,9 @@ int m6502_search(m6502_ctx* ctx, const m6502_search_cfg* cfg, const uint16_t* ta
     std::memset(&st, 0, sizeof st);
     ctx->staging.clear();
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    for (uint64_t b = 0; b < n; b += ctx->pass_targets) {
+    const bool async_ok = cfg->semantics == M6502_SEM_CUDA && cfg->max_cand_len <= 1 &&
+                          n <= (uint64_t)kMaxAsyncPasses * ctx->pass_targets;
+    for (uint64_t b = async_ok ? n : 0; b < n; b += ctx->pass_targets) {   // passes one by one otherwise
         uint64_t nt = std::min<uint64_t>(ctx->pass_targets, n - b);
         const uint16_t* d_t;
         if (on_dev) {
@@ -2246,6 +2405,7 @@ int m6502_search(m6502_ctx* ctx, const m6502_search_cfg* cfg, const uint16_t* ta
         }
         TRY(run_pass(ctx, *cfg, d_t, nt, tlen, nullptr, b, &st));
     }
+    if (async_ok && n) TRY(search_async(ctx, *cfg, targets, n, tlen, on_dev, &st));
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     CK(cudaEventSynchronize(ctx->ev1));
     float ms = 0;
