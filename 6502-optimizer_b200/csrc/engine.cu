@@ -281,9 +281,16 @@ __device__ __forceinline__ uint32_t state_diff(const PairView& pv, const Fields&
     St in;
     in.a = fld(f, 0, s); in.x = fld(f, 1, s); in.y = fld(f, 2, s); in.s = fld(f, 3, s);
     in.m = fld(f, 4, s); in.s0 = fld(f, 5, s); in.s1 = fld(f, 6, s); in.p = fld(f, 7, s);
-    St t = in, c = in;
-    for (int i = 0; i < pv.tn; i++) exec(t, pv.t[i]);
-    for (int i = 0; i < pv.cn; i++) exec(c, pv.c[i]);
+    // One loop over target then candidate: a single inlined copy of the
+    // opcode switch per call site keeps the kernels' code (and instruction-
+    // cache misses) small.
+    St c = in, t = in;
+    const int n = pv.tn + pv.cn;
+    for (int i = 0; i < n; i++) {
+        if (i == pv.tn) { t = c; c = in; }
+        exec(c, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
+    }
+    if (pv.cn == 0) { t = c; c = in; }
     return ((t.a ^ c.a) & m.a) | ((t.x ^ c.x) & m.x) | ((t.y ^ c.y) & m.y) | ((t.p ^ c.p) & m.p) |
            ((t.s ^ c.s) & m.s) | ((t.m ^ c.m) & m.m) | ((t.s0 ^ c.s0) & m.s0) | ((t.s1 ^ c.s1) & m.s1);
 }
@@ -1153,9 +1160,10 @@ __device__ __forceinline__ unsigned long long algo_ops(const uint16_t* t, uint32
     return (1ull << bits) * (unsigned long long)(10 * (tn + cn) + 3);
 }
 
-// CUDA semantics: every passing survivor is a rule.
+// CUDA semantics: every passing survivor is a rule; its target is ids[t], or
+// tbase + t (the pass-local index made global) without ids.
 __global__ void k_emit_all(const Surv* __restrict__ surv, const unsigned long long* n_ptr, uint64_t n_cap,
-                           const uint32_t* __restrict__ fail, const uint64_t* __restrict__ ids, uint64_t base,
+                           const uint32_t* __restrict__ fail, const uint64_t* __restrict__ ids, uint64_t tbase,
                            uint32_t run_dead, m6502_rule* __restrict__ rules, uint64_t rcap,
                            unsigned long long* rule_ctr, Counters* cnt, int check_exh,
                            const uint16_t* __restrict__ targets, uint32_t tlen, uint32_t sweep_mode) {
@@ -1170,7 +1178,7 @@ __global__ void k_emit_all(const Surv* __restrict__ surv, const unsigned long lo
         if (pass) {
             Surv s = surv[p];
             uint32_t idx = s.c & 0x7FFFFFu;
-            r.target = ids ? ids[s.t] : base + s.t;
+            r.target = ids ? ids[s.t] : tbase + s.t;
             r.dead_flags = (uint8_t)run_dead;
             if (s.c & kSurvLen2) { r.cand_len = 2; r.cand[0] = c_tab[idx / kNumInsns]; r.cand[1] = c_tab[idx % kNumInsns]; }
             else { r.cand_len = 1; r.cand[0] = c_tab[idx]; }

@@ -312,15 +312,32 @@ def stoke_once(eng, targets, args, model=None):
     res, proofs, st = eng.stoke(targets, **kw)
     times = sorted(r["first_proof_ms"] for r in res if r["first_proof_ms"] >= 0)
     steps = sorted(r["first_proof_step"] for r in res if r["first_proof_ms"] >= 0)
+    q = lambda xs, f: xs[int(f * (len(xs) - 1))] if xs else None  # noqa: E731
     summary = {"median_ms": statistics.median(times) if times else None,
-               "p90_ms": times[int(0.9 * (len(times) - 1))] if times else None,
+               "p75_ms": q(times, 0.75), "p90_ms": q(times, 0.9),
                "median_steps": statistics.median(steps) if steps else None,
+               "p75_steps": q(steps, 0.75), "p90_steps": q(steps, 0.9),
                "proved": len(times), "censored": len(targets) - len(times),
                "proofs": st["proofs"], "candidates": st["candidates"], "verified": st["verified"],
                "undecided": st["undecided"], "epochs": st["epochs"],
                "chain_steps_per_s": st["steps"] / (st["ms_device"] / 1e3) if st["ms_device"] else None,
                "ms_device": st["ms_device"], "ms_chains": st["ms_chains"], "ms_verify": st["ms_verify"]}
     return res, summary
+
+
+def hard_target_speedup(res_u, res_l, min_steps, budget):
+    """Median ratio of first-proof steps (uniform / learned) over the targets
+    uniform STOKE needed at least min_steps for; an unproved target counts at
+    the step budget, and targets neither proposal proved are left out."""
+    ratios = []
+    for ru, rl in zip(res_u, res_l):
+        su = ru["first_proof_step"] if ru["first_proof_ms"] >= 0 else budget
+        sl = rl["first_proof_step"] if rl["first_proof_ms"] >= 0 else budget
+        if su < min_steps or (ru["first_proof_ms"] < 0 and rl["first_proof_ms"] < 0):
+            continue
+        ratios.append((su + 1) / (sl + 1))
+    return {"targets": len(ratios), "min_uniform_steps": min_steps,
+            "median_step_ratio": statistics.median(ratios) if ratios else None}
 
 
 def run_stoke(args):
@@ -340,7 +357,10 @@ def run_stoke(args):
     torch.cuda.set_device(local)
     targets = inst.draw_targets(2, 4, 8, 512, reject_pruned=False)
     eng = m6502.Engine(device=local)
-    eng.stoke(targets[:8], chains_per_target=8, steps=2000, steps_per_epoch=1000, seed=1, cost=_lib.COST_HAMMING)
+    # warm-up at full size (every device buffer allocated before the timed runs)
+    eng.stoke(targets, chains_per_target=128, steps=4 * args.stoke_first_epoch, steps_per_epoch=args.stoke_epoch,
+              first_epoch=args.stoke_first_epoch, seed=1, cost=_lib.COST_HAMMING, sweep=_lib.SWEEP_FULL,
+              stop_on_proof=True)
     learned = args.workload == "stoke-learned"
     model, train_info, train_s = None, None, None
     if learned:
@@ -351,8 +371,8 @@ def run_stoke(args):
         train_s = time.perf_counter() - t0
     clocks = ClockSampler(local)
     clocks.start()
-    _, uni = stoke_once(eng, targets, args)
-    lrn = stoke_once(eng, targets, args, model)[1] if learned else None
+    res_u, uni = stoke_once(eng, targets, args)
+    res_l, lrn = stoke_once(eng, targets, args, model) if learned else (None, None)
     clk = clocks.stop()
     main = lrn if learned else uni
     line = {"metric": "STOKE time-to-proof (median over proved targets)", "value": main["median_ms"], "unit": "ms",
@@ -373,6 +393,9 @@ def run_stoke(args):
             line["speedup_median_ms"] = uni["median_ms"] / main["median_ms"]
         if uni["median_steps"] and main["median_steps"]:
             line["speedup_median_steps"] = uni["median_steps"] / main["median_steps"]
+        # most targets fall to the first random delete under either proposal;
+        # the proposal matters on the rest
+        line["hard_targets"] = hard_target_speedup(res_u, res_l, 1000, args.stoke_steps)
         model.close()
     print(json.dumps(line), flush=True)
     eng.close()
