@@ -150,8 +150,40 @@ __host__ __device__ __forceinline__ uint64_t key_mix(uint64_t z) {
     z ^= z >> 33;
     return z;
 }
-__host__ __device__ __forceinline__ uint64_t key_step(uint64_t h, uint64_t masked_out, int v) {
-    return key_mix(h ^ (masked_out + (uint64_t)(v + 1) * 0x9E3779B97F4A7C15ull));
+// key = mix(0x6502 ^ XOR over vectors v of mix(masked output v + (v + 1) * phi)):
+// the per-vector terms are independent, so a warp computes them on 8 lanes at
+// once and combines them with 3 shuffles.
+__host__ __device__ __forceinline__ uint64_t key_term(uint64_t masked_out, int v) {
+    return key_mix(masked_out + (uint64_t)(v + 1) * 0x9E3779B97F4A7C15ull);
+}
+__host__ __device__ __forceinline__ uint64_t key_final(uint64_t x) { return key_mix(x ^ 0x6502ull); }
+
+// Warp-collective key of the outputs held by lanes 0..7 (lane v: vector v).
+__device__ __forceinline__ uint64_t warp_key(uint64_t tv, uint64_t mask, int lane) {
+    uint64_t h = lane < 8 ? key_term(tv & mask, lane) : 0ull;
+    h ^= __shfl_xor_sync(kFull, h, 1);
+    h ^= __shfl_xor_sync(kFull, h, 2);
+    h ^= __shfl_xor_sync(kFull, h, 4);
+    return key_final(__shfl_sync(kFull, h, 0));
+}
+
+// First index of a sorted array with keys[i] >= key; the warp splits the
+// range 33 ways per step (one load per lane).
+__device__ __forceinline__ uint32_t warp_lower_bound(const uint64_t* __restrict__ keys, uint32_t n, uint64_t key,
+                                                     int lane) {
+    uint32_t lo = 0, hi = n;   // the answer lies in [lo, hi]
+    while (hi - lo > 32) {
+        const uint32_t piv = lo + (uint32_t)(((uint64_t)(hi - lo) * (uint64_t)(lane + 1)) / 33u);
+        const unsigned less = __ballot_sync(kFull, keys[piv] < key);
+        const int k = __popc(less);   // pivots ascend, so the lanes below k are exactly the ones below key
+        const uint32_t plo = __shfl_sync(kFull, piv, k > 0 ? k - 1 : 0);
+        const uint32_t phi = __shfl_sync(kFull, piv, k < 32 ? k : 31);
+        const uint32_t nlo = k > 0 ? plo + 1 : lo;
+        hi = k < 32 ? phi : hi;
+        lo = nlo;
+    }
+    const uint32_t i = lo + (uint32_t)lane;
+    return lo + (uint32_t)__popc(__ballot_sync(kFull, i < hi && keys[i] < key));
 }
 
 // Survivor record: target (index within the pass) and candidate code:
@@ -523,6 +555,7 @@ struct ExhArgs {
     Counters* cnt;
     uint32_t sweep;              // M6502_SWEEP_*
     uint32_t brute;
+    uint32_t defer_bits;         // > 0: pairs with a cone above 2^defer_bits states get fail = 4 (deferred)
 };
 
 // ---------------------------------------------------------------------------
@@ -762,14 +795,8 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint16_t* __restrict__ ta
             tb += GO ? bytes_go(insn & 0xFFu) : bytes_cuda(insn & 0xFFu);
         }
         const uint64_t tv = fp_of(st);   // lane v holds the target's output on vector v
-        uint64_t key = 0x6502;
-#pragma unroll
-        for (int v = 0; v < 8; v++) key = key_step(key, __shfl_sync(kFull, tv, v) & loose, v);
-        uint32_t lo = 0, hi = nsorted;            // lower bound of key
-        while (lo < hi) {
-            uint32_t mid = (lo + hi) >> 1;
-            if (s_key[mid] < key) lo = mid + 1; else hi = mid;
-        }
+        const uint64_t key = warp_key(tv, loose, lane);
+        const uint32_t lo = warp_lower_bound(s_key, nsorted, key, lane);
         uint32_t end = lo;
         while (end < nsorted && s_key[end] == key) end++;
         if (lo == end) continue;
@@ -828,36 +855,19 @@ __global__ void k_cand2_keys(uint32_t dead, uint64_t* __restrict__ keys, uint32_
     const uint32_t n = (uint32_t)kNumInsns * (uint32_t)kNumInsns;
     for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < n; c += gridDim.x * blockDim.x) {
         const uint16_t i0 = c_tab[c / kNumInsns], i1 = c_tab[c % kNumInsns];
-        uint64_t key = 0x6502;
+        uint64_t x = 0;
         for (int v = 0; v < 8; v++) {
             St s = unpack(c_vec[v]);
             exec(s, i0);
             exec(s, i1);
-            key = key_step(key, fp_of(s) & loose, v);
+            x ^= key_term(fp_of(s) & loose, v);
         }
+        const uint64_t key = key_final(x);
         keys[c] = key;
         idx[c] = c;
     }
 }
 
-// First index of a sorted array with keys[i] >= key; the warp splits the
-// range 33 ways per step (one load per lane).
-__device__ __forceinline__ uint32_t warp_lower_bound(const uint64_t* __restrict__ keys, uint32_t n, uint64_t key,
-                                                     int lane) {
-    uint32_t lo = 0, hi = n;   // the answer lies in [lo, hi]
-    while (hi - lo > 32) {
-        const uint32_t piv = lo + (uint32_t)(((uint64_t)(hi - lo) * (uint64_t)(lane + 1)) / 33u);
-        const unsigned less = __ballot_sync(kFull, keys[piv] < key);
-        const int k = __popc(less);   // pivots ascend, so the lanes below k are exactly the ones below key
-        const uint32_t plo = __shfl_sync(kFull, piv, k > 0 ? k - 1 : 0);
-        const uint32_t phi = __shfl_sync(kFull, piv, k < 32 ? k : 31);
-        const uint32_t nlo = k > 0 ? plo + 1 : lo;
-        hi = k < 32 ? phi : hi;
-        lo = nlo;
-    }
-    const uint32_t i = lo + (uint32_t)lane;
-    return lo + (uint32_t)__popc(__ballot_sync(kFull, i < hi && keys[i] < key));
-}
 
 // QC (+ MidCheck) of targets x all length-2 candidates through the sorted
 // table.  Lane v executes the candidate on vector v.  The byte filter and
@@ -979,9 +989,7 @@ __global__ void __launch_bounds__(256) k_qc_join2(Join2Args a) {
         const bool use_exact = GO && !need_m;
         const uint64_t* skeys = use_exact ? a.ekeys : a.lkeys;
         const uint64_t km = use_exact ? exact : loose;
-        uint64_t key = 0x6502;
-#pragma unroll
-        for (int v = 0; v < 8; v++) key = key_step(key, __shfl_sync(kFull, tv, v) & km, v);
+        const uint64_t key = warp_key(tv, km, lane);
         const uint32_t lo = warp_lower_bound(skeys, a.nsorted, key, lane);
         const uint32_t hi = key == ~0ull ? a.nsorted : warp_lower_bound(skeys, a.nsorted, key + 1, lane);
         if (hi - lo <= kJoinChunk) {
@@ -1070,6 +1078,12 @@ __global__ void __launch_bounds__(256, 4) k_exhaustive(Src src, const unsigned l
                                      : __any_sync(kFull, ((lg.maxm >> lane) & 1u) && lg.mybits > kMaxConeBits);
         if (too_big) {
             if (lane == 0) a.fail[p] = 3u;   // undecided: sweep beyond the cap
+            __syncwarp();
+            continue;
+        }
+        if (a.defer_bits && !a.brute &&
+            __any_sync(kFull, ((lg.maxm >> lane) & 1u) && lg.mybits > a.defer_bits)) {
+            if (lane == 0) a.fail[p] = 4u;   // deferred: a cone above this round's budget
             __syncwarp();
             continue;
         }
@@ -1535,7 +1549,8 @@ struct m6502_ctx {
     uint32_t join_n[256] = {};
     DevBuf st_tins, st_toffs, st_tout, st_tbytes, st_chains, st_entries, st_vidx, st_proven, st_cnt, st_pidx,
         st_mex, st_probs, st_traj;
-    DevBuf st_keys, st_keys2, st_vals2, st_rep, st_ord, st_verdict, st_vlist, st_vpos, st_sort_tmp;
+    DevBuf st_keys, st_keys2, st_vals2, st_rep, st_ord, st_verdict, st_vlist, st_vpos, st_sort_tmp, st_vphase,
+        st_pphase;
 };
 
 namespace {
@@ -1657,8 +1672,9 @@ int join_table(m6502_ctx* ctx, uint32_t dead) {
     std::vector<std::pair<uint64_t, uint16_t>> v;
     for (int c = 0; c < kNumInsns; c++) {
         if (ctx->h_cmeta[c] & 0x10) continue;
-        uint64_t key = 0x6502;
-        for (int q = 0; q < 8; q++) key = key_step(key, ctx->h_cfp8[(size_t)q * kNumInsns + c] & loose, q);
+        uint64_t x = 0;
+        for (int q = 0; q < 8; q++) x ^= key_term(ctx->h_cfp8[(size_t)q * kNumInsns + c] & loose, q);
+        const uint64_t key = key_final(x);
         v.emplace_back(key, (uint16_t)c);
     }
     std::sort(v.begin(), v.end());
@@ -2007,7 +2023,8 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
 // buffers (nothing is dropped).  Returns M6502_E_INVAL when the search does
 // not fit this path.
 int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* targets, uint64_t n, uint32_t tlen,
-                 bool on_dev, m6502_stats* st) {
+                 bool on_dev, m6502_stats* st, m6502_rule* out, uint64_t out_cap, bool* delivered) {
+    *delivered = false;
     const uint64_t P = ctx->pass_targets;
     const uint64_t npass = (n + P - 1) / P;
     if (npass == 0 || npass > (uint64_t)kMaxAsyncPasses) return set_err(ctx, M6502_E_INVAL, "too many passes");
@@ -2100,11 +2117,18 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
         const uint64_t nrules = hc[0].rules;
         if (nrules > rcap) { rcap = nrules + nrules / 4 + 1024; redo = true; }
         if (redo) continue;
-        const size_t old = ctx->staging.size();
-        ctx->staging.resize(old + nrules);
-        if (nrules)
-            CK(cudaMemcpyAsync(ctx->staging.data() + old, ctx->rules.p, nrules * sizeof(m6502_rule),
-                               cudaMemcpyDeviceToHost, ctx->stream));
+        if (out && nrules <= out_cap && ctx->staging.empty()) {   // straight into the caller's buffer
+            if (nrules)
+                CK(cudaMemcpyAsync(out, ctx->rules.p, nrules * sizeof(m6502_rule), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+            *delivered = true;
+        } else {
+            const size_t old = ctx->staging.size();
+            ctx->staging.resize(old + nrules);
+            if (nrules)
+                CK(cudaMemcpyAsync(ctx->staging.data() + old, ctx->rules.p, nrules * sizeof(m6502_rule),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+        }
         CK(cudaStreamSynchronize(ctx->stream));
         if (st) {
             for (uint64_t p = 0; p < npass; p++) {
@@ -2232,7 +2256,7 @@ void m6502_destroy(m6502_ctx* ctx) {
                       &ctx->st_keys2, &ctx->st_vals2, &ctx->st_rep, &ctx->st_ord, &ctx->st_verdict,
                       &ctx->st_vlist, &ctx->st_vpos, &ctx->st_sort_tmp, &ctx->c2_keys_in, &ctx->c2_idx_in,
                       &ctx->c2_sort_tmp, &ctx->go_keys, &ctx->go_keys2, &ctx->go_ord, &ctx->go_round,
-                      &ctx->go_sort_tmp, &ctx->jitems, &ctx->cnt_slots};
+                      &ctx->go_sort_tmp, &ctx->jitems, &ctx->cnt_slots, &ctx->st_vphase, &ctx->st_pphase};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->sev2) if (e) cudaEventDestroy(e);
@@ -2413,13 +2437,18 @@ int m6502_search(m6502_ctx* ctx, const m6502_search_cfg* cfg, const uint16_t* ta
         }
         TRY(run_pass(ctx, *cfg, d_t, nt, tlen, nullptr, b, &st));
     }
-    if (async_ok && n) TRY(search_async(ctx, *cfg, targets, n, tlen, on_dev, &st));
+    bool delivered = false;
+    if (async_ok && n) TRY(search_async(ctx, *cfg, targets, n, tlen, on_dev, &st, out, cap, &delivered));
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     CK(cudaEventSynchronize(ctx->ev1));
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     st.ms_device = ms;
     if (stats) *stats = st;
+    if (delivered) {
+        if (n_out) *n_out = st.rules;
+        return M6502_OK;
+    }
     return finish(ctx, out, cap, n_out);
 }
 

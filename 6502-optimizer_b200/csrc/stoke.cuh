@@ -45,6 +45,7 @@ struct StokeCounters {
 };
 
 constexpr uint32_t kVerifyBatch = 8;   // distinct candidates per target per round under stop_on_proof
+constexpr uint32_t kStokeDeferBits = 24;   // first verification phase: cones of at most 2^24 states
 
 // Sort key of an entry: target, length, then a 33-bit hash of the
 // instructions, so that identical (target, candidate) pairs are adjacent and
@@ -436,15 +437,18 @@ __global__ void __launch_bounds__(1024) k_stoke_dedupe(const uint64_t* __restric
 }
 
 // One verification round: the distinct pairs whose per-target ordinal lies
-// in [lo, hi), skipping targets already proved when stop_on_proof is set.
+// in [lo, hi) -- or, with deferred_only, the pairs an earlier round deferred
+// -- skipping targets already proved when stop_on_proof is set.
 __global__ void k_stoke_select(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ vals,
                                const uint32_t* __restrict__ rep, const uint32_t* __restrict__ ord, uint32_t lo,
                                uint32_t hi, uint32_t stop_on_proof, const uint32_t* __restrict__ proven,
+                               const uint32_t* __restrict__ verdict, uint32_t deferred_only,
                                uint32_t* __restrict__ vlist, uint32_t* __restrict__ vpos,
                                StokeCounters* __restrict__ sc) {
     const uint32_t n = (uint32_t)sc->vec_ok;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        if (rep[i] != i || ord[i] < lo || ord[i] >= hi) continue;
+        if (rep[i] != i) continue;
+        if (deferred_only ? verdict[i] != 4u : (ord[i] < lo || ord[i] >= hi)) continue;
         if (stop_on_proof && proven[(uint32_t)(keys[i] >> 38)]) continue;
         const unsigned long long p = atomicAdd(&sc->round_n, 1ull);
         vlist[p] = vals[i];
@@ -456,30 +460,33 @@ __global__ void k_stoke_select(const uint64_t* __restrict__ keys, const uint32_t
 // targets are marked.
 __global__ void k_stoke_verdicts(const uint32_t* __restrict__ fail, const uint32_t* __restrict__ vpos,
                                  const uint64_t* __restrict__ keys, uint32_t* __restrict__ verdict,
-                                 uint32_t* __restrict__ proven, StokeCounters* __restrict__ sc) {
+                                 uint8_t* __restrict__ vphase, uint32_t phase, uint32_t* __restrict__ proven,
+                                 StokeCounters* __restrict__ sc) {
     const uint32_t n = (uint32_t)sc->round_n;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += gridDim.x * blockDim.x) {
         const uint32_t i = vpos[p];
         verdict[i] = fail[p];
+        vphase[i] = (uint8_t)phase;
         if (fail[p] == 0) proven[(uint32_t)(keys[i] >> 38)] = 1;
         if (fail[p] == 3) atomicAdd(&sc->undecided, 1ull);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) sc->verified += n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) sc->verified += n;   // deferred pairs count again when swept
 }
 
 // Every vec_ok entry whose distinct pair was proved becomes a proof (as in
 // the reference, each chain's verified best is one result); its chain
 // restarts (search.go:151-154).
 __global__ void k_stoke_collect(const uint32_t* __restrict__ vals, const uint32_t* __restrict__ rep,
-                                const uint32_t* __restrict__ verdict, const StokeEntry* __restrict__ entries,
-                                StokeCounters* __restrict__ sc, StokeChain* __restrict__ chains,
-                                uint32_t* __restrict__ proof_idx, uint64_t pcap) {
+                                const uint32_t* __restrict__ verdict, const uint8_t* __restrict__ vphase,
+                                const StokeEntry* __restrict__ entries, StokeCounters* __restrict__ sc,
+                                StokeChain* __restrict__ chains, uint32_t* __restrict__ proof_idx,
+                                uint8_t* __restrict__ proof_phase, uint64_t pcap) {
     const uint32_t n = (uint32_t)sc->vec_ok;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (verdict[rep[i]] != 0) continue;
         const uint32_t e = vals[i];
         const unsigned long long k = atomicAdd(&sc->proofs, 1ull);
-        if (k < pcap) proof_idx[k] = e;
+        if (k < pcap) { proof_idx[k] = e; proof_phase[k] = vphase[rep[i]]; }
         chains[entries[e].chain].status = 0;
     }
 }
@@ -549,6 +556,8 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
     TRY(ensure(ctx, ctx->st_verdict, ecap * 4));
     TRY(ensure(ctx, ctx->st_vlist, ecap * 4));
     TRY(ensure(ctx, ctx->st_vpos, ecap * 4));
+    TRY(ensure(ctx, ctx->st_vphase, ecap));
+    TRY(ensure(ctx, ctx->st_pphase, ecap));
     size_t sort_bytes = 0;
     CK(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (const uint64_t*)nullptr, (uint64_t*)nullptr,
                                        (const uint32_t*)nullptr, (uint32_t*)nullptr, (int)ecap, 0, 64, ctx->stream));
@@ -592,7 +601,7 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
     std::vector<StokeEntry> h_entries;
     std::vector<m6502_stoke_proof> found;
     std::vector<double> first_ms(n_targets, -1.0);
-    std::vector<uint64_t> first_step(n_targets, 0);
+    std::vector<uint64_t> first_step(n_targets, 0), first_epoch(n_targets, 0);
     m6502_stoke_stats st;
     std::memset(&st, 0, sizeof st);
     StokeCounters* sc = (StokeCounters*)ctx->st_cnt.p;
@@ -649,23 +658,27 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
             CK(cudaStreamSynchronize(ctx->stream));
             max_ord = (uint32_t)hv.max_ord;
         }
-        // Rounds of at most kVerifyBatch distinct candidates per target under
-        // stop_on_proof (a target proved in one round is skipped in the next);
-        // a single round of all of them otherwise.
+        // Phase 0: rounds of at most kVerifyBatch distinct candidates per
+        // target under stop_on_proof (a target proved in one round is skipped
+        // in the next; a single round of all of them otherwise), sweeping only
+        // pairs whose cones stay within 2^kStokeDeferBits states.  Phase 1:
+        // the deferred pairs of targets still unproved.  Proofs of phase 0 are
+        // timed at its end, so one expensive pair does not delay the rest.
         const uint32_t batch = cfg->stop_on_proof ? kVerifyBatch : 0xFFFFFFFFu;
         StokeSource src{(const StokeEntry*)ctx->st_entries.p, (const uint32_t*)ctx->st_vlist.p, tg, cfg->dead_flags};
-        for (uint32_t lo = 0; n_ok && lo <= max_ord; lo = (batch > 0xFFFFFFFFu - lo) ? 0xFFFFFFFFu : lo + batch) {
-            const uint32_t hi = batch > 0xFFFFFFFFu - lo ? 0xFFFFFFFFu : lo + batch;
+        auto verify_round = [&](uint32_t lo, uint32_t hi, uint32_t phase) -> int {
             CK(cudaMemsetAsync(&sc->round_n, 0, sizeof(unsigned long long), ctx->stream));
             k_stoke_select<<<ctx->sms * 4, 256, 0, ctx->stream>>>(
                 (const uint64_t*)ctx->st_keys2.p, (const uint32_t*)ctx->st_vals2.p, (const uint32_t*)ctx->st_rep.p,
                 (const uint32_t*)ctx->st_ord.p, lo, hi, cfg->stop_on_proof, (const uint32_t*)ctx->st_proven.p,
-                (uint32_t*)ctx->st_vlist.p, (uint32_t*)ctx->st_vpos.p, sc);
+                (const uint32_t*)ctx->st_verdict.p, phase, (uint32_t*)ctx->st_vlist.p, (uint32_t*)ctx->st_vpos.p,
+                sc);
             CKL("k_stoke_select");
             for (int attempt = 0;; attempt++) {
                 TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
                 CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), ctx->stream));
-                ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg->sweep, 0};
+                ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg->sweep, 0,
+                           phase == 0 ? kStokeDeferBits : 0u};
                 k_exhaustive<StokeSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &sc->round_n, ecap, ea);
                 CKL("k_exhaustive(stoke)");
                 k_exh_items<StokeSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
@@ -679,15 +692,22 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
             }
             k_stoke_verdicts<<<ctx->sms * 4, 256, 0, ctx->stream>>>(
                 (const uint32_t*)ctx->fail.p, (const uint32_t*)ctx->st_vpos.p, (const uint64_t*)ctx->st_keys2.p,
-                (uint32_t*)ctx->st_verdict.p, (uint32_t*)ctx->st_proven.p, sc);
+                (uint32_t*)ctx->st_verdict.p, (uint8_t*)ctx->st_vphase.p, phase, (uint32_t*)ctx->st_proven.p, sc);
             CKL("k_stoke_verdicts");
+            return M6502_OK;
+        };
+        for (uint32_t lo = 0; n_ok && lo <= max_ord; lo = (batch > 0xFFFFFFFFu - lo) ? 0xFFFFFFFFu : lo + batch) {
+            const uint32_t hi = batch > 0xFFFFFFFFu - lo ? 0xFFFFFFFFu : lo + batch;
+            TRY(verify_round(lo, hi, 0));
             if (hi == 0xFFFFFFFFu) break;
         }
+        CK(cudaEventRecord(ctx->sev[3], ctx->stream));   // phase-0 proofs are complete here
+        if (n_ok) TRY(verify_round(0, 0, 1));
         if (n_ok) {
             k_stoke_collect<<<ctx->sms * 4, 256, 0, ctx->stream>>>(
                 (const uint32_t*)ctx->st_vals2.p, (const uint32_t*)ctx->st_rep.p, (const uint32_t*)ctx->st_verdict.p,
-                (const StokeEntry*)ctx->st_entries.p, sc, (StokeChain*)ctx->st_chains.p, (uint32_t*)ctx->st_pidx.p,
-                ecap);
+                (const uint8_t*)ctx->st_vphase.p, (const StokeEntry*)ctx->st_entries.p, sc,
+                (StokeChain*)ctx->st_chains.p, (uint32_t*)ctx->st_pidx.p, (uint8_t*)ctx->st_pphase.p, ecap);
             CKL("k_stoke_collect");
         }
         CK(cudaEventRecord(ctx->sev[2], ctx->stream));
@@ -719,32 +739,43 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
         }
         if (hc.proofs) {
             std::vector<uint32_t> pidx(hc.proofs);
+            std::vector<uint8_t> pph(hc.proofs);
             h_entries.resize(std::min<uint64_t>(hc.entries, ecap));
             CK(cudaMemcpyAsync(pidx.data(), ctx->st_pidx.p, pidx.size() * 4, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaMemcpyAsync(pph.data(), ctx->st_pphase.p, pph.size(), cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaMemcpyAsync(h_entries.data(), ctx->st_entries.p, h_entries.size() * sizeof(StokeEntry),
                                cudaMemcpyDeviceToHost, ctx->stream));
             CK(cudaStreamSynchronize(ctx->stream));
+            float a_ms = 0;   // end of verification phase 0
+            cudaEventElapsedTime(&a_ms, ctx->ev0, ctx->sev[3]);
+            std::vector<uint32_t> order(pidx.size());
+            for (size_t k = 0; k < order.size(); k++) order[k] = (uint32_t)k;
             // deterministic order within the epoch: target, step, chain
-            std::sort(pidx.begin(), pidx.end(), [&](uint32_t a, uint32_t b) {
-                const StokeEntry &x = h_entries[a], &y = h_entries[b];
+            std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
+                const StokeEntry &x = h_entries[pidx[a]], &y = h_entries[pidx[b]];
                 if (x.target != y.target) return x.target < y.target;
                 if (x.step != y.step) return x.step < y.step;
                 return x.chain < y.chain;
             });
-            for (uint32_t e : pidx) {
-                const StokeEntry& en = h_entries[e];
+            for (uint32_t k : order) {
+                const StokeEntry& en = h_entries[pidx[k]];
+                const double pms = pph[k] ? e_ms : a_ms;
                 m6502_stoke_proof pr;
                 std::memset(&pr, 0, sizeof pr);
-                pr.target = en.target; pr.chain = en.chain; pr.step = en.step; pr.ms = e_ms;
+                pr.target = en.target; pr.chain = en.chain; pr.step = en.step; pr.ms = pms;
                 pr.cand_len = en.len; pr.dead_flags = en.dead_flags;
                 std::memcpy(pr.cand, en.ins, sizeof pr.cand);
                 found.push_back(pr);
-                if (first_ms[en.target] < 0) {
-                    first_ms[en.target] = e_ms;
-                    first_step[en.target] = en.step;
+                const uint32_t t = en.target;
+                if (first_ms[t] < 0) {
+                    first_ms[t] = pms;
+                    first_step[t] = en.step;
+                    first_epoch[t] = st.epochs;
                     proven_targets++;
-                } else if (en.step < first_step[en.target] && first_ms[en.target] == e_ms) {
-                    first_step[en.target] = en.step;
+                } else if (first_epoch[t] == st.epochs &&
+                           (pms < first_ms[t] || (pms == first_ms[t] && en.step < first_step[t]))) {
+                    first_ms[t] = pms;
+                    first_step[t] = en.step;
                 }
             }
             st.proofs += hc.proofs;

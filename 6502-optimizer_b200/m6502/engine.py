@@ -106,11 +106,11 @@ class Engine:
     def _run(self, fn, cap, *args):
         st = _lib.Stats()
         n_out = ctypes.c_uint64(0)
-        out = np.zeros(max(cap, 1), dtype=_lib.RULE_DTYPE)
+        out = np.empty(max(cap, 1), dtype=_lib.RULE_DTYPE)
         rc = fn(*args, out.ctypes.data_as(ctypes.c_void_p), cap, ctypes.byref(n_out), ctypes.byref(st))
         if rc == _lib.M6502_E_OVERFLOW:   # the rest of the rules stay staged: fetch them, no re-run
             n = int(n_out.value)
-            full = np.zeros(n, dtype=_lib.RULE_DTYPE)
+            full = np.empty(n, dtype=_lib.RULE_DTYPE)
             full[:cap] = out[:cap]
             rest = ctypes.c_uint64(0)
             rc = self._L.m6502_fetch_rules(self._ctx, full[cap:].ctypes.data_as(ctypes.c_void_p), n - cap,

@@ -286,7 +286,9 @@ def run_engine(args):
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
             "e2e": {"value": e2e_value, "unit": "pair-checks/s", "h2d_bytes_per_step": int(shard.nbytes),
                     "d2h_bytes_per_step": int(e2e_rules * 16 + 8 * 16 * s0["passes"])},
-            "gpu_launches": int(5 * s0["passes"] * args.steps),
+            # per pass: QC join, exhaustive, work items, emit (the join computes the
+            # targets' outputs itself, so no fingerprint launch)
+            "gpu_launches": int(4 * s0["passes"] * args.steps),
         }
         if world == 1 and not args.no_cpu_baseline:
             rate, kind, ns, stride, dt = cpu_reference_rate(all_targets, args.cpu_sample, os.cpu_count() or 1)

@@ -271,7 +271,8 @@ typedef struct m6502_stoke_cfg {
 typedef struct m6502_stoke_proof {
     uint32_t target, chain;
     uint64_t step;              /* chain step that found the rewrite */
-    double ms;                  /* device time from the call's start to the proof round */
+    double ms;                  /* device time from the call's start to the end of the verification
+                                   phase that proved it */
     uint16_t cand[16];
     uint8_t cand_len;
     uint8_t dead_flags;         /* FlagDiff of a masked run (search.go:105-108), else 0 */
