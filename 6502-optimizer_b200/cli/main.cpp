@@ -13,12 +13,14 @@
 //
 // All checking runs on the GPU through the C ABI; there is no CPU path.
 #include <algorithm>
+#include <cctype>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iostream>
+#include <iterator>
 #include <map>
 #include <string>
 #include <vector>
@@ -471,7 +473,165 @@ void usage() {
                  "  enumerate      enumerate all target sequences and find shorter replacements\n"
                  "  target         find the optimal replacement for one instruction sequence\n"
                  "  verify-jsonl   verify JSONL rules with ExhaustiveCheck on the GPU\n"
-                 "  stoke          STOKE stochastic search (batched MCMC chains on the GPU)\n");
+                 "  stoke          STOKE stochastic search (batched MCMC chains on the GPU)\n"
+                 "  export         export a rules JSON file as Go peephole code (-f go)\n");
+}
+
+// ---- export: the JSON rule array (WriteJSON's layout) -> Go peephole code ----
+
+// Minimal reader of the JSON array that `enumerate --output` writes
+// (pkg/result/output.go:21-35 layout): per object the string arrays
+// "source" and "replacement" and the integers "bytes_saved",
+// "cycles_saved"; other keys are skipped.
+struct JsonRule {
+    std::vector<std::string> source, replacement;
+    long bytes_saved = 0, cycles_saved = 0;
+};
+
+struct JsonReader {
+    const std::string& s;
+    size_t i = 0;
+    explicit JsonReader(const std::string& text) : s(text) {}
+    void ws() { while (i < s.size() && std::isspace((unsigned char)s[i])) i++; }
+    bool eat(char c) { ws(); if (i < s.size() && s[i] == c) { i++; return true; } return false; }
+    bool str(std::string* out) {
+        ws();
+        if (i >= s.size() || s[i] != '"') return false;
+        std::string r;
+        for (i++; i < s.size() && s[i] != '"'; i++) {
+            if (s[i] == '\\' && i + 1 < s.size()) i++;
+            r += s[i];
+        }
+        if (i >= s.size()) return false;
+        i++;
+        *out = r;
+        return true;
+    }
+    bool num(long* out) {
+        ws();
+        size_t j = i;
+        if (j < s.size() && (s[j] == '-' || s[j] == '+')) j++;
+        while (j < s.size() && std::isdigit((unsigned char)s[j])) j++;
+        if (j == i) return false;
+        *out = std::strtol(s.substr(i, j - i).c_str(), nullptr, 10);
+        i = j;
+        return true;
+    }
+    bool skip_value() {   // a value not needed: string, number, literal, array or object
+        ws();
+        std::string tmp;
+        long n;
+        if (i < s.size() && s[i] == '"') return str(&tmp);
+        if (i < s.size() && (s[i] == '[' || s[i] == '{')) {
+            const char open = s[i], close = open == '[' ? ']' : '}';
+            i++;
+            if (eat(close)) return true;
+            do {
+                if (open == '{' && !(str(&tmp) && eat(':'))) return false;
+                if (!skip_value()) return false;
+            } while (eat(','));
+            return eat(close);
+        }
+        if (num(&n)) return true;
+        for (const char* lit : {"true", "false", "null"})
+            if (s.compare(i, std::strlen(lit), lit) == 0) { i += std::strlen(lit); return true; }
+        return false;
+    }
+    bool str_array(std::vector<std::string>* out) {
+        if (!eat('[')) return false;
+        if (eat(']')) return true;
+        do {
+            std::string v;
+            if (!str(&v)) return false;
+            out->push_back(v);
+        } while (eat(','));
+        return eat(']');
+    }
+    bool rules(std::vector<JsonRule>* out) {
+        if (!eat('[')) return false;
+        if (eat(']')) return true;
+        do {
+            JsonRule r;
+            if (!eat('{')) return false;
+            if (!eat('}')) {
+                do {
+                    std::string key;
+                    if (!str(&key) || !eat(':')) return false;
+                    bool ok;
+                    if (key == "source") ok = str_array(&r.source);
+                    else if (key == "replacement") ok = str_array(&r.replacement);
+                    else if (key == "bytes_saved") ok = num(&r.bytes_saved);
+                    else if (key == "cycles_saved") ok = num(&r.cycles_saved);
+                    else ok = skip_value();
+                    if (!ok) return false;
+                } while (eat(','));
+                if (!eat('}')) return false;
+            }
+            out->push_back(r);
+        } while (eat(','));
+        return eat(']');
+    }
+};
+
+// Go's %q of a disassembled instruction (printable ASCII: quote and backslash escaped).
+std::string go_quote(const std::string& s) { return json_str(s); }
+
+// export -f go (cmd/6502opt/main.go:147-194, WriteGoCode pkg/result/output.go:47-75).
+// As in the reference, the JSON's dead_flags are not carried into the code.
+int cmd_export(const Args& a) {
+    if (a.pos.size() != 1) { std::fprintf(stderr, "usage: 6502opt export [-f go] rules.json\n"); return 1; }
+    const std::string fmt = a.get("-f", a.get("--format", "go"));
+    std::ifstream in(a.pos[0]);
+    if (!in) { std::fprintf(stderr, "open %s: no such file\n", a.pos[0].c_str()); return 1; }
+    std::string text((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
+    std::vector<JsonRule> jr;
+    JsonReader rd(text);
+    if (!rd.rules(&jr)) { std::fprintf(stderr, "invalid rules JSON: %s\n", a.pos[0].c_str()); return 1; }
+    if (fmt != "go") { std::fprintf(stderr, "unknown format: %s\n", fmt.c_str()); return 1; }
+    struct Parsed { std::vector<uint16_t> src, rep; long b, c; };
+    std::vector<Parsed> rules;
+    auto parse_slice = [](const std::vector<std::string>& v, std::vector<uint16_t>* out, std::string* bad) {
+        for (const std::string& x : v) {
+            uint16_t one[2];
+            if (m6502_parse(x.c_str(), one, 2) != 1) { *bad = x; return false; }
+            out->push_back(one[0]);
+        }
+        return true;
+    };
+    for (const JsonRule& r : jr) {
+        Parsed p{{}, {}, r.bytes_saved, r.cycles_saved};
+        std::string bad;
+        if (!parse_slice(r.source, &p.src, &bad)) {
+            std::fprintf(stderr, "skipping rule (bad source): %s\n", bad.c_str());
+            continue;
+        }
+        if (!parse_slice(r.replacement, &p.rep, &bad)) {
+            std::fprintf(stderr, "skipping rule (bad replacement): %s\n", bad.c_str());
+            continue;
+        }
+        rules.push_back(p);
+    }
+    auto join = [](const std::vector<uint16_t>& v) {
+        std::string s;
+        for (size_t k = 0; k < v.size(); k++) { if (k) s += " : "; s += disasm(v[k]); }
+        return s;
+    };
+    auto slice = [](const std::vector<uint16_t>& v) {
+        std::string s = "[]string{";
+        for (size_t k = 0; k < v.size(); k++) { if (k) s += ", "; s += go_quote(disasm(v[k])); }
+        return s + "}";
+    };
+    std::printf("package peephole\n\n// Generated by 6502opt. DO NOT EDIT.\n\n");
+    std::printf("type PeepholeRule struct {\n\tSource      []string\n\tReplacement []string\n"
+                "\tBytesSaved  int\n\tCyclesSaved int\n\tDeadFlags   string\n}\n\n");
+    std::printf("var Rules = []PeepholeRule{\n");
+    for (const Parsed& p : rules) {
+        std::printf("\t// %s -> %s (-%ld bytes, -%ld cycles)\n", join(p.src).c_str(), join(p.rep).c_str(), p.b, p.c);
+        std::printf("\t{Source: %s, Replacement: %s, BytesSaved: %ld, CyclesSaved: %ld},\n", slice(p.src).c_str(),
+                    slice(p.rep).c_str(), p.b, p.c);
+    }
+    std::printf("}\n");
+    return 0;
 }
 
 }  // namespace
@@ -484,6 +644,7 @@ int main(int argc, char** argv) {
     if (cmd == "target") return cmd_target(a);
     if (cmd == "verify-jsonl") return cmd_verify(a);
     if (cmd == "stoke") return cmd_stoke(a);
+    if (cmd == "export") return cmd_export(a);
     usage();
     return 1;
 }

@@ -7,9 +7,9 @@ engine (libm6502gpu.so).
   search  -- pkg/search/search.go: Config, Run, SearchSingle(Masked)
   result  -- pkg/result: Rule, DeadFlagDesc, JSON and JSONL output
 """
-from . import _lib, inst, result  # noqa: F401
-from ._lib import (CHECK_ALL, CHECK_EXH, CHECK_MID, CHECK_QC, EXH_BRUTE, EXH_CONES,  # noqa: F401
-                   SEM_CUDA, SEM_GO, SWEEP_FULL, SWEEP_REFERENCE, M6502Error)
+from . import _lib, inst, mlp, result  # noqa: F401
+from ._lib import (CHECK_ALL, CHECK_EXH, CHECK_MID, CHECK_QC, COST_HAMMING, COST_REF,  # noqa: F401
+                   EXH_BRUTE, EXH_CONES, SEM_CUDA, SEM_GO, SWEEP_FULL, SWEEP_REFERENCE, M6502Error)
 from .engine import (DeadAll, DeadNone, Engine, ExhaustiveCheck, ExhaustiveCheckMasked,  # noqa: F401
                      FlagDiff, Fingerprint, MidCheck, MidCheckMasked, QuickCheck,
                      QuickCheckMasked, ShouldPrune, default_engine)
