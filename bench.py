@@ -169,9 +169,10 @@ def run_engine(args):
     torch.cuda.set_device(local)
     import m6502
     from m6502 import inst, _lib
+    from m6502.distributed import shard_indices
 
     all_targets = inst.enumerate_targets(2, args.first_op, args.last_op)
-    shard = np.ascontiguousarray(all_targets[rank::world])
+    shard = np.ascontiguousarray(all_targets[shard_indices(len(all_targets), rank, world)])
     n = len(shard)
     eng = m6502.Engine(device=local)
     stream = torch.cuda.ExternalStream(eng.stream, device=local)
