@@ -48,7 +48,7 @@ constexpr int kMaxSeq = 16;          // longest sequence the pairwise API takes
 constexpr int kWarpsPerBlock = 8;    // 256-thread CTAs
 constexpr uint64_t kSmallSweep = 1ull << 13;  // sweep in-warp up to this many states
 constexpr uint64_t kProbe = 1ull << 12;       // in-warp probe of a large cone
-constexpr uint64_t kChunk = 1ull << 13;       // states per work item (at least)
+constexpr uint64_t kChunk = 1ull << 11;       // states per work item (at least)
 constexpr uint64_t kMaxItemsPerCone = 1ull << 16;   // larger cones get larger items
 // Largest cone a pair may need swept (2^34 states, about 0.1 s of the whole
 // GPU).  Pairs of long sequences that read many registers can need far

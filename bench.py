@@ -144,6 +144,12 @@ def run_reference(args):
         dist.destroy_process_group()
 
 
+# Issue-slot utilisation (smsp__issue_active.avg.pct_of_peak_sustained_active)
+# of the committed ncu captures in profiles/ (k_exhaustive_len2.md,
+# k_qc_join_len2.md, k_exh_items_len2.md).
+ISSUE_ACTIVE = {"k_exhaustive": 0.735, "k_qc_join": 0.701, "k_exh_items": 0.246}
+
+
 def load_traffic():
     """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of
     each kernel from the committed ncu summary, profiles/traffic.txt."""
@@ -244,6 +250,8 @@ def run_engine(args):
         exh_ms = avg("ms_exhaustive") + avg("ms_exh_items")
         qc_ms = avg("ms_qc")
         exh_achieved = s0["exh_algo_ops"] / (exh_ms / 1e3) if exh_ms > 0 else 0.0
+        exh_exec = ((s0["exh_states"] + 64 * s0["exh_checked"]) * (10 * 3 + 3) / (exh_ms / 1e3)
+                    if exh_ms > 0 else 0.0)
         qc_algo = 13 * s0["pairs"] + 13 * (7 + 24) * s0["qc_hits"]
         qc_achieved = qc_algo / (qc_ms / 1e3) if qc_ms > 0 else 0.0
         stages = {"fingerprint_ms": avg("ms_fingerprint"), "qc_mid_ms": qc_ms,
@@ -281,7 +289,11 @@ def run_engine(args):
                          "peak_basis": f"{sms} SMs x 128 int32 lanes x {f_mhz:.0f} MHz (median SM clock sampled)",
                          "note": "exhaustive work is counted as the full product sweep; the cone "
                                  "decomposition evaluates fewer states, so frac may exceed 1 "
-                                 "(emulation-equivalent)"},
+                                 "(emulation-equivalent)",
+                         # the states the kernels actually evaluated (cone sweeps + 64-state
+                         # probes) at the same 10 ops per instruction + 3 per compare
+                         "executed": exh_exec / 1e12, "executed_frac": exh_exec / peak_lane_ops,
+                         "issue_active_ncu": ISSUE_ACTIVE.get(dominant)},
             "roofline_qc": {"achieved": qc_achieved / 1e12, "unit": "Tlane-op/s",
                             "frac": qc_achieved / peak_lane_ops},
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
