@@ -309,13 +309,23 @@ __device__ __forceinline__ OutMask out_mask(uint64_t om) {
 
 // Nonzero when target and candidate disagree on a compared output from
 // the input state with index s.
-__device__ __forceinline__ uint32_t state_diff(const PairView& pv, const Fields& f, const OutMask& m, uint64_t s) {
+__device__ __forceinline__ St decode_state(const Fields& f, uint64_t s) {
     St in;
     in.a = fld(f, 0, s); in.x = fld(f, 1, s); in.y = fld(f, 2, s); in.s = fld(f, 3, s);
     in.m = fld(f, 4, s); in.s0 = fld(f, 5, s); in.s1 = fld(f, 6, s); in.p = fld(f, 7, s);
-    // One loop over target then candidate: a single inlined copy of the
-    // opcode switch per call site keeps the kernels' code (and instruction-
-    // cache misses) small.
+    return in;
+}
+
+__device__ __forceinline__ uint32_t out_diff(const St& t, const St& c, const OutMask& m) {
+    return ((t.a ^ c.a) & m.a) | ((t.x ^ c.x) & m.x) | ((t.y ^ c.y) & m.y) | ((t.p ^ c.p) & m.p) |
+           ((t.s ^ c.s) & m.s) | ((t.m ^ c.m) & m.m) | ((t.s0 ^ c.s0) & m.s0) | ((t.s1 ^ c.s1) & m.s1);
+}
+
+// Target and candidate on one state: one loop over target then candidate (a
+// single inlined copy of the opcode switch per call site keeps the code, and
+// instruction-cache misses, small).
+__device__ __forceinline__ uint32_t state_diff(const PairView& pv, const Fields& f, const OutMask& m, uint64_t s) {
+    const St in = decode_state(f, s);
     St c = in, t = in;
     const int n = pv.tn + pv.cn;
     for (int i = 0; i < n; i++) {
@@ -323,9 +333,26 @@ __device__ __forceinline__ uint32_t state_diff(const PairView& pv, const Fields&
         exec(c, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
     }
     if (pv.cn == 0) { t = c; c = in; }
-    return ((t.a ^ c.a) & m.a) | ((t.x ^ c.x) & m.x) | ((t.y ^ c.y) & m.y) | ((t.p ^ c.p) & m.p) |
-           ((t.s ^ c.s) & m.s) | ((t.m ^ c.m) & m.m) | ((t.s0 ^ c.s0) & m.s0) | ((t.s1 ^ c.s1) & m.s1);
+    return out_diff(t, c, m);
 }
+
+// Target and candidate on two states per lane: one loop over target then
+// candidate (a single inlined copy of the opcode switch per call site keeps
+// the code, and instruction-cache misses, small) and one dispatch per
+// instruction for both states (exec2).  The inputs are decoded again for the
+// candidate instead of being kept live.
+__device__ __forceinline__ uint32_t state_diff2(const PairView& pv, const Fields& f, const OutMask& m, uint64_t sa,
+                                                uint64_t sb) {
+    St c0 = decode_state(f, sa), c1 = decode_state(f, sb), t0 = c0, t1 = c1;
+    const int n = pv.tn + pv.cn;
+    for (int i = 0; i < n; i++) {
+        if (i == pv.tn) { t0 = c0; t1 = c1; c0 = decode_state(f, sa); c1 = decode_state(f, sb); }
+        exec2(c0, c1, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
+    }
+    if (pv.cn == 0) { t0 = c0; t1 = c1; c0 = decode_state(f, sa); c1 = decode_state(f, sb); }
+    return out_diff(t0, c0, m) | out_diff(t1, c1, m);
+}
+
 
 // Probe: 64 pseudo-random states of the pair's whole sweep domain, all
 // outputs compared.  A mismatch anywhere in the domain decides the pair
@@ -335,7 +362,7 @@ __device__ __forceinline__ bool probe_domain(const PairView& pv, uint32_t swept,
     Fields f = make_fields(swept, swept, rep);
     const OutMask m = out_mask(cmp_mask(dead));
     const uint64_t dom = (f.bits >= 64) ? ~0ull : ((1ull << f.bits) - 1);
-    for (int it = 0; it < 2; it++) {
+    for (int it = 0; it < 2; it++) {   // 32 states at a time: most failing pairs fail in the first
         uint64_t z = salt + (uint64_t)(lane + 32 * it) * 0x9E3779B97F4A7C15ull;
         z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
         z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
@@ -349,19 +376,30 @@ __device__ __forceinline__ bool probe_domain(const PairView& pv, uint32_t swept,
 // on the compared outputs in every state.  Warp-collective.  When `stop`
 // becomes nonzero (another item of the same pair failed) the sweep ends
 // early; its result is then irrelevant.
+// PER_LANE = 2: two states per lane and opcode dispatch (the work items'
+// long sweeps); 1: one (the in-warp sweeps of small cones, where the extra
+// registers cost more than the shared dispatch saves).
+template <int PER_LANE>
 __device__ __forceinline__ bool sweep_states(const PairView& pv, const Fields& f, uint64_t om, uint64_t s0,
                                              uint64_t s1, const volatile uint32_t* stop, unsigned long long* nstates,
                                              int lane) {
     const OutMask m = out_mask(om);
     uint64_t iter = 0;
-    for (uint64_t b = s0; b < s1; b += 32, iter++) {
-        uint64_t s = b + (uint64_t)lane;
-        uint32_t d = s < s1 ? state_diff(pv, f, m, s) : 0u;
+    constexpr uint64_t kStep = 32 * PER_LANE;
+    for (uint64_t b = s0; b < s1; b += kStep, iter++) {   // lane: states b + lane (+ 32)
+        const uint64_t sa = b + (uint64_t)lane;
+        uint32_t d = 0;
+        if (PER_LANE == 2) {
+            const uint64_t sb = sa + 32;   // past the end: evaluate a state in range again
+            d = sa < s1 ? state_diff2(pv, f, m, sa, sb < s1 ? sb : sa) : 0u;
+        } else {
+            d = sa < s1 ? state_diff(pv, f, m, sa) : 0u;
+        }
         if (__any_sync(kFull, d != 0)) {
-            if (lane == 0) *nstates += (b - s0) + 32;
+            if (lane == 0) *nstates += min((b - s0) + kStep, s1 - s0);
             return false;
         }
-        if ((iter & 255) == 255 && stop) {
+        if ((iter & (255 / PER_LANE)) == (255 / PER_LANE) && stop) {
             uint32_t sv = lane == 0 ? *stop : 0u;   // one read, broadcast: keeps the warp uniform
             if (__shfl_sync(kFull, sv, 0)) break;
         }
@@ -1097,7 +1135,7 @@ __global__ void __launch_bounds__(256, 4) k_exhaustive(Src src, const unsigned l
             Fields f = make_fields(cone, fl.swept, rep);
             const uint64_t total = 1ull << bits;
             const uint64_t end = total <= kSmallSweep ? total : kProbe;
-            ok = sweep_states(pv, f, mask, 0, end, nullptr, &nstates, lane);
+            ok = sweep_states<1>(pv, f, mask, 0, end, nullptr, &nstates, lane);
             if (ok && end < total) big |= 1u << o;
         }
         if (ok && big) {
@@ -1154,7 +1192,7 @@ __global__ void __launch_bounds__(256) k_exh_items(Src src, ExhArgs a) {
         __syncwarp();
         Flow fl = dataflow_s(pv, lane, s_dep);
         Fields f = make_fields(it.cone, fl.swept, it.rep != 0);
-        bool ok = sweep_states(pv, f, it.outmask, it.start, it.start + it.count, flag, &nstates, lane);
+        bool ok = sweep_states<2>(pv, f, it.outmask, it.start, it.start + it.count, flag, &nstates, lane);
         if (!ok && lane == 0) *flag = 1u;
         __syncwarp();
     }
@@ -1491,7 +1529,7 @@ __global__ void __launch_bounds__(256) k_exhaustive_static(StaticCsrSource src, 
         bool ok = true;
         for (int i = 0; i < g.n && ok; i++) {
             Fields f = make_fields(g.cone[i], fl.swept, rep);
-            ok = sweep_states(pv, f, g.mask[i], 0, 1ull << g.bits[i], nullptr, &nstates, lane);
+            ok = sweep_states<1>(pv, f, g.mask[i], 0, 1ull << g.bits[i], nullptr, &nstates, lane);
         }
         if (lane == 0) scr->fail[p] = ok ? 0u : 1u;
         __syncwarp();

@@ -92,70 +92,91 @@ M6502_HD uint32_t pull(St& s) {
     return v;
 }
 
-// One instruction; insn = op | imm << 8.  Semantics of pkg/cpu/exec.go:8-189
-// (binary-mode ADC/SBC, PHP pushes B and U, pulls zero S1).  An opcode
-// outside [0, 58) leaves the state unchanged; callers validate inputs.
+// The opcode table as an X-macro: X(opcode, statements on the state `s`;
+// `imm` is the operand).  Semantics of pkg/cpu/exec.go:8-189 (binary-mode
+// ADC/SBC, PHP pushes B and U, pulls zero S1).
+#define M6502_OPCODES(X) \
+    X(TAX, s.x = s.a; set_nz(s, s.x)) \
+    X(TAY, s.y = s.a; set_nz(s, s.y)) \
+    X(TXA, s.a = s.x; set_nz(s, s.a)) \
+    X(TYA, s.a = s.y; set_nz(s, s.a)) \
+    X(TSX, s.x = s.s; set_nz(s, s.x)) \
+    X(TXS, s.s = s.x) \
+    X(INX, s.x = (s.x + 1u) & 0xFFu; set_nz(s, s.x)) \
+    X(INY, s.y = (s.y + 1u) & 0xFFu; set_nz(s, s.y)) \
+    X(DEX, s.x = (s.x - 1u) & 0xFFu; set_nz(s, s.x)) \
+    X(DEY, s.y = (s.y - 1u) & 0xFFu; set_nz(s, s.y)) \
+    X(ASL_A, s.a = op_asl(s, s.a)) \
+    X(LSR_A, s.a = op_lsr(s, s.a)) \
+    X(ROL_A, s.a = op_rol(s, s.a)) \
+    X(ROR_A, s.a = op_ror(s, s.a)) \
+    X(CLC, s.p &= ~kFlagC) \
+    X(SEC, s.p |= kFlagC) \
+    X(CLD, s.p &= ~kFlagD) \
+    X(SED, s.p |= kFlagD) \
+    X(CLI, s.p &= ~kFlagI) \
+    X(SEI, s.p |= kFlagI) \
+    X(CLV, s.p &= ~kFlagV) \
+    X(PHA, push(s, s.a)) \
+    X(PLA, s.a = pull(s); set_nz(s, s.a)) \
+    X(PHP, push(s, s.p | kFlagB | kFlagU)) \
+    X(PLP, s.p = pull(s)) \
+    X(NOP, (void)s) \
+    X(LDA_IMM, s.a = imm; set_nz(s, imm)) \
+    X(LDX_IMM, s.x = imm; set_nz(s, imm)) \
+    X(LDY_IMM, s.y = imm; set_nz(s, imm)) \
+    X(ADC_IMM, op_adc(s, imm)) \
+    X(SBC_IMM, op_sbc(s, imm)) \
+    X(AND_IMM, s.a &= imm; set_nz(s, s.a)) \
+    X(ORA_IMM, s.a |= imm; set_nz(s, s.a)) \
+    X(EOR_IMM, s.a ^= imm; set_nz(s, s.a)) \
+    X(CMP_IMM, op_cmp(s, s.a, imm)) \
+    X(CPX_IMM, op_cmp(s, s.x, imm)) \
+    X(CPY_IMM, op_cmp(s, s.y, imm)) \
+    X(LDA_M, s.a = s.m; set_nz(s, s.a)) \
+    X(LDX_M, s.x = s.m; set_nz(s, s.x)) \
+    X(LDY_M, s.y = s.m; set_nz(s, s.y)) \
+    X(STA_M, s.m = s.a) \
+    X(STX_M, s.m = s.x) \
+    X(STY_M, s.m = s.y) \
+    X(ADC_M, op_adc(s, s.m)) \
+    X(SBC_M, op_sbc(s, s.m)) \
+    X(AND_M, s.a &= s.m; set_nz(s, s.a)) \
+    X(ORA_M, s.a |= s.m; set_nz(s, s.a)) \
+    X(EOR_M, s.a ^= s.m; set_nz(s, s.a)) \
+    X(CMP_M, op_cmp(s, s.a, s.m)) \
+    X(CPX_M, op_cmp(s, s.x, s.m)) \
+    X(CPY_M, op_cmp(s, s.y, s.m)) \
+    X(INC_M, s.m = (s.m + 1u) & 0xFFu; set_nz(s, s.m)) \
+    X(DEC_M, s.m = (s.m - 1u) & 0xFFu; set_nz(s, s.m)) \
+    X(ASL_M, s.m = op_asl(s, s.m)) \
+    X(LSR_M, s.m = op_lsr(s, s.m)) \
+    X(ROL_M, s.m = op_rol(s, s.m)) \
+    X(ROR_M, s.m = op_ror(s, s.m)) \
+    X(BIT_M, s.p = (s.p & 0x3Du) | (s.m & 0xC0u) | ((s.a & s.m) == 0u ? kFlagZ : 0u))
+
+// One instruction; insn = op | imm << 8.  An opcode outside [0, 58) leaves
+// the state unchanged; callers validate inputs.
 M6502_HD void exec(St& s, uint32_t insn) {
     const uint32_t imm = insn >> 8;
+    (void)imm;
     switch (insn & 0xFFu) {
-    case TAX: s.x = s.a; set_nz(s, s.x); break;
-    case TAY: s.y = s.a; set_nz(s, s.y); break;
-    case TXA: s.a = s.x; set_nz(s, s.a); break;
-    case TYA: s.a = s.y; set_nz(s, s.a); break;
-    case TSX: s.x = s.s; set_nz(s, s.x); break;
-    case TXS: s.s = s.x; break;
-    case INX: s.x = (s.x + 1u) & 0xFFu; set_nz(s, s.x); break;
-    case INY: s.y = (s.y + 1u) & 0xFFu; set_nz(s, s.y); break;
-    case DEX: s.x = (s.x - 1u) & 0xFFu; set_nz(s, s.x); break;
-    case DEY: s.y = (s.y - 1u) & 0xFFu; set_nz(s, s.y); break;
-    case ASL_A: s.a = op_asl(s, s.a); break;
-    case LSR_A: s.a = op_lsr(s, s.a); break;
-    case ROL_A: s.a = op_rol(s, s.a); break;
-    case ROR_A: s.a = op_ror(s, s.a); break;
-    case CLC: s.p &= ~kFlagC; break;
-    case SEC: s.p |= kFlagC; break;
-    case CLD: s.p &= ~kFlagD; break;
-    case SED: s.p |= kFlagD; break;
-    case CLI: s.p &= ~kFlagI; break;
-    case SEI: s.p |= kFlagI; break;
-    case CLV: s.p &= ~kFlagV; break;
-    case PHA: push(s, s.a); break;
-    case PLA: s.a = pull(s); set_nz(s, s.a); break;
-    case PHP: push(s, s.p | kFlagB | kFlagU); break;
-    case PLP: s.p = pull(s); break;
-    case NOP: break;
-    case LDA_IMM: s.a = imm; set_nz(s, imm); break;
-    case LDX_IMM: s.x = imm; set_nz(s, imm); break;
-    case LDY_IMM: s.y = imm; set_nz(s, imm); break;
-    case ADC_IMM: op_adc(s, imm); break;
-    case SBC_IMM: op_sbc(s, imm); break;
-    case AND_IMM: s.a &= imm; set_nz(s, s.a); break;
-    case ORA_IMM: s.a |= imm; set_nz(s, s.a); break;
-    case EOR_IMM: s.a ^= imm; set_nz(s, s.a); break;
-    case CMP_IMM: op_cmp(s, s.a, imm); break;
-    case CPX_IMM: op_cmp(s, s.x, imm); break;
-    case CPY_IMM: op_cmp(s, s.y, imm); break;
-    case LDA_M: s.a = s.m; set_nz(s, s.a); break;
-    case LDX_M: s.x = s.m; set_nz(s, s.x); break;
-    case LDY_M: s.y = s.m; set_nz(s, s.y); break;
-    case STA_M: s.m = s.a; break;
-    case STX_M: s.m = s.x; break;
-    case STY_M: s.m = s.y; break;
-    case ADC_M: op_adc(s, s.m); break;
-    case SBC_M: op_sbc(s, s.m); break;
-    case AND_M: s.a &= s.m; set_nz(s, s.a); break;
-    case ORA_M: s.a |= s.m; set_nz(s, s.a); break;
-    case EOR_M: s.a ^= s.m; set_nz(s, s.a); break;
-    case CMP_M: op_cmp(s, s.a, s.m); break;
-    case CPX_M: op_cmp(s, s.x, s.m); break;
-    case CPY_M: op_cmp(s, s.y, s.m); break;
-    case INC_M: s.m = (s.m + 1u) & 0xFFu; set_nz(s, s.m); break;
-    case DEC_M: s.m = (s.m - 1u) & 0xFFu; set_nz(s, s.m); break;
-    case ASL_M: s.m = op_asl(s, s.m); break;
-    case LSR_M: s.m = op_lsr(s, s.m); break;
-    case ROL_M: s.m = op_rol(s, s.m); break;
-    case ROR_M: s.m = op_ror(s, s.m); break;
-    case BIT_M: s.p = (s.p & 0x3Du) | (s.m & 0xC0u) | ((s.a & s.m) == 0u ? kFlagZ : 0u); break;
+#define M6502_CASE1(op, ...) case op: { __VA_ARGS__; } break;
+        M6502_OPCODES(M6502_CASE1)
+#undef M6502_CASE1
+    default: break;
+    }
+}
+
+// The same instruction on two states with one dispatch (the sweeps run two
+// states per lane so the opcode switch is paid once per pair of states).
+M6502_HD void exec2(St& s0, St& s1, uint32_t insn) {
+    const uint32_t imm = insn >> 8;
+    (void)imm;
+    switch (insn & 0xFFu) {
+#define M6502_CASE2(op, ...) case op: { { St& s = s0; __VA_ARGS__; } { St& s = s1; __VA_ARGS__; } } break;
+        M6502_OPCODES(M6502_CASE2)
+#undef M6502_CASE2
     default: break;
     }
 }

@@ -11,6 +11,7 @@ The metric is pair-checks/s of the whole job.
   python bench.py --workload len3            # 4,096 length-3 targets x length-1+2 candidates x 4 masks
   python bench.py --workload stoke           # STOKE time-to-proof, uniform proposal
   python bench.py --workload stoke-learned   # the same with the trained 50/50 mixed proposal
+  python bench.py --workload gemm            # the proposal's tcgen05 bf16 GEMM, TFLOP/s
 
 With N > 1 (torchrun) the target list is split strided across ranks (no
 collective on the data path; the fixed job is shared, "scaling": "strong").
@@ -416,6 +417,56 @@ def run_stoke(args):
     eng.close()
 
 
+def run_gemm(args):
+    """The learned proposal's dense-layer kernel (tcgen05 bf16 GEMM, fp32
+    accumulate in TMEM) on a square problem, against the measured cuBLAS bf16
+    peak of this pool (MEASURED_PEAKS.json, burst figure)."""
+    import torch
+    import m6502
+    from m6502.mlp import gemm_bf16
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    n = args.gemm_n
+    eng = m6502.Engine(device=local)
+    stream = torch.cuda.ExternalStream(eng.stream, device=local)
+    g = torch.Generator(device=f"cuda:{local}").manual_seed(0)
+    a = torch.randn(n, n, device=f"cuda:{local}", generator=g).to(torch.bfloat16)
+    b = torch.randn(n, n, device=f"cuda:{local}", generator=g).to(torch.bfloat16)
+    for _ in range(max(args.warmup, 3)):
+        c = gemm_bf16(eng, a, b)
+    torch.cuda.synchronize()
+    ref = a[:256].float() @ b.float().T
+    err = float((c[:256] - ref).abs().max() / ref.abs().max())
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        gemm_bf16(eng, a, b)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    tflops = 2.0 * n ** 3 / (ms / 1e3) / 1e12
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    peak = peaks.get("bf16_tflops", 1590.0)
+    line = {"metric": "bf16 GEMM TFLOP/s (tcgen05, 128x128 tiles)", "value": tflops, "unit": "TFLOP/s",
+            "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
+            "ms_per_step": ms, "dtype": "bf16", "data": "synthetic (seeded normal)",
+            "config": {"workload": f"gemm-{n}", "M": n, "N": n, "K": n},
+            "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
+                         "frac": tflops / peak, "peak_source": "measured" if peaks else "fallback"},
+            "max_rel_err_vs_fp32": err,
+            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}}
+    print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def go_checked_pairs(targets, rules, dead, nc2=True):
     """Pairs the Go worker enumerates before it stops (worker.go:122-176:
     every candidate of each length it tries up to and including the first
@@ -540,7 +591,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1500, help="targets in the CPU baseline sample")
     ap.add_argument("--ref-sample", type=int, default=600, help="targets per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["len2", "len3", "stoke", "stoke-learned"], default="len2")
+    ap.add_argument("--workload", choices=["len2", "len3", "stoke", "stoke-learned", "gemm"], default="len2")
+    ap.add_argument("--gemm-n", type=int, default=8192, help="GEMM workload: M = N = K")
     ap.add_argument("--first-op", type=int, default=0,
                     help="length-2 workload: first instructions [first-op, last-op) of the CUDA-order table "
                          "(a subset, for small profiler captures)")
@@ -554,6 +606,8 @@ def main():
         run_stoke(args)
     elif args.workload == "len3":
         run_len3(args)
+    elif args.workload == "gemm":
+        run_gemm(args)
     elif args.impl == "reference":
         run_reference(args)
     else:
