@@ -326,9 +326,10 @@ const int kLayerW[4] = {T_W1, T_W2, T_W3, T_W4};
 int gemm(m6502_mlp* mlp, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, int M, int N, int K,
          tcg::Epilogue epi) {
     if (K % tcg::kBK != 0 || lda % 8 || ldb % 8) { mlp->err = "gemm shape"; return M6502_E_INVAL; }
-    dim3 grid((N + tcg::kBN - 1) / tcg::kBN, (M + tcg::kBM - 1) / tcg::kBM);
-    tcg::k_gemm<<<grid, tcg::kThreads, tcg::kSmemBytes, mlp->stream>>>(A, lda, B, ldb, M, N, K, epi, mlp->d_err);
-    MLP_CK(cudaGetLastError());
+    if (!tcg::launch_gemm(A, lda, B, ldb, M, N, K, epi, mlp->d_err, mlp->stream)) {
+        mlp->err = "tensor-core GEMM launch failed (tensor map or launch)";
+        return M6502_E_CUDA;
+    }
     return M6502_OK;
 }
 
@@ -622,10 +623,8 @@ int m6502_gemm_bf16(m6502_ctx* ctx, int M, int N, int K, const void* A, const vo
     if (cudaMemsetAsync(d_err, 0, sizeof(int), st) != cudaSuccess) return M6502_E_CUDA;
     tcg::Epilogue e;
     e.mode = tcg::EPI_F32; e.out_f32 = C; e.out_bf16 = nullptr; e.bias = nullptr; e.act = nullptr; e.ldc = N;
-    dim3 grid((N + tcg::kBN - 1) / tcg::kBN, (M + tcg::kBM - 1) / tcg::kBM);
-    tcg::k_gemm<<<grid, tcg::kThreads, tcg::kSmemBytes, st>>>((const __nv_bfloat16*)A, K, (const __nv_bfloat16*)B, K,
-                                                               M, N, K, e, d_err);
-    if (cudaGetLastError() != cudaSuccess) return M6502_E_CUDA;
+    if (!tcg::launch_gemm((const __nv_bfloat16*)A, K, (const __nv_bfloat16*)B, K, M, N, K, e, d_err, st))
+        return M6502_E_CUDA;
     int h = 0;
     if (cudaMemcpyAsync(&h, d_err, sizeof h, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)

@@ -1,29 +1,43 @@
-// tc_gemm.cuh -- bf16 GEMM on the 5th-generation tensor cores (tcgen05).
+// tc_gemm.cuh -- bf16 GEMM on the 5th-generation tensor cores (tcgen05),
+// operands brought in by the Tensor Memory Accelerator.
 //
 //   C[M x N] (fp32 accumulate) = A[M x K] . B[N x K]^T,  A and B bf16, K-major
 //
-// One CTA of 128 threads computes a 128 x 128 tile.  Per 64-wide K block the
-// CTA stages A and B into shared memory in the canonical K-major
-// 128-byte-swizzled layout (8-row atoms of 1,024 bytes; the 16-byte chunk
-// index of row r is XORed with r % 8), one elected thread issues four
-// tcgen05.mma (M = 128, N = 128, K = 16 each) with the accumulator in tensor
-// memory, and tcgen05.commit signals an mbarrier when the tensor core has
-// finished reading the stage.  Two stages: the loads of block k+1 overlap
-// the MMAs of block k.  The epilogue reads the accumulator with
-// tcgen05.ld (warp w owns TMEM lanes 32w..32w+31 = tile rows) and applies a
-// fused bias / ReLU / ReLU-gradient / conversion.  Every mbarrier wait is
-// bounded; on expiry the kernel records an error and skips the epilogue.
+// One CTA of 128 threads computes a 128 x 256 tile; the fp32 accumulator
+// (256 columns) lives in tensor memory.  The K loop runs through a ring of
+// kStages shared-memory stages (A 16 KB + B 32 KB each):
+//   - lane 0 of warp 0 (producer) waits until a stage is free (its `empty`
+//     mbarrier), arms its `full` mbarrier with the stage's byte count and
+//     issues two TMA tile loads (cp.async.bulk.tensor, 128-byte swizzle)
+//     that complete on it;
+//   - lane 0 of warp 1 (MMA issuer) waits for `full`, issues four
+//     tcgen05.mma (M = 128, N = 256, K = 16) on the swizzled stage, and
+//     tcgen05.commit arrives on the stage's `empty` barrier once the tensor
+//     core has read it;
+//   - after the last K block a commit on `done` releases the epilogue: all
+//     four warps read the accumulator with tcgen05.ld (warp w owns TMEM
+//     lanes 32w..32w+31 = tile rows) and apply the fused bias / ReLU /
+//     ReLU-gradient / conversion.
+// Rows and columns past M, N are zero-filled by the TMA and not stored.
+// Every mbarrier wait is bounded; on expiry the kernel records an error,
+// stops issuing, waits a bounded time for work in flight, frees TMEM and
+// returns.  No cluster multicast is used.
 #pragma once
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_runtime.h>
 #include <cstdint>
 
 namespace tcg {
 
-constexpr int kBM = 128, kBN = 128, kBK = 64;
+constexpr int kBM = 128, kBN = 256, kBK = 64;
+constexpr int kStages = 4;
 constexpr int kThreads = 128;
-constexpr int kStageBytes = (kBM + kBN) * kBK * 2;       // 32 KB per stage (A + B)
-constexpr int kSmemBytes = 2 * kStageBytes + 1024;       // + slack to align to 1,024 bytes
-constexpr uint32_t kWaitLimit = 1u << 26;                // bounded mbarrier polling
+constexpr int kStageA = kBM * kBK * 2;                  // 16 KB
+constexpr int kStageB = kBN * kBK * 2;                  // 32 KB
+constexpr int kStageBytes = kStageA + kStageB;          // 48 KB
+constexpr int kSmemBytes = kStages * kStageBytes + 1024;   // + slack to align to 1,024 bytes
+constexpr uint32_t kWaitLimit = 1u << 26;               // bounded mbarrier polling
 
 // Epilogue modes.
 enum : int {
@@ -65,9 +79,9 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 }
 
 // Waits for the phase with the given parity to complete; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kWaitLimit) {
     const uint32_t a = smem_u32(bar);
-    for (uint32_t i = 0; i < kWaitLimit; i++) {
+    for (uint32_t i = 0; i < limit; i++) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -81,65 +95,76 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     return false;
 }
 
-// Copies rows [r0, r0 + rows) x K block [k0, k0 + 64) of a K-major bf16
-// matrix into a swizzled tile; rows at or past `rows_valid` are zero-filled.
-__device__ __forceinline__ void stage_tile(uint8_t* tile, const __nv_bfloat16* g, int ld, int r0, int rows,
-                                           int rows_valid, int k0) {
-    for (int i = threadIdx.x; i < rows * 8; i += kThreads) {
-        const int r = i >> 3, j = i & 7;
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (r0 + r < rows_valid) v = *reinterpret_cast<const uint4*>(g + (size_t)(r0 + r) * ld + k0 + j * 8);
-        *reinterpret_cast<uint4*>(tile + r * 128 + ((j ^ (r & 7)) << 4)) = v;
-    }
+// Arms a barrier for `bytes` of asynchronous copies (this thread's arrival
+// included).
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
 }
 
-__global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restrict__ A, int lda,
-                                                    const __nv_bfloat16* __restrict__ B, int ldb, int M, int N,
-                                                    int K, Epilogue epi, int* __restrict__ err) {
+// 2-D TMA tile load (no multicast): box at element coordinates (x = K, y = row).
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(dst)), "l"((uint64_t)map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+__global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUtensorMap tmA,
+                                                    const __grid_constant__ CUtensorMap tmB, int M, int N, int K,
+                                                    Epilogue epi, int* __restrict__ err) {
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t bars[2];
+    __shared__ uint64_t full[kStages], empty[kStages], done;
     __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
+    const int nk = K / kBK;
 
-    if (warp == 0) {   // 128 TMEM columns: one fp32 accumulator column per N
+    if (warp == 0) {   // 256 TMEM columns: one fp32 accumulator column per N
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                      "r"(kBN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        for (int s = 0; s < kStages; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(&done, 1);
+        s_fail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmA) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmB) : "memory");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = s_tmem;
-    const uint32_t idesc = idesc_bf16(kBM, kBN);
-    const int nk = K / kBK;
-    uint32_t phase[2] = {0, 0};
-    bool ok = true;
 
-    for (int kb = 0; kb < nk; kb++) {
-        const int s = kb & 1;
-        uint8_t* sa = smem + s * kStageBytes;
-        uint8_t* sb = sa + kBM * kBK * 2;
-        if (kb >= 2) {   // the MMAs of block kb-2 read this stage: wait for their commit
-            ok = mbar_wait(&bars[s], phase[s]);
-            phase[s] ^= 1;
-            ok = __syncthreads_and(ok ? 1 : 0) != 0;   // uniform decision
-            if (!ok) break;
+    if (warp == 0 && lane == 0) {
+        // producer: stage s of round r is free once the MMAs of round r-1 committed on empty[s]
+        for (int kb = 0; kb < nk; kb++) {
+            const int s = kb % kStages, r = kb / kStages;
+            if (r > 0 && !mbar_wait(&empty[s], (uint32_t)((r - 1) & 1))) { atomicExch(&s_fail, 1); break; }
+            if (*(volatile int*)&s_fail) break;
+            uint8_t* sa = smem + s * kStageBytes;
+            mbar_expect_tx(&full[s], (uint32_t)kStageBytes);
+            tma_load_2d(sa, &tmA, kb * kBK, m0, &full[s]);
+            tma_load_2d(sa + kStageA, &tmB, kb * kBK, n0, &full[s]);
         }
-        stage_tile(sa, A, lda, m0, kBM, M, kb * kBK);
-        stage_tile(sb, B, ldb, n0, kBN, N, kb * kBK);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic-proxy writes -> tensor core
-        asm volatile("tcgen05.fence::before_thread_sync;");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        if (threadIdx.x == 0) {
-            const uint32_t a0 = smem_u32(sa), b0 = smem_u32(sb);
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        const uint32_t idesc = idesc_bf16(kBM, kBN);
+        for (int kb = 0; kb < nk; kb++) {
+            const int s = kb % kStages, r = kb / kStages;
+            if (!mbar_wait(&full[s], (uint32_t)(r & 1)) || *(volatile int*)&s_fail) {
+                atomicExch(&s_fail, 1);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t a0 = smem_u32(smem + s * kStageBytes), b0 = a0 + kStageA;
 #pragma unroll
             for (int kk = 0; kk < kBK / 16; kk++) {   // K = 16 per MMA: +32 bytes along the swizzled row
                 const uint64_t da = sw128_desc(a0 + kk * 32), db = sw128_desc(b0 + kk * 32);
@@ -151,27 +176,25 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
                     ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc));
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                         ::"r"(smem_u32(&bars[s])) : "memory");
+                         ::"r"(smem_u32(&empty[s])) : "memory");
         }
-        __syncwarp();
+        // done fires when every MMA issued so far has completed
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     ::"r"(smem_u32(&done)) : "memory");
     }
-    // Each stage used has exactly one commit not yet waited for.
-    if (ok) {
-        for (int s = 0; s < 2; s++)
-            if (nk > s) { ok = ok && mbar_wait(&bars[s], phase[s]); phase[s] ^= 1; }
-    } else {
-        // Timed out: give the tensor core a last bounded chance to finish before TMEM is freed.
-        for (int s = 0; s < 2; s++) if (nk > s) mbar_wait(&bars[s], phase[s]);
-    }
-    const bool all_ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    __syncwarp();
+    // Everyone waits for the accumulator (bounded).
+    bool ok = mbar_wait(&done, 0);
+    ok = __syncthreads_and((ok && !s_fail) ? 1 : 0) != 0;
     asm volatile("tcgen05.fence::after_thread_sync;");
-    if (!all_ok) {
+    if (!ok) {
         if (threadIdx.x == 0) atomicExch(err, 1);
     } else {
         // Epilogue: row = m0 + 32 * warp + lane; 16 columns per tcgen05.ld.
         const int row = m0 + 32 * warp + lane;
 #pragma unroll 1
         for (int c0 = 0; c0 < kBN; c0 += 16) {
+            if (n0 + c0 >= N) break;   // warp-uniform
             uint32_t v[16];
             const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0;
             asm volatile(
@@ -204,6 +227,52 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __nv_bfloat16* __restri
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kBN));
+}
+
+// ---- host side ----
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                    const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// The driver's tensor-map encoder, found through the runtime (no libcuda link).
+inline EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// Tensor map of a K-major bf16 matrix [rows x K] with leading dimension ld
+// (elements), box kBK x box_rows, 128-byte swizzle, zero fill out of bounds.
+inline bool make_map(CUtensorMap* map, const void* base, int rows, int K, int ld, int box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn || ((uintptr_t)base & 15u) || (ld * 2) % 16) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// C = A . B^T with the fused epilogue, on `stream`.  K must be a multiple of
+// kBK; lda and ldb multiples of 8; A and B 16-byte aligned.  Returns false if
+// the shapes or the tensor maps are not usable (nothing is launched).
+inline bool launch_gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, int M, int N, int K,
+                        const Epilogue& epi, int* err, cudaStream_t stream) {
+    if (M <= 0 || N <= 0 || K <= 0 || K % kBK) return false;
+    CUtensorMap ma, mb;
+    if (!make_map(&ma, A, M, K, lda, kBM) || !make_map(&mb, B, N, K, ldb, kBN)) return false;
+    dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
+    k_gemm<<<grid, kThreads, kSmemBytes, stream>>>(ma, mb, M, N, K, epi, err);
+    return cudaGetLastError() == cudaSuccess;
 }
 
 }  // namespace tcg

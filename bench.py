@@ -455,7 +455,7 @@ def run_gemm(args):
     except OSError:
         pass
     peak = peaks.get("bf16_tflops", 1590.0)
-    line = {"metric": "bf16 GEMM TFLOP/s (tcgen05, 128x128 tiles)", "value": tflops, "unit": "TFLOP/s",
+    line = {"metric": "bf16 GEMM TFLOP/s (tcgen05, TMA, 128x256 tiles)", "value": tflops, "unit": "TFLOP/s",
             "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
             "ms_per_step": ms, "dtype": "bf16", "data": "synthetic (seeded normal)",
             "config": {"workload": f"gemm-{n}", "M": n, "N": n, "K": n},
