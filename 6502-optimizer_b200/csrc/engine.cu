@@ -268,6 +268,8 @@ struct Fields {
     uint32_t sh[8], mk[8], base[8];   // order: A, X, Y, S, M, S0, S1, carry
     uint32_t rep_mask;                // fields translated through c_rep
     uint32_t bits;
+    int low;                          // the field at bit 0 if it is at least 2 bits wide, else -1
+    uint32_t low_mk;                  // its mask (its values are state & low_mk)
 };
 
 __device__ __forceinline__ Fields make_fields(uint32_t cone, uint32_t swept, bool rep) {
@@ -275,6 +277,8 @@ __device__ __forceinline__ Fields make_fields(uint32_t cone, uint32_t swept, boo
     uint32_t bit = 0;
     const uint32_t locs[8] = {L_A, L_X, L_Y, L_S, L_M, L_S0, L_S1, L_C};
     f.rep_mask = 0;
+    f.low = -1;
+    f.low_mk = 0;
 #pragma unroll
     for (int i = 0; i < 8; i++) {
         uint32_t l = locs[i];
@@ -282,6 +286,7 @@ __device__ __forceinline__ Fields make_fields(uint32_t cone, uint32_t swept, boo
         f.base[i] = (l == L_S && !(swept & LB(L_S))) ? 0xFDu : 0u;
         if (cone & LB(l)) {
             uint32_t w = (l == L_C) ? 1u : ((rep && l != L_A) ? 5u : 8u);
+            if (bit == 0) { f.low = w >= 2 ? i : -1; f.low_mk = (1u << w) - 1u; }
             f.sh[i] = bit; f.mk[i] = (1u << w) - 1u; f.base[i] = 0;
             if (rep && l != L_A && l != L_C) f.rep_mask |= 1u << i;
             bit += w;
@@ -376,20 +381,66 @@ __device__ __forceinline__ bool probe_domain(const PairView& pv, uint32_t swept,
 // on the compared outputs in every state.  Warp-collective.  When `stop`
 // becomes nonzero (another item of the same pair failed) the sweep ends
 // early; its result is then irrelevant.
-// PER_LANE = 2: two states per lane and opcode dispatch (the work items'
-// long sweeps); 1: one (the in-warp sweeps of small cones, where the extra
-// registers cost more than the shared dispatch saves).
+// Four consecutive states s..s+3 (s a multiple of 4) packed one per byte
+// (see exec_x4).  They differ only in the low two bits of the lowest field,
+// so one scalar decode plus that field's four values builds them.
+__device__ __forceinline__ St decode_x4(const Fields& f, uint64_t s) {
+    const St in = decode_state(f, s);
+    St o;
+    o.a = in.a * kB1; o.x = in.x * kB1; o.y = in.y * kB1; o.s = in.s * kB1;
+    o.m = in.m * kB1; o.s0 = in.s0 * kB1; o.s1 = in.s1 * kB1; o.p = in.p * kB1;
+    uint32_t low;
+    const uint32_t i0 = (uint32_t)s & f.low_mk;   // the lowest field starts at bit 0 and has base 0
+    if (f.rep_mask & (1u << f.low))
+        low = c_rep[i0] | (c_rep[i0 + 1] << 8) | (c_rep[i0 + 2] << 16) | (c_rep[i0 + 3] << 24);
+    else
+        low = i0 * kB1 + 0x03020100u;
+    switch (f.low) {   // warp-uniform
+    case 0: o.a = low; break;
+    case 1: o.x = low; break;
+    case 2: o.y = low; break;
+    case 3: o.s = low; break;
+    case 4: o.m = low; break;
+    case 5: o.s0 = low; break;
+    default: o.s1 = low; break;
+    }
+    return o;
+}
+
+__device__ __forceinline__ uint32_t state_diff_x4(const PairView& pv, const Fields& f, const OutMask& m4, uint64_t s) {
+    St c = decode_x4(f, s), t = c;
+    const int n = pv.tn + pv.cn;
+    for (int i = 0; i < n; i++) {
+        if (i == pv.tn) { t = c; c = decode_x4(f, s); }
+        exec_x4(c, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
+    }
+    if (pv.cn == 0) { t = c; c = decode_x4(f, s); }
+    return out_diff(t, c, m4);
+}
+
+// PER_LANE = 4: four consecutive states per lane packed one per byte
+// (exec_x4: one dispatch, byte-parallel arithmetic); 2: two states per lane
+// and dispatch; 1: one.  The packed path needs 4-aligned ranges and a
+// lowest field of at least 2 bits, and falls back to one state per lane.
 template <int PER_LANE>
 __device__ __forceinline__ bool sweep_states(const PairView& pv, const Fields& f, uint64_t om, uint64_t s0,
                                              uint64_t s1, const volatile uint32_t* stop, unsigned long long* nstates,
                                              int lane) {
-    const OutMask m = out_mask(om);
+    if (PER_LANE == 4 && (f.low < 0 || (s0 & 3) || (s1 & 3)))   // packed sweep needs 4-aligned runs
+        return sweep_states<1>(pv, f, om, s0, s1, stop, nstates, lane);
+    OutMask m = out_mask(om);
+    if (PER_LANE == 4) {
+        m.a *= kB1; m.x *= kB1; m.y *= kB1; m.p *= kB1; m.s *= kB1; m.m *= kB1; m.s0 *= kB1; m.s1 *= kB1;
+    }
     uint64_t iter = 0;
     constexpr uint64_t kStep = 32 * PER_LANE;
     for (uint64_t b = s0; b < s1; b += kStep, iter++) {   // lane: states b + lane (+ 32)
         const uint64_t sa = b + (uint64_t)lane;
         uint32_t d = 0;
-        if (PER_LANE == 2) {
+        if (PER_LANE == 4) {
+            const uint64_t s4 = b + 4 * (uint64_t)lane;
+            d = s4 < s1 ? state_diff_x4(pv, f, m, s4) : 0u;
+        } else if (PER_LANE == 2) {
             const uint64_t sb = sa + 32;   // past the end: evaluate a state in range again
             d = sa < s1 ? state_diff2(pv, f, m, sa, sb < s1 ? sb : sa) : 0u;
         } else {
@@ -1135,7 +1186,7 @@ __global__ void __launch_bounds__(256, 4) k_exhaustive(Src src, const unsigned l
             Fields f = make_fields(cone, fl.swept, rep);
             const uint64_t total = 1ull << bits;
             const uint64_t end = total <= kSmallSweep ? total : kProbe;
-            ok = sweep_states<1>(pv, f, mask, 0, end, nullptr, &nstates, lane);
+            ok = sweep_states<4>(pv, f, mask, 0, end, nullptr, &nstates, lane);
             if (ok && end < total) big |= 1u << o;
         }
         if (ok && big) {
@@ -1192,7 +1243,7 @@ __global__ void __launch_bounds__(256) k_exh_items(Src src, ExhArgs a) {
         __syncwarp();
         Flow fl = dataflow_s(pv, lane, s_dep);
         Fields f = make_fields(it.cone, fl.swept, it.rep != 0);
-        bool ok = sweep_states<2>(pv, f, it.outmask, it.start, it.start + it.count, flag, &nstates, lane);
+        bool ok = sweep_states<4>(pv, f, it.outmask, it.start, it.start + it.count, flag, &nstates, lane);
         if (!ok && lane == 0) *flag = 1u;
         __syncwarp();
     }

@@ -181,6 +181,146 @@ M6502_HD void exec2(St& s0, St& s1, uint32_t insn) {
     }
 }
 
+// ---- Four states per register (SWAR) ----
+//
+// The same St holds four machine states: byte k of every field is state k.
+// All arithmetic stays inside its byte: additions are done on the low 7 bits
+// with bit 7 restored by XOR, and carries, zero tests and shifts are masked
+// per byte.  exec_x4 applies one instruction to the four states with a
+// single opcode dispatch; its results equal four scalar exec calls
+// (tests/test_abi_host.py checks every instruction).
+constexpr uint32_t kB1 = 0x01010101u, kH = 0x80808080u, kL7 = 0x7F7F7F7Fu;
+
+M6502_HD uint32_t x4_zero(uint32_t v) { return ~(((v & kL7) + kL7) | v) & kH; }   // 0x80 in zero bytes
+M6502_HD uint32_t x4_nzf(uint32_t v) { return (v & kH) | (x4_zero(v) >> 6); }
+M6502_HD void x4_set_nz(St& s, uint32_t v) { s.p = (s.p & (0x7Du * kB1)) | x4_nzf(v); }
+// a + b + c per byte (c is 0 or 1 per byte); cout: the carry out of each byte (0 or 1).
+M6502_HD uint32_t x4_add(uint32_t a, uint32_t b, uint32_t c, uint32_t& cout) {
+    const uint32_t r = ((a & kL7) + (b & kL7) + c) ^ ((a ^ b) & kH);
+    cout = (((a & b) | ((a | b) & ~r)) >> 7) & kB1;
+    return r;
+}
+M6502_HD uint32_t x4_inc(uint32_t v) { return ((v & kL7) + kB1) ^ (v & kH); }
+M6502_HD uint32_t x4_dec(uint32_t v) { return ((v & kL7) + kL7) ^ (~v & kH); }
+
+M6502_HD void x4_adc(St& s, uint32_t m) {
+    uint32_t co;
+    const uint32_t r = x4_add(s.a, m, s.p & kB1, co);
+    const uint32_t v = (s.a ^ r) & (m ^ r) & kH;
+    s.p = (s.p & (0x3Cu * kB1)) | x4_nzf(r) | co | (v >> 1);
+    s.a = r;
+}
+M6502_HD void x4_sbc(St& s, uint32_t m) {
+    uint32_t co;
+    const uint32_t r = x4_add(s.a, ~m, s.p & kB1, co);
+    const uint32_t v = (s.a ^ r) & (s.a ^ m) & kH;
+    s.p = (s.p & (0x3Cu * kB1)) | x4_nzf(r) | co | (v >> 1);
+    s.a = r;
+}
+M6502_HD void x4_cmp(St& s, uint32_t reg, uint32_t m) {
+    uint32_t co;   // reg + ~m + 1: the carry out is reg >= m
+    const uint32_t r = x4_add(reg, ~m, kB1, co);
+    s.p = (s.p & (0x7Cu * kB1)) | x4_nzf(r) | co;
+}
+M6502_HD uint32_t x4_asl(St& s, uint32_t v) {
+    const uint32_t r = (v & kL7) << 1;
+    s.p = (s.p & (0x7Cu * kB1)) | x4_nzf(r) | ((v >> 7) & kB1);
+    return r;
+}
+M6502_HD uint32_t x4_lsr(St& s, uint32_t v) {
+    const uint32_t r = (v >> 1) & kL7;
+    s.p = (s.p & (0x7Cu * kB1)) | x4_nzf(r) | (v & kB1);
+    return r;
+}
+M6502_HD uint32_t x4_rol(St& s, uint32_t v) {
+    const uint32_t r = ((v & kL7) << 1) | (s.p & kB1);
+    s.p = (s.p & (0x7Cu * kB1)) | x4_nzf(r) | ((v >> 7) & kB1);
+    return r;
+}
+M6502_HD uint32_t x4_ror(St& s, uint32_t v) {
+    const uint32_t r = ((v >> 1) & kL7) | ((s.p & kB1) << 7);
+    s.p = (s.p & (0x7Cu * kB1)) | x4_nzf(r) | (v & kB1);
+    return r;
+}
+M6502_HD void x4_push(St& s, uint32_t v) { s.s1 = s.s0; s.s0 = v; s.s = x4_dec(s.s); }
+M6502_HD uint32_t x4_pull(St& s) {
+    const uint32_t v = s.s0;
+    s.s0 = s.s1; s.s1 = 0; s.s = x4_inc(s.s);
+    return v;
+}
+
+#define M6502_OPCODES_X4(X) \
+    X(TAX, s.x = s.a; x4_set_nz(s, s.x)) \
+    X(TAY, s.y = s.a; x4_set_nz(s, s.y)) \
+    X(TXA, s.a = s.x; x4_set_nz(s, s.a)) \
+    X(TYA, s.a = s.y; x4_set_nz(s, s.a)) \
+    X(TSX, s.x = s.s; x4_set_nz(s, s.x)) \
+    X(TXS, s.s = s.x) \
+    X(INX, s.x = x4_inc(s.x); x4_set_nz(s, s.x)) \
+    X(INY, s.y = x4_inc(s.y); x4_set_nz(s, s.y)) \
+    X(DEX, s.x = x4_dec(s.x); x4_set_nz(s, s.x)) \
+    X(DEY, s.y = x4_dec(s.y); x4_set_nz(s, s.y)) \
+    X(ASL_A, s.a = x4_asl(s, s.a)) \
+    X(LSR_A, s.a = x4_lsr(s, s.a)) \
+    X(ROL_A, s.a = x4_rol(s, s.a)) \
+    X(ROR_A, s.a = x4_ror(s, s.a)) \
+    X(CLC, s.p &= ~(kFlagC * kB1)) \
+    X(SEC, s.p |= kFlagC * kB1) \
+    X(CLD, s.p &= ~(kFlagD * kB1)) \
+    X(SED, s.p |= kFlagD * kB1) \
+    X(CLI, s.p &= ~(kFlagI * kB1)) \
+    X(SEI, s.p |= kFlagI * kB1) \
+    X(CLV, s.p &= ~(kFlagV * kB1)) \
+    X(PHA, x4_push(s, s.a)) \
+    X(PLA, s.a = x4_pull(s); x4_set_nz(s, s.a)) \
+    X(PHP, x4_push(s, s.p | ((kFlagB | kFlagU) * kB1))) \
+    X(PLP, s.p = x4_pull(s)) \
+    X(NOP, (void)s) \
+    X(LDA_IMM, s.a = immw; x4_set_nz(s, immw)) \
+    X(LDX_IMM, s.x = immw; x4_set_nz(s, immw)) \
+    X(LDY_IMM, s.y = immw; x4_set_nz(s, immw)) \
+    X(ADC_IMM, x4_adc(s, immw)) \
+    X(SBC_IMM, x4_sbc(s, immw)) \
+    X(AND_IMM, s.a &= immw; x4_set_nz(s, s.a)) \
+    X(ORA_IMM, s.a |= immw; x4_set_nz(s, s.a)) \
+    X(EOR_IMM, s.a ^= immw; x4_set_nz(s, s.a)) \
+    X(CMP_IMM, x4_cmp(s, s.a, immw)) \
+    X(CPX_IMM, x4_cmp(s, s.x, immw)) \
+    X(CPY_IMM, x4_cmp(s, s.y, immw)) \
+    X(LDA_M, s.a = s.m; x4_set_nz(s, s.a)) \
+    X(LDX_M, s.x = s.m; x4_set_nz(s, s.x)) \
+    X(LDY_M, s.y = s.m; x4_set_nz(s, s.y)) \
+    X(STA_M, s.m = s.a) \
+    X(STX_M, s.m = s.x) \
+    X(STY_M, s.m = s.y) \
+    X(ADC_M, x4_adc(s, s.m)) \
+    X(SBC_M, x4_sbc(s, s.m)) \
+    X(AND_M, s.a &= s.m; x4_set_nz(s, s.a)) \
+    X(ORA_M, s.a |= s.m; x4_set_nz(s, s.a)) \
+    X(EOR_M, s.a ^= s.m; x4_set_nz(s, s.a)) \
+    X(CMP_M, x4_cmp(s, s.a, s.m)) \
+    X(CPX_M, x4_cmp(s, s.x, s.m)) \
+    X(CPY_M, x4_cmp(s, s.y, s.m)) \
+    X(INC_M, s.m = x4_inc(s.m); x4_set_nz(s, s.m)) \
+    X(DEC_M, s.m = x4_dec(s.m); x4_set_nz(s, s.m)) \
+    X(ASL_M, s.m = x4_asl(s, s.m)) \
+    X(LSR_M, s.m = x4_lsr(s, s.m)) \
+    X(ROL_M, s.m = x4_rol(s, s.m)) \
+    X(ROR_M, s.m = x4_ror(s, s.m)) \
+    X(BIT_M, s.p = (s.p & (0x3Du * kB1)) | (s.m & (0xC0u * kB1)) | (x4_zero(s.a & s.m) >> 6))
+
+// One instruction on the four states packed in s (see above).
+M6502_HD void exec_x4(St& s, uint32_t insn) {
+    const uint32_t immw = (insn >> 8) * kB1;
+    (void)immw;
+    switch (insn & 0xFFu) {
+#define M6502_CASE_X4(op, ...) case op: { __VA_ARGS__; } break;
+        M6502_OPCODES_X4(M6502_CASE_X4)
+#undef M6502_CASE_X4
+    default: break;
+    }
+}
+
 M6502_HD uint64_t pack(const St& s) {
     return (uint64_t)(s.a | (s.x << 8) | (s.y << 16) | (s.p << 24)) |
            ((uint64_t)(s.s | (s.m << 8) | (s.s0 << 16) | (s.s1 << 24)) << 32);

@@ -173,3 +173,15 @@ def test_draw_targets_matches_oracle_draw():
     var = I.draw_targets(2, 4, 8, 512, reject_pruned=False)
     assert len(var) == 512 and all(4 <= len(s) <= 8 for s in var)
     assert len({len(s) for s in var}) == 5
+
+
+def test_swar_exec_matches_scalar(tmp_path):
+    """exec_x4 (four machine states per 32-bit register, one dispatch) gives
+    the same result as four scalar exec calls for every instruction."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = str(tmp_path / "x4_check")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(root, "6502-optimizer_b200", "csrc"),
+                    "-o", exe, os.path.join(root, "tests", "x4_check.cpp")], check=True)
+    run = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert run.returncode == 0, run.stdout
