@@ -377,10 +377,6 @@ __device__ __forceinline__ bool probe_domain(const PairView& pv, uint32_t swept,
     return true;
 }
 
-// Sweeps states [s0, s1) of one cone; true when target and candidate agree
-// on the compared outputs in every state.  Warp-collective.  When `stop`
-// becomes nonzero (another item of the same pair failed) the sweep ends
-// early; its result is then irrelevant.
 // Four consecutive states s..s+3 (s a multiple of 4) packed one per byte
 // (see exec_x4).  They differ only in the low two bits of the lowest field,
 // so one scalar decode plus that field's four values builds them.
@@ -418,6 +414,10 @@ __device__ __forceinline__ uint32_t state_diff_x4(const PairView& pv, const Fiel
     return out_diff(t, c, m4);
 }
 
+// Sweeps states [s0, s1) of one cone; true when target and candidate agree
+// on the compared outputs in every state.  Warp-collective.  When `stop`
+// becomes nonzero (another item of the same pair failed) the sweep ends
+// early; its result is then irrelevant.
 // PER_LANE = 4: four consecutive states per lane packed one per byte
 // (exec_x4: one dispatch, byte-parallel arithmetic); 2: two states per lane
 // and dispatch; 1: one.  The packed path needs 4-aligned ranges and a
