@@ -1611,6 +1611,12 @@ struct m6502_ctx {
     cudaEvent_t sev[6] = {};   // stage boundaries of one pass
     cudaEvent_t sev2[6] = {};  // stage boundaries of the length-2 candidate phase
     cudaEvent_t aev[6 * kMaxAsyncPasses] = {};   // stage boundaries of the queued passes
+    struct SearchGraph {       // the queued passes of the last device-resident search, recorded
+        cudaGraphExec_t exec = nullptr;
+        std::vector<uint64_t> key;   // everything the recorded launches depend on
+        bool broken = false;         // recording failed once: launch directly from then on
+        std::string why;             // the error that stopped recording
+    } graph;
     DevBuf cnt_slots;          // Counters of the queued passes
     std::string err;
     std::mutex mu;
@@ -2138,63 +2144,117 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
         TRY(ensure(ctx, ctx->fail, scap * sizeof(uint32_t)));
         TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
         TRY(ensure(ctx, ctx->rules, rcap * sizeof(m6502_rule)));
-        CK(cudaMemsetAsync(slots, 0, npass * sizeof(Counters), ctx->stream));
-        for (uint64_t p = 0; p < npass; p++) {
-            const uint64_t b = p * P, nt = std::min(P, n - b);
-            const uint16_t* d_t;
-            if (on_dev) {
-                d_t = targets + b * tlen;
-            } else {   // stream order keeps the previous pass's kernels ahead of this copy
-                CK(cudaMemcpyAsync(ctx->targets.p, targets + b * tlen, nt * tlen * 2, cudaMemcpyHostToDevice,
-                                   ctx->stream));
-                d_t = (const uint16_t*)ctx->targets.p;
+        // All passes, queued with no host round trip.  Device-resident targets:
+        // recorded once as a CUDA graph and replayed by identical later calls.
+        bool capturing = false;
+        // Stage events: inside a capture they must be external record nodes
+        // (a plain record there only orders streams and records nothing).
+        auto rec = [&](cudaEvent_t e) -> cudaError_t {
+            return capturing ? cudaEventRecordWithFlags(e, ctx->stream, cudaEventRecordExternal)
+                             : cudaEventRecord(e, ctx->stream);
+        };
+        auto enqueue = [&]() -> int {
+            CK(cudaMemsetAsync(slots, 0, npass * sizeof(Counters), ctx->stream));
+            for (uint64_t p = 0; p < npass; p++) {
+                const uint64_t b = p * P, nt = std::min(P, n - b);
+                const uint16_t* d_t;
+                if (on_dev) {
+                    d_t = targets + b * tlen;
+                } else {   // stream order keeps the previous pass's kernels ahead of this copy
+                    CK(cudaMemcpyAsync(ctx->targets.p, targets + b * tlen, nt * tlen * 2, cudaMemcpyHostToDevice,
+                                       ctx->stream));
+                    d_t = (const uint16_t*)ctx->targets.p;
+                }
+                Counters* cnt = slots + p;
+                cudaEvent_t* ev = ctx->aev + 6 * p;
+                CK(rec(ev[0]));
+                if (scan) {
+                    k_fingerprint<FixedSeqs><<<ctx->fp_blocks, 256, 0, ctx->stream>>>(
+                        FixedSeqs{d_t, tlen}, nt, (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p);
+                    CKL("k_fingerprint(targets)");
+                }
+                CK(rec(ev[1]));
+                if (scan) {
+                    const uint32_t qgrid = (uint32_t)std::min<uint64_t>(ctx->qc_blocks, (nt + kQcTile - 1) / kQcTile);
+                    k_qc1<false><<<qgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
+                                                                 (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
+                                                                 (uint8_t*)ctx->cmeta1.p, dead, stages,
+                                                                 (Surv*)ctx->surv.p, scap, cnt);
+                    CKL("k_qc1");
+                } else {
+                    const uint32_t jgrid = (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8,
+                                                                        (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
+                    k_qc_join<false><<<jgrid, 256, 0, ctx->stream>>>(
+                        d_t, tlen, (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p, (uint8_t*)ctx->cmeta1.p,
+                        (const uint64_t*)ctx->join_keys[dead].p, (const uint16_t*)ctx->join_idx[dead].p,
+                        ctx->join_n[dead], dead, stages, (Surv*)ctx->surv.p, scap, cnt);
+                    CKL("k_qc_join");
+                }
+                CK(rec(ev[2]));
+                SurvSource src{(const Surv*)ctx->surv.p, d_t, tlen, dead, 0};
+                ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep,
+                           cfg.exh_mode == M6502_EXH_BRUTE};
+                if (exh) {
+                    k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &cnt->surv, scap, ea);
+                    CKL("k_exhaustive");
+                }
+                CK(rec(ev[3]));
+                if (exh) {
+                    k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
+                    CKL("k_exh_items");
+                }
+                CK(rec(ev[4]));
+                k_emit_all<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
+                                                                  (const uint32_t*)ctx->fail.p, nullptr, b, dead,
+                                                                  (m6502_rule*)ctx->rules.p, rcap, &slots[0].rules, cnt,
+                                                                  exh ? 1 : 0, d_t, tlen, cfg.sweep);
+                CKL("k_emit_all");
+                CK(rec(ev[5]));
             }
-            Counters* cnt = slots + p;
-            cudaEvent_t* ev = ctx->aev + 6 * p;
-            CK(cudaEventRecord(ev[0], ctx->stream));
-            if (scan) {
-                k_fingerprint<FixedSeqs><<<ctx->fp_blocks, 256, 0, ctx->stream>>>(
-                    FixedSeqs{d_t, tlen}, nt, (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p);
-                CKL("k_fingerprint(targets)");
-            }
-            CK(cudaEventRecord(ev[1], ctx->stream));
-            if (scan) {
-                const uint32_t qgrid = (uint32_t)std::min<uint64_t>(ctx->qc_blocks, (nt + kQcTile - 1) / kQcTile);
-                k_qc1<false><<<qgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
-                                                             (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
-                                                             (uint8_t*)ctx->cmeta1.p, dead, stages,
-                                                             (Surv*)ctx->surv.p, scap, cnt);
-                CKL("k_qc1");
+            return M6502_OK;
+        };
+        const bool use_graph = on_dev && !(cfg.flags & M6502_NO_GRAPH) && !ctx->graph.broken;
+        bool replayed = false, launched = false;
+        if (use_graph) {
+            const std::vector<uint64_t> key = {
+                (uint64_t)(uintptr_t)targets, n, tlen, cfg.semantics, cfg.sweep, cfg.exh_mode, stages,
+                cfg.flags, dead, scap, icap, rcap, P, (uint64_t)(uintptr_t)ctx->surv.p,
+                (uint64_t)(uintptr_t)ctx->fail.p, (uint64_t)(uintptr_t)ctx->items.p,
+                (uint64_t)(uintptr_t)ctx->rules.p, (uint64_t)(uintptr_t)ctx->cnt_slots.p,
+                (uint64_t)(uintptr_t)ctx->tfp.p, (uint64_t)(uintptr_t)ctx->tmeta.p,
+                (uint64_t)(uintptr_t)ctx->join_keys[dead].p};
+            if (!(ctx->graph.exec && ctx->graph.key == key)) {
+                if (ctx->graph.exec) { cudaGraphExecDestroy(ctx->graph.exec); ctx->graph.exec = nullptr; }
+                // Record; if recording or instantiation fails, this context stops
+                // using graphs and the passes are launched directly below.
+                cudaGraph_t g = nullptr;
+                bool ok = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                if (ok) {
+                    capturing = true;
+                    const int rc = enqueue();
+                    capturing = false;
+                    ok = cudaStreamEndCapture(ctx->stream, &g) == cudaSuccess && rc == M6502_OK && g;
+                    ok = ok && cudaGraphInstantiate(&ctx->graph.exec, g, 0) == cudaSuccess;
+                    if (g) cudaGraphDestroy(g);
+                }
+                if (!ok) {
+                    ctx->graph.exec = nullptr;
+                    ctx->graph.broken = true;
+                    ctx->graph.why = cudaGetErrorString(cudaGetLastError());   // clears the launch error
+                    set_err(ctx, M6502_OK, "CUDA graph recording failed (" + ctx->graph.why +
+                                               "); passes are launched directly");
+                } else {
+                    ctx->graph.key = key;
+                }
             } else {
-                const uint32_t jgrid = (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8,
-                                                                    (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
-                k_qc_join<false><<<jgrid, 256, 0, ctx->stream>>>(
-                    d_t, tlen, (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p, (uint8_t*)ctx->cmeta1.p,
-                    (const uint64_t*)ctx->join_keys[dead].p, (const uint16_t*)ctx->join_idx[dead].p,
-                    ctx->join_n[dead], dead, stages, (Surv*)ctx->surv.p, scap, cnt);
-                CKL("k_qc_join");
+                replayed = true;
             }
-            CK(cudaEventRecord(ev[2], ctx->stream));
-            SurvSource src{(const Surv*)ctx->surv.p, d_t, tlen, dead, 0};
-            ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep,
-                       cfg.exh_mode == M6502_EXH_BRUTE};
-            if (exh) {
-                k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &cnt->surv, scap, ea);
-                CKL("k_exhaustive");
+            if (ctx->graph.exec) {
+                CK(cudaGraphLaunch(ctx->graph.exec, ctx->stream));
+                launched = true;
             }
-            CK(cudaEventRecord(ev[3], ctx->stream));
-            if (exh) {
-                k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
-                CKL("k_exh_items");
-            }
-            CK(cudaEventRecord(ev[4], ctx->stream));
-            k_emit_all<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
-                                                              (const uint32_t*)ctx->fail.p, nullptr, b, dead,
-                                                              (m6502_rule*)ctx->rules.p, rcap, &slots[0].rules, cnt,
-                                                              exh ? 1 : 0, d_t, tlen, cfg.sweep);
-            CKL("k_emit_all");
-            CK(cudaEventRecord(ev[5], ctx->stream));
         }
+        if (!launched) TRY(enqueue());
         std::vector<Counters> hc(npass);
         CK(cudaMemcpyAsync(hc.data(), slots, npass * sizeof(Counters), cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
@@ -2243,6 +2303,7 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
                 st->passes += 1;
             }
             st->rules += nrules;
+            st->graph_replays = replayed ? 1u : 0u;
         }
         return M6502_OK;
     }
@@ -2350,6 +2411,7 @@ void m6502_destroy(m6502_ctx* ctx) {
     for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->sev2) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->aev) if (e) cudaEventDestroy(e);
+    if (ctx->graph.exec) cudaGraphExecDestroy(ctx->graph.exec);
     for (auto& t : ctx->cand2) {
         if (t.keys.p) cudaFree(t.keys.p);
         if (t.idx.p) cudaFree(t.idx.p);

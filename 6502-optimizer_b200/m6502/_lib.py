@@ -30,6 +30,7 @@ EXH_CONES, EXH_BRUTE = 0, 1
 CHECK_QC, CHECK_MID, CHECK_EXH, CHECK_ALL = 1, 2, 4, 7
 TARGETS_ON_DEVICE = 1
 QC_SCAN = 2
+NO_GRAPH = 4
 
 
 class M6502Error(RuntimeError):
@@ -65,7 +66,8 @@ class Stats(ctypes.Structure):
                 ("targets", "pairs", "qc_hits", "mid_hits", "exh_checked", "exh_passed",
                  "rules", "exh_states", "exh_items", "exh_algo_ops", "passes", "exh_probe_rejects")] + \
                [(n, ctypes.c_double) for n in ("ms_device", "ms_fingerprint", "ms_qc", "ms_exhaustive",
-                                               "ms_exh_items", "ms_emit")]
+                                               "ms_exh_items", "ms_emit")] + \
+               [("graph_replays", ctypes.c_uint64)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

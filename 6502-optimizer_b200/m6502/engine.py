@@ -122,7 +122,7 @@ class Engine:
 
     def search(self, targets, dead_flags=0, semantics=_lib.SEM_CUDA, sweep=_lib.SWEEP_FULL,
                exh_mode=_lib.EXH_CONES, stages=_lib.CHECK_ALL, max_cand_len=1, cap=None,
-               device_ptr=None, qc_scan=False):
+               device_ptr=None, qc_scan=False, graph=True):
         """Searches targets (n x tlen array of packed insns, or a device pointer with
         device_ptr=(ptr, n, tlen)) for shorter replacements.  Returns (rules, stats)."""
         if device_ptr is not None:
@@ -138,6 +138,8 @@ class Engine:
             flags = 0
         if qc_scan:
             flags |= _lib.QC_SCAN
+        if not graph:   # device-resident searches are otherwise recorded once and replayed as a CUDA graph
+            flags |= _lib.NO_GRAPH
         cfg = self._cfg(semantics, dead_flags, sweep, exh_mode, stages, max_cand_len, flags)
         cap = cap if cap is not None else max(1024, n // 2)
         with self._lock:

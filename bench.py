@@ -278,6 +278,7 @@ def run_engine(args):
                        "parallelism": f"strided target shards x{world}",
                        "l2": "512 MB buffer written between timed steps"},
             "len2_wall_s": total_ms / args.steps / 1000.0,
+            "cuda_graph_replayed": bool(s0.get("graph_replays", 0)),
             "rules": total_rules,
             "stage_counts": {k: s0[k] for k in ("qc_hits", "mid_hits", "exh_checked", "exh_passed", "rules",
                                                   "exh_states", "exh_items", "exh_probe_rejects")},

@@ -227,3 +227,24 @@ def test_overflow_fetch_returns_every_rule(engine):
     assert len(full) > 4
     assert sorted(map(key, small)) == sorted(map(key, full))
     assert st_small["passes"] == st_full["passes"]
+
+
+def test_device_search_replays_cuda_graph(engine):
+    """A device-resident search is recorded as a CUDA graph on its first call
+    and replayed by identical later calls; the rules equal those of the same
+    search launched without a graph, call after call."""
+    import torch
+    targets = np.asarray(oracle.draw_targets(0, 2, 256), dtype=np.uint16)
+    d = torch.from_numpy(targets.view(np.int16)).to("cuda:0")
+    key = lambda r: (int(r["target"]), tuple(int(x) for x in r["cand"][:r["cand_len"]]))  # noqa: E731
+    plain, _ = engine.search(None, sweep=_lib.SWEEP_FULL, device_ptr=(d.data_ptr(), len(targets), 2), graph=False)
+    want = sorted(map(key, plain))
+    replays = []
+    for _ in range(3):
+        rules, st = engine.search(None, sweep=_lib.SWEEP_FULL, device_ptr=(d.data_ptr(), len(targets), 2))
+        assert sorted(map(key, rules)) == want
+        replays.append(st["graph_replays"])
+    assert replays[1:] == [1, 1], engine._L.m6502_last_error(engine._ctx).decode()
+    d2 = d.clone()   # another buffer: recorded again
+    rules, st = engine.search(None, sweep=_lib.SWEEP_FULL, device_ptr=(d2.data_ptr(), len(targets), 2))
+    assert st["graph_replays"] == 0 and sorted(map(key, rules)) == want
