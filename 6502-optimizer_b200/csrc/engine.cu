@@ -329,8 +329,7 @@ __device__ __forceinline__ uint32_t out_diff(const St& t, const St& c, const Out
 // Target and candidate on one state: one loop over target then candidate (a
 // single inlined copy of the opcode switch per call site keeps the code, and
 // instruction-cache misses, small).
-__device__ __forceinline__ uint32_t state_diff(const PairView& pv, const Fields& f, const OutMask& m, uint64_t s) {
-    const St in = decode_state(f, s);
+__device__ __forceinline__ uint32_t state_diff_in(const PairView& pv, const OutMask& m, const St& in) {
     St c = in, t = in;
     const int n = pv.tn + pv.cn;
     for (int i = 0; i < n; i++) {
@@ -339,6 +338,9 @@ __device__ __forceinline__ uint32_t state_diff(const PairView& pv, const Fields&
     }
     if (pv.cn == 0) { t = c; c = in; }
     return out_diff(t, c, m);
+}
+__device__ __forceinline__ uint32_t state_diff(const PairView& pv, const Fields& f, const OutMask& m, uint64_t s) {
+    return state_diff_in(pv, m, decode_state(f, s));
 }
 
 // Target and candidate on two states per lane: one loop over target then
@@ -359,20 +361,43 @@ __device__ __forceinline__ uint32_t state_diff2(const PairView& pv, const Fields
 }
 
 
-// Probe: 64 pseudo-random states of the pair's whole sweep domain, all
-// outputs compared.  A mismatch anywhere in the domain decides the pair
-// (not equivalent) without the cone analysis; passing decides nothing.
+// One uniformly random state of a pair's whole sweep domain, from 64 random
+// bits: every swept register takes its own byte of z (its representative
+// value, c_rep[byte & 31], under the reduced sweep, A excepted), the carry
+// bit 63; the others hold the sweep's fixed values (S = 0xFD, the rest 0,
+// the other flags clear) -- the same domain make_fields(swept, swept, rep)
+// enumerates, drawn without packing a state index.
+__device__ __forceinline__ St probe_state(uint32_t swept, bool rep, uint64_t z) {
+    const uint32_t lo = (uint32_t)z, hi = (uint32_t)(z >> 32);
+    auto reg = [&](uint32_t loc, uint32_t byte, uint32_t fixed) -> uint32_t {
+        if (!(swept & LB(loc))) return fixed;
+        return rep ? c_rep[byte & 31u] : byte;
+    };
+    St in;
+    in.a = lo & 0xFFu;
+    in.x = reg(L_X, (lo >> 8) & 0xFFu, 0u);
+    in.y = reg(L_Y, (lo >> 16) & 0xFFu, 0u);
+    in.s = reg(L_S, lo >> 24, 0xFDu);
+    in.m = reg(L_M, hi & 0xFFu, 0u);
+    in.s0 = reg(L_S0, (hi >> 8) & 0xFFu, 0u);
+    in.s1 = reg(L_S1, (hi >> 16) & 0xFFu, 0u);
+    in.p = hi >> 31;
+    return in;
+}
+
+// Probe: 64 pseudo-random states of the pair's whole sweep domain (A and
+// carry always swept), all outputs compared.  A mismatch anywhere in the
+// domain decides the pair (not equivalent) without the cone analysis;
+// passing decides nothing.
 __device__ __forceinline__ bool probe_domain(const PairView& pv, uint32_t swept, bool rep, uint32_t dead,
                                              uint64_t salt, int lane) {
-    Fields f = make_fields(swept, swept, rep);
     const OutMask m = out_mask(cmp_mask(dead));
-    const uint64_t dom = (f.bits >= 64) ? ~0ull : ((1ull << f.bits) - 1);
     for (int it = 0; it < 2; it++) {   // 32 states at a time: most failing pairs fail in the first
         uint64_t z = salt + (uint64_t)(lane + 32 * it) * 0x9E3779B97F4A7C15ull;
         z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
         z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
         z ^= z >> 31;
-        if (__any_sync(kFull, state_diff(pv, f, m, z & dom) != 0)) return false;
+        if (__any_sync(kFull, state_diff_in(pv, m, probe_state(swept, rep, z)) != 0)) return false;
     }
     return true;
 }
@@ -563,15 +588,19 @@ __device__ Groups make_groups(const Flow& fl, uint32_t dead, bool rep, bool brut
 
 // The same composition reading the dependency table from shared memory
 // (13 lanes read 13 different entries: constant memory would serialise).
+// Most locations of an instruction depend on nothing or on themselves only,
+// so only the locations that feed another one (`cross`, a few per
+// instruction) are fetched from their lanes.
 __device__ __forceinline__ uint32_t compose_s(uint32_t D, const uint16_t* seq, int n, int lane, uint32_t& written,
                                               uint32_t& sweep, const uint16_t (*dep_tab)[NUM_LOCS]) {
     for (int i = 0; i < n; i++) {
         uint32_t op = seq[i] & 0xFFu;
         uint32_t dep = (lane < NUM_LOCS) ? dep_tab[op][lane] : 0u;
-        uint32_t nd = 0;
-#pragma unroll
-        for (int l = 0; l < NUM_LOCS; l++) {
-            uint32_t x = __shfl_sync(kFull, D, l);
+        const uint32_t self = 1u << lane;
+        uint32_t nd = (dep & self) ? D : 0u;
+        for (uint32_t cross = __reduce_or_sync(kFull, dep & ~self); cross; cross &= cross - 1) {
+            const int l = __ffs(cross) - 1;
+            const uint32_t x = __shfl_sync(kFull, D, l);
             if (dep & (1u << l)) nd |= x;
         }
         D = nd;
@@ -612,10 +641,10 @@ __device__ __forceinline__ LaneGroups lane_groups(const Flow& fl, uint32_t dead,
     const bool act = lane < NUM_LOCS && ((g.active >> lane) & 1u);
     g.my = act ? fl.cone : 0u;
     bool ismax = act;
-#pragma unroll
-    for (int q = 0; q < NUM_LOCS; q++) {
+    for (uint32_t rest = g.active & ((1u << NUM_LOCS) - 1u); rest; rest &= rest - 1) {   // compared outputs only
+        const int q = __ffs(rest) - 1;
         const uint32_t cq = __shfl_sync(kFull, g.my, q);
-        if (((g.active >> q) & 1u) && q != lane && (cq & g.my) == g.my && (cq != g.my || q < lane)) ismax = false;
+        if (q != lane && (cq & g.my) == g.my && (cq != g.my || q < lane)) ismax = false;
     }
     g.maxm = __ballot_sync(kFull, ismax);
     g.mybits = ismax ? cone_bits(g.my, rep) : 0xFFu;
@@ -1130,12 +1159,15 @@ __global__ void __launch_bounds__(256, 4) k_exhaustive(Src src, const unsigned l
     const uint64_t n = min((uint64_t)*n_pairs_ptr, n_cap);
     unsigned long long nstates = 0, probe_rej = 0;
     unsigned long long next = 0, lim = 0;   // this warp's batch of tickets
+    // Lane 0 claims the following batch while the warp works on the current
+    // one, so the atomic's latency is hidden behind a batch of pairs.
+    unsigned long long ahead = 0;
+    if (lane == 0) ahead = atomicAdd(&a.cnt->exh_ticket, (unsigned long long)kTicketBatch);
     for (;;) {
         if (next >= lim) {
-            unsigned long long b = 0;
-            if (lane == 0) b = atomicAdd(&a.cnt->exh_ticket, (unsigned long long)kTicketBatch);
-            next = __shfl_sync(kFull, b, 0);
+            next = __shfl_sync(kFull, ahead, 0);
             lim = next + kTicketBatch;
+            if (lane == 0 && next < n) ahead = atomicAdd(&a.cnt->exh_ticket, (unsigned long long)kTicketBatch);
         }
         const unsigned long long p = next++;
         if (p >= n) break;
