@@ -55,6 +55,7 @@ constexpr uint64_t kMaxItemsPerCone = 1ull << 16;   // larger cones get larger i
 // more; they get the verdict "undecided" instead of an endless sweep.
 constexpr uint32_t kMaxConeBits = 34;
 constexpr unsigned kTicketBatch = 4;           // pairs a warp takes per ticket atomic
+constexpr int kJoinBatch = 4;                  // candidate rows a join warp loads before using them
 constexpr int kMaxAsyncPasses = 64;            // passes of one search queued without a host round trip
 
 // Test vectors: TestVectors + MidCheckVectors of pkg/search/verifier.go:18-67
@@ -918,32 +919,50 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint16_t* __restrict__ ta
         uint32_t end = lo;
         while (end < nsorted && s_key[end] == key) end++;
         if (lo == end) continue;
-        for (uint32_t i = lo; i < end; i++) {
-            const uint32_t c = s_idx[i];
-            const uint32_t cm = s_meta[c];
-            const uint32_t cb = GO ? ((cm >> 2) & 3u) : (cm & 3u);
-            if ((cm & 0x10u) || cb >= tb) continue;          // pruned or not shorter (uniform)
-            const uint64_t x = tv ^ cfp_cm[(uint64_t)c * 32 + lane];   // one coalesced 256-byte row
-            const unsigned lo_eq = __ballot_sync(kFull, (x & loose) == 0);
-            const unsigned ex_eq = __ballot_sync(kFull, (x & exact) == 0);
-            if ((lo_eq & 0xFFu) != 0xFFu) continue;          // QuickCheck fails
-            bool pass = false;
-            uint32_t code = c;
-            if (!GO) {
-                nqc += lane == 0;
-                const bool mid = !(stages & M6502_CHECK_MID) || lo_eq == kFull;
-                if (mid) { nmid += lane == 0; pass = true; }
-            } else if ((ex_eq & 0xFFu) == 0xFFu) {           // processTask: unmasked QC passes
-                nqc += lane == 0; nmid += lane == 0; pass = true;
-            } else if (dead) {                               // processTaskMasked, FlagDiff != 0
-                uint32_t fd = lane < 8 ? ((uint32_t)(x >> 24) & kPMask) : 0u;
-                fd = __reduce_or_sync(kFull, fd);
-                if (fd) {
-                    nqc += lane == 0; nmid += lane == 0; pass = true;
-                    code = c | kSurvMasked | (fd_pack(fd) << 25);
+        for (uint32_t i0 = lo; i0 < end; i0 += kJoinBatch) {
+            // The rows of up to kJoinBatch candidates are loaded before any is
+            // used, so their latencies overlap.
+            uint64_t row[kJoinBatch];
+            uint32_t cidx[kJoinBatch];
+            bool keep[kJoinBatch];
+#pragma unroll
+            for (int j = 0; j < kJoinBatch; j++) {
+                keep[j] = false; row[j] = 0; cidx[j] = 0;
+                if (i0 + j < end) {
+                    const uint32_t c = s_idx[i0 + j];
+                    const uint32_t cm = s_meta[c];
+                    const uint32_t cb = GO ? ((cm >> 2) & 3u) : (cm & 3u);
+                    cidx[j] = c;
+                    keep[j] = !((cm & 0x10u) || cb >= tb);   // pruned or not shorter (uniform)
+                    if (keep[j]) row[j] = cfp_cm[(uint64_t)c * 32 + lane];   // one coalesced 256-byte row
                 }
             }
-            stage_push(pass && lane == 0, Surv{t, code}, stage, nstage, surv, cap, &cnt->surv, lane);
+#pragma unroll
+            for (int j = 0; j < kJoinBatch; j++) {
+                if (!keep[j]) continue;
+                const uint32_t c = cidx[j];
+                const uint64_t x = tv ^ row[j];
+                const unsigned lo_eq = __ballot_sync(kFull, (x & loose) == 0);
+                const unsigned ex_eq = __ballot_sync(kFull, (x & exact) == 0);
+                if ((lo_eq & 0xFFu) != 0xFFu) continue;          // QuickCheck fails
+                bool pass = false;
+                uint32_t code = c;
+                if (!GO) {
+                    nqc += lane == 0;
+                    const bool mid = !(stages & M6502_CHECK_MID) || lo_eq == kFull;
+                    if (mid) { nmid += lane == 0; pass = true; }
+                } else if ((ex_eq & 0xFFu) == 0xFFu) {           // processTask: unmasked QC passes
+                    nqc += lane == 0; nmid += lane == 0; pass = true;
+                } else if (dead) {                               // processTaskMasked, FlagDiff != 0
+                    uint32_t fd = lane < 8 ? ((uint32_t)(x >> 24) & kPMask) : 0u;
+                    fd = __reduce_or_sync(kFull, fd);
+                    if (fd) {
+                        nqc += lane == 0; nmid += lane == 0; pass = true;
+                        code = c | kSurvMasked | (fd_pack(fd) << 25);
+                    }
+                }
+                stage_push(pass && lane == 0, Surv{t, code}, stage, nstage, surv, cap, &cnt->surv, lane);
+            }
         }
     }
     stage_flush(stage, nstage, surv, cap, &cnt->surv, lane);
