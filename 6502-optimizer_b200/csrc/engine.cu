@@ -56,6 +56,7 @@ constexpr uint64_t kMaxItemsPerCone = 1ull << 16;   // larger cones get larger i
 constexpr uint32_t kMaxConeBits = 34;
 constexpr unsigned kTicketBatch = 4;           // pairs a warp takes per ticket atomic
 constexpr int kJoinBatch = 4;                  // candidate rows a join warp loads before using them
+constexpr int kDirBits = 12;                   // key-bucket directory of the length-1 join (4,096 buckets)
 constexpr int kMaxAsyncPasses = 64;            // passes of one search queued without a host round trip
 
 // Test vectors: TestVectors + MidCheckVectors of pkg/search/verifier.go:18-67
@@ -890,6 +891,7 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint16_t* __restrict__ ta
     __shared__ uint64_t s_key[kNumInsns];
     __shared__ uint16_t s_idx[kNumInsns];
     __shared__ uint8_t s_meta[kNumInsns];
+    __shared__ uint16_t s_dir[(1u << kDirBits) + 1];
     __shared__ Surv s_stage[kWarpsPerBlock][kStage];
     Surv* stage = s_stage[threadIdx.x >> 5];
     int nstage = 0;
@@ -899,25 +901,53 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint16_t* __restrict__ ta
     }
     for (uint32_t i = threadIdx.x; i < (uint32_t)kNumInsns; i += blockDim.x) s_meta[i] = cmeta[i];
     __syncthreads();
+    // Bucket directory over the keys' top kDirBits bits: s_dir[b] is the
+    // first index whose key lies in bucket b or above.  Index i fills the
+    // buckets above its predecessor's, up to its own.
+    for (uint32_t i = threadIdx.x; i <= nsorted; i += blockDim.x) {
+        const uint32_t b0 = i == 0 ? 0u : (uint32_t)(s_key[i - 1] >> (64 - kDirBits)) + 1u;
+        const uint32_t b1 = i == nsorted ? (1u << kDirBits) : (uint32_t)(s_key[i] >> (64 - kDirBits));
+        for (uint32_t b = b0; b <= b1; b++) s_dir[b] = (uint16_t)i;
+    }
+    __syncthreads();
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t loose = cmp_mask(dead), exact = cmp_mask(0);
+    const uint64_t vin = c_vec[lane];   // lane v's test vector, read once
     unsigned long long nqc = 0, nmid = 0;
-    for (uint32_t t = blockIdx.x * kWarpsPerBlock + w; t < nt; t += gridDim.x * kWarpsPerBlock) {
+    const uint32_t stride = gridDim.x * kWarpsPerBlock;
+    uint32_t t = blockIdx.x * kWarpsPerBlock + w;
+    // Lane i holds instruction i of the warp's target (tlen <= 32); the next
+    // target's are loaded while this one is processed.
+    uint32_t ins_next = (t < nt && lane < (int)tlen) ? targets[(uint64_t)t * tlen + lane] : 0u;
+    for (; t < nt; t += stride) {
+        const uint32_t ins = ins_next;
+        const uint64_t tnext = (uint64_t)t + stride;
+        ins_next = (tnext < nt && lane < (int)tlen) ? targets[tnext * tlen + lane] : 0u;
         // The target's outputs, computed here rather than stored: lane v runs
-        // it on vector v (its instructions are warp-uniform loads).
-        const uint16_t* ts = targets + (uint64_t)t * tlen;
-        St st = unpack(c_vec[lane]);
-        uint32_t tb = 0;
-        for (uint32_t i = 0; i < tlen; i++) {
-            const uint16_t insn = ts[i];
-            exec(st, insn);
-            tb += GO ? bytes_go(insn & 0xFFu) : bytes_cuda(insn & 0xFFu);
-        }
+        // it on vector v (its instructions are warp-uniform shuffles).
+        St st = unpack(vin);
+        for (uint32_t i = 0; i < tlen; i++) exec(st, __shfl_sync(kFull, ins, (int)i));
+        const uint32_t tb = __reduce_add_sync(
+            kFull, lane < (int)tlen ? (GO ? bytes_go(ins & 0xFFu) : bytes_cuda(ins & 0xFFu)) : 0u);
         const uint64_t tv = fp_of(st);   // lane v holds the target's output on vector v
         const uint64_t key = warp_key(tv, loose, lane);
-        const uint32_t lo = warp_lower_bound(s_key, nsorted, key, lane);
-        uint32_t end = lo;
-        while (end < nsorted && s_key[end] == key) end++;
+        // The equal range within the key's bucket: one compare per lane when
+        // the bucket holds at most 32 keys, else a search inside it.
+        const uint32_t bkt = (uint32_t)(key >> (64 - kDirBits));
+        uint32_t lo = s_dir[bkt], end;
+        const uint32_t bhi = s_dir[bkt + 1];
+        if (bhi - lo <= 32) {
+            const uint32_t i = lo + (uint32_t)lane;
+            const uint64_t k = i < bhi ? s_key[i] : ~0ull;
+            const unsigned below = __ballot_sync(kFull, i < bhi && k < key);
+            const unsigned same = __ballot_sync(kFull, i < bhi && k == key);
+            lo += (uint32_t)__popc(below);
+            end = lo + (uint32_t)__popc(same);
+        } else {
+            lo += warp_lower_bound(s_key + lo, bhi - lo, key, lane);
+            end = lo;
+            while (end < bhi && s_key[end] == key) end++;
+        }
         if (lo == end) continue;
         for (uint32_t i0 = lo; i0 < end; i0 += kJoinBatch) {
             // The rows of up to kJoinBatch candidates are loaded before any is
