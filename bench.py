@@ -148,7 +148,7 @@ def run_reference(args):
 # Issue-slot utilisation (smsp__issue_active.avg.pct_of_peak_sustained_active)
 # of the committed ncu captures in profiles/ (k_exhaustive_len2.md,
 # k_qc_join_len2.md, k_exh_items_len2.md).
-ISSUE_ACTIVE = {"k_exhaustive": 0.633, "k_qc_join": 0.701, "k_exh_items": 0.204}
+ISSUE_ACTIVE = {"k_exhaustive": 0.676, "k_qc_join": 0.726, "k_exh_items": 0.204}
 
 
 def load_traffic():
