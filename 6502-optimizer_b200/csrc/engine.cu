@@ -1554,6 +1554,15 @@ __global__ void k_exec_batch(CsrSeqs src, uint64_t n, const uint64_t* __restrict
     }
 }
 
+// Sets *bad when an instruction word's opcode is outside the table (the
+// search's input check for targets in device memory).
+__global__ void k_check_ops(const uint16_t* __restrict__ ins, uint64_t n, uint32_t* __restrict__ bad) {
+    bool b = false;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        b |= (ins[i] & 0xFFu) >= (uint32_t)NUM_OPS;
+    if (__any_sync(kFull, b) && (threadIdx.x & 31) == 0) *bad = 1u;
+}
+
 // Pruned target enumeration: ids in [id0, id1) of the length-L space,
 // compacted into targets/ids (order unspecified).
 __global__ void k_enum_targets(uint64_t id0, uint64_t id1, uint32_t len, uint16_t* __restrict__ targets,
@@ -1699,6 +1708,8 @@ struct m6502_ctx {
         std::string why;             // the error that stopped recording
     } graph;
     DevBuf cnt_slots;          // Counters of the queued passes
+    DevBuf tall;               // host targets of a queued search, copied to the device at once
+    DevBuf opflag;             // k_check_ops result
     std::string err;
     std::mutex mu;
     int sms = 148;
@@ -2197,9 +2208,9 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
 // global target index.  One synchronisation at the end reads every pass's
 // counters; if any buffer overflowed, the whole search is re-run with larger
 // buffers (nothing is dropped).  Returns M6502_E_INVAL when the search does
-// not fit this path.
+// not fit this path.  `targets` is in device memory.
 int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* targets, uint64_t n, uint32_t tlen,
-                 bool on_dev, m6502_stats* st, m6502_rule* out, uint64_t out_cap, bool* delivered) {
+                 m6502_stats* st, m6502_rule* out, uint64_t out_cap, bool* delivered) {
     *delivered = false;
     const uint64_t P = ctx->pass_targets;
     const uint64_t npass = (n + P - 1) / P;
@@ -2216,7 +2227,6 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
         TRY(ensure(ctx, ctx->tfp, pmax * 32 * sizeof(uint64_t)));
         TRY(ensure(ctx, ctx->tmeta, pmax));
     }
-    if (!on_dev) TRY(ensure(ctx, ctx->targets, pmax * tlen * 2));
     if (!scan) TRY(join_table(ctx, dead));
     TRY(ensure(ctx, ctx->cnt_slots, npass * sizeof(Counters)));
     Counters* slots = (Counters*)ctx->cnt_slots.p;
@@ -2225,8 +2235,8 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
         TRY(ensure(ctx, ctx->fail, scap * sizeof(uint32_t)));
         TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
         TRY(ensure(ctx, ctx->rules, rcap * sizeof(m6502_rule)));
-        // All passes, queued with no host round trip.  Device-resident targets:
-        // recorded once as a CUDA graph and replayed by identical later calls.
+        // All passes, queued with no host round trip, recorded once as a CUDA
+        // graph and replayed by identical later calls.
         bool capturing = false;
         // Stage events: inside a capture they must be external record nodes
         // (a plain record there only orders streams and records nothing).
@@ -2238,14 +2248,7 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
             CK(cudaMemsetAsync(slots, 0, npass * sizeof(Counters), ctx->stream));
             for (uint64_t p = 0; p < npass; p++) {
                 const uint64_t b = p * P, nt = std::min(P, n - b);
-                const uint16_t* d_t;
-                if (on_dev) {
-                    d_t = targets + b * tlen;
-                } else {   // stream order keeps the previous pass's kernels ahead of this copy
-                    CK(cudaMemcpyAsync(ctx->targets.p, targets + b * tlen, nt * tlen * 2, cudaMemcpyHostToDevice,
-                                       ctx->stream));
-                    d_t = (const uint16_t*)ctx->targets.p;
-                }
+                const uint16_t* d_t = targets + b * tlen;
                 Counters* cnt = slots + p;
                 cudaEvent_t* ev = ctx->aev + 6 * p;
                 CK(rec(ev[0]));
@@ -2294,7 +2297,7 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
             }
             return M6502_OK;
         };
-        const bool use_graph = on_dev && !(cfg.flags & M6502_NO_GRAPH) && !ctx->graph.broken;
+        const bool use_graph = !(cfg.flags & M6502_NO_GRAPH) && !ctx->graph.broken;
         bool replayed = false, launched = false;
         if (use_graph) {
             const std::vector<uint64_t> key = {
@@ -2419,6 +2422,21 @@ bool valid_seq(const uint16_t* s, uint64_t n) {
     return true;
 }
 
+// The opcode check of n instruction words already in device memory: one
+// pass over them and a 4-byte read-back.
+int check_ops_device(m6502_ctx* ctx, const uint16_t* d_ins, uint64_t n) {
+    if (n == 0) return M6502_OK;
+    TRY(ensure(ctx, ctx->opflag, sizeof(uint32_t)));
+    CK(cudaMemsetAsync(ctx->opflag.p, 0, sizeof(uint32_t), ctx->stream));
+    const uint32_t grid = (uint32_t)std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sms * 16);
+    k_check_ops<<<grid, 256, 0, ctx->stream>>>(d_ins, n, (uint32_t*)ctx->opflag.p);
+    CKL("k_check_ops");
+    uint32_t bad = 0;
+    CK(cudaMemcpyAsync(&bad, ctx->opflag.p, sizeof bad, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return bad ? set_err(ctx, M6502_E_INVAL, "opcode out of range") : M6502_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -2487,7 +2505,8 @@ void m6502_destroy(m6502_ctx* ctx) {
                       &ctx->st_keys2, &ctx->st_vals2, &ctx->st_rep, &ctx->st_ord, &ctx->st_verdict,
                       &ctx->st_vlist, &ctx->st_vpos, &ctx->st_sort_tmp, &ctx->c2_keys_in, &ctx->c2_idx_in,
                       &ctx->c2_sort_tmp, &ctx->go_keys, &ctx->go_keys2, &ctx->go_ord, &ctx->go_round,
-                      &ctx->go_sort_tmp, &ctx->jitems, &ctx->cnt_slots, &ctx->st_vphase, &ctx->st_pphase};
+                      &ctx->go_sort_tmp, &ctx->jitems, &ctx->cnt_slots, &ctx->st_vphase, &ctx->st_pphase,
+                      &ctx->tall, &ctx->opflag};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->sev2) if (e) cudaEventDestroy(e);
@@ -2649,14 +2668,26 @@ int m6502_search(m6502_ctx* ctx, const m6502_search_cfg* cfg, const uint16_t* ta
     if (n > 0xFFFFFFFFull) return set_err(ctx, M6502_E_INVAL, "too many targets for one call");
     if (n && !targets) return set_err(ctx, M6502_E_INVAL, "NULL targets");
     const bool on_dev = (cfg->flags & M6502_TARGETS_ON_DEVICE) != 0;
-    if (!on_dev && !valid_seq(targets, n * tlen)) return set_err(ctx, M6502_E_INVAL, "opcode out of range");
+    const bool async_ok = cfg->semantics == M6502_SEM_CUDA && cfg->max_cand_len <= 1 &&
+                          n <= (uint64_t)kMaxAsyncPasses * ctx->pass_targets;
+    // Opcodes are checked on the host only for host targets searched pass
+    // by pass; queued searches check them on the device.
+    if (!on_dev && !async_ok && !valid_seq(targets, n * tlen))
+        return set_err(ctx, M6502_E_INVAL, "opcode out of range");
     CK(cudaSetDevice(ctx->device));
     m6502_stats st;
     std::memset(&st, 0, sizeof st);
     ctx->staging.clear();
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
-    const bool async_ok = cfg->semantics == M6502_SEM_CUDA && cfg->max_cand_len <= 1 &&
-                          n <= (uint64_t)kMaxAsyncPasses * ctx->pass_targets;
+    // A queued search of host targets copies them all to the device first and
+    // then runs exactly as a device-resident one (CUDA graph included).
+    const uint16_t* q_targets = targets;
+    if (async_ok && n && !on_dev) {
+        TRY(ensure(ctx, ctx->tall, n * tlen * sizeof(uint16_t)));
+        CK(cudaMemcpyAsync(ctx->tall.p, targets, n * tlen * sizeof(uint16_t), cudaMemcpyHostToDevice, ctx->stream));
+        q_targets = (const uint16_t*)ctx->tall.p;
+    }
+    if (on_dev || (async_ok && n)) TRY(check_ops_device(ctx, q_targets, n * tlen));
     for (uint64_t b = async_ok ? n : 0; b < n; b += ctx->pass_targets) {   // passes one by one otherwise
         uint64_t nt = std::min<uint64_t>(ctx->pass_targets, n - b);
         const uint16_t* d_t;
@@ -2670,7 +2701,7 @@ int m6502_search(m6502_ctx* ctx, const m6502_search_cfg* cfg, const uint16_t* ta
         TRY(run_pass(ctx, *cfg, d_t, nt, tlen, nullptr, b, &st));
     }
     bool delivered = false;
-    if (async_ok && n) TRY(search_async(ctx, *cfg, targets, n, tlen, on_dev, &st, out, cap, &delivered));
+    if (async_ok && n) TRY(search_async(ctx, *cfg, q_targets, n, tlen, &st, out, cap, &delivered));
     CK(cudaEventRecord(ctx->ev1, ctx->stream));
     CK(cudaEventSynchronize(ctx->ev1));
     float ms = 0;

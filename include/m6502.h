@@ -70,7 +70,8 @@ enum {
 
 /* m6502_search_cfg.flags */
 enum {
-    M6502_TARGETS_ON_DEVICE = 1, /* `targets` is a device pointer (already in HBM) */
+    M6502_TARGETS_ON_DEVICE = 1, /* `targets` is a device pointer (already in HBM); its
+                                    opcodes are checked on the device */
     M6502_QC_SCAN = 2,           /* QuickCheck by scanning every pair instead of the
                                     exact join on vector-0 outputs (same survivors) */
     M6502_NO_GRAPH = 4           /* do not record or replay the search as a CUDA graph */
@@ -132,8 +133,9 @@ typedef struct m6502_stats {
     double ms_fingerprint, ms_qc, ms_exhaustive, ms_exh_items, ms_emit; /* per-stage
                               device time summed over passes, CUDA events */
     uint64_t graph_replays; /* 1 when the call replayed the CUDA graph recorded by an
-                              earlier identical call (device-resident targets, CUDA
-                              semantics, length-1 candidates), else 0 */
+                              earlier identical call (CUDA semantics, length-1
+                              candidates; host targets are first copied to the
+                              device), else 0 */
 } m6502_stats;
 
 /* ---- context ---- */

@@ -248,3 +248,31 @@ def test_device_search_replays_cuda_graph(engine):
     d2 = d.clone()   # another buffer: recorded again
     rules, st = engine.search(None, sweep=_lib.SWEEP_FULL, device_ptr=(d2.data_ptr(), len(targets), 2))
     assert st["graph_replays"] == 0 and sorted(map(key, rules)) == want
+
+
+def test_host_search_is_queued_and_checks_opcodes_on_the_device(engine):
+    """Host targets of a queued search are copied to the device at once and
+    searched like device-resident ones: identical calls replay one CUDA graph
+    and give the rules of the unrecorded search.  An opcode outside the table
+    is refused with M6502_E_INVAL for host and device targets alike (the
+    device check runs before any search kernel)."""
+    import torch
+    targets = np.asarray(oracle.draw_targets(0, 2, 256), dtype=np.uint16)
+    key = lambda r: (int(r["target"]), tuple(int(x) for x in r["cand"][:r["cand_len"]]))  # noqa: E731
+    plain, _ = engine.search(targets, sweep=_lib.SWEEP_FULL, graph=False)
+    want = sorted(map(key, plain))
+    replays = []
+    for _ in range(3):
+        rules, st = engine.search(targets, sweep=_lib.SWEEP_FULL)
+        assert sorted(map(key, rules)) == want
+        replays.append(st["graph_replays"])
+    assert replays[1:] == [1, 1], engine._L.m6502_last_error(engine._ctx).decode()
+    bad = targets.copy()
+    bad[200, 1] = 0x3A
+    with pytest.raises(m6502.M6502Error):
+        engine.search(bad)
+    d = torch.from_numpy(bad.view(np.int16)).to("cuda:0")
+    with pytest.raises(m6502.M6502Error):
+        engine.search(None, device_ptr=(d.data_ptr(), len(bad), 2))
+    rules, _ = engine.search(targets, sweep=_lib.SWEEP_FULL)   # the context is still usable
+    assert sorted(map(key, rules)) == want
