@@ -2417,9 +2417,10 @@ int finish(m6502_ctx* ctx, m6502_rule* out, uint64_t cap, uint64_t* n_out) {
     return M6502_OK;
 }
 
-bool valid_seq(const uint16_t* s, uint64_t n) {
-    for (uint64_t i = 0; i < n; i++) if ((s[i] & 0xFF) >= NUM_OPS) return false;
-    return true;
+bool valid_seq(const uint16_t* s, uint64_t n) {   // no early exit: the loop vectorises
+    uint32_t bad = 0;
+    for (uint64_t i = 0; i < n; i++) bad |= (uint32_t)((s[i] & 0xFFu) >= (uint32_t)NUM_OPS);
+    return bad == 0;
 }
 
 // The opcode check of n instruction words already in device memory: one

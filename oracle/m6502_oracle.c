@@ -574,6 +574,37 @@ int or_exhaustive(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t 
     return 1;
 }
 
+/* A state of the full-sweep domain of (t, c) on which the two differ,
+ * looked for among `tries` states drawn uniformly from that domain
+ * (splitmix64 from `seed`): any A and carry, any value of every extra
+ * register either sequence reads, the rest as in or_exhaustive.  Returns 1
+ * and writes the state to *out, or 0 when no drawn state differs.  This
+ * project's check, not the reference's: it shows pairs that the reduced
+ * sweep (32 representative values when three or more extra registers are
+ * read) accepts and the full sweep rejects. */
+int or_full_sweep_witness(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead,
+                          uint64_t tries, uint64_t seed, or_state *out) {
+    int extra[6];
+    int k = or_swept_regs(t, tn, c, cn, extra);
+    uint64_t z = seed;
+    for (uint64_t i = 0; i < tries; i++) {
+        z += 0x9E3779B97F4A7C15ull;
+        uint64_t r = z;
+        r = (r ^ (r >> 30)) * 0xBF58476D1CE4E5B9ull;
+        r = (r ^ (r >> 27)) * 0x94D049BB133111EBull;
+        r ^= r >> 31;
+        or_state s;
+        memset(&s, 0, sizeof s);
+        s.A = (uint8_t)r; s.P = (uint8_t)((r >> 8) & 1u); s.S = 0xFD;
+        for (int j = 0; j < k; j++) set_reg(&s, extra[j], (uint8_t)(r >> (16 + 8 * j)));
+        or_state x = s, y = s;
+        or_exec_seq(&x, t, tn);
+        or_exec_seq(&y, c, cn);
+        if (!or_states_equal(&x, &y, dead)) { *out = s; return 1; }
+    }
+    return 0;
+}
+
 /* ------------------------------------------------------------------ */
 /* Search drivers                                                      */
 /* ------------------------------------------------------------------ */

@@ -70,6 +70,8 @@ int  or_midcheck(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t d
 int  or_exhaustive(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead, int sweep);
 uint8_t or_flagdiff(const uint16_t *t, int tn, const uint16_t *c, int cn);
 int  or_swept_regs(const uint16_t *t, int tn, const uint16_t *c, int cn, int *extra);
+int  or_full_sweep_witness(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead,
+                           uint64_t tries, uint64_t seed, or_state *out);
 
 /* ---- Pruner (pkg/search/pruner.go) ---- */
 int or_should_prune(const uint16_t *seq, int n);

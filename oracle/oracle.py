@@ -112,6 +112,15 @@ def flagdiff(t, c):
     return int(_pair(lib().or_flagdiff, t, c))
 
 
+def full_sweep_witness(t, c, dead=0, tries=1 << 22, seed=0):
+    """A full-sweep domain state (A, X, Y, P, S, M, S0, S1) on which t and c
+    differ, among `tries` uniform draws; None if no draw differs."""
+    s = State()
+    ok = _pair(lib().or_full_sweep_witness, t, c, ctypes.c_uint8(dead), ctypes.c_uint64(tries),
+               ctypes.c_uint64(seed), ctypes.byref(s))
+    return s.tuple() if ok else None
+
+
 def fingerprint(seq):
     a, p, n = _seq(seq)
     out = (ctypes.c_uint8 * 64)()
