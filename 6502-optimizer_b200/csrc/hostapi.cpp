@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <memory>
 #include <string>
 
 #include "isa.cuh"
@@ -26,6 +27,33 @@ const char* const kMnemonic[NUM_OPS] = {
     "LDA M", "LDX M", "LDY M", "STA M", "STX M", "STY M", "ADC M", "SBC M",
     "AND M", "ORA M", "EOR M", "CMP M", "CPX M", "CPY M", "INC M", "DEC M",
     "ASL M", "LSR M", "ROL M", "ROR M", "BIT M"};
+
+const char kHex[] = "0123456789ABCDEF";
+
+// Appenders of the JSONL writer: each writes at q and returns the new end.
+char* put_str(char* q, const char* s) {
+    while (*s) *q++ = *s++;
+    return q;
+}
+// The disassembly of a valid instruction, as m6502_disasm prints it.
+char* put_insn(char* q, uint16_t insn) {
+    const uint32_t op = insn & 0xFFu;
+    q = put_str(q, kMnemonic[op]);
+    if (has_imm(op)) {
+        const uint32_t v = insn >> 8;
+        *q++ = ' '; *q++ = '#'; *q++ = '$'; *q++ = kHex[v >> 4]; *q++ = kHex[v & 15];
+    }
+    return q;
+}
+char* put_int(char* q, int v) {
+    unsigned u = v < 0 ? 0u - (unsigned)v : (unsigned)v;
+    if (v < 0) *q++ = '-';
+    char d[10];
+    int k = 0;
+    do { d[k++] = (char)('0' + u % 10); u /= 10; } while (u);
+    while (k) *q++ = d[--k];
+    return q;
+}
 
 std::string trim(const std::string& s) {
     size_t a = 0, b = s.size();
@@ -211,27 +239,49 @@ int m6502_format_jsonl(const uint16_t* target, int tlen, const m6502_rule* rule,
     if (!target || !rule || !buf || cap <= 0 || tlen < 1 || rule->cand_len < 1 || rule->cand_len > 3 ||
         !valid(target, tlen) || !valid(rule->cand, rule->cand_len))
         return M6502_E_INVAL;
-    std::string src, rep;
-    char tmp[32];
+    // Written straight into a local line (an instruction is at most 10
+    // characters, its separator 3), then copied like snprintf: at most cap - 1
+    // characters and a NUL; the return value is the whole line's length.
+    char local[1024];
+    std::unique_ptr<char[]> heap;
+    const size_t need = 256 + 13 * (size_t)(tlen + rule->cand_len);
+    char* line = local;
+    if (need > sizeof local) { heap.reset(new char[need]); line = heap.get(); }
+    char* q = line;
+    int sb = 0, cb = 0, cs = 0;
+    q = put_str(q, "{\"source_asm\":\"");
     for (int i = 0; i < tlen; i++) {
-        m6502_disasm(target[i], tmp, sizeof tmp);
-        if (i) src += " : ";
-        src += tmp;
+        if (i) q = put_str(q, " : ");
+        q = put_insn(q, target[i]);
+        sb += (int)bytes_cuda(target[i] & 0xFF);
+        cs += (int)cycles(target[i] & 0xFF);
     }
+    q = put_str(q, "\",\"replacement_asm\":\"");
     for (int i = 0; i < rule->cand_len; i++) {
-        m6502_disasm(rule->cand[i], tmp, sizeof tmp);
-        if (i) rep += " : ";
-        rep += tmp;
+        if (i) q = put_str(q, " : ");
+        q = put_insn(q, rule->cand[i]);
+        cb += (int)bytes_cuda(rule->cand[i] & 0xFF);
+        cs -= (int)cycles(rule->cand[i] & 0xFF);
     }
-    int sb = m6502_seq_bytes(target, tlen, M6502_SEM_CUDA), cb = m6502_seq_bytes(rule->cand, rule->cand_len, M6502_SEM_CUDA);
-    int cs = m6502_seq_cycles(target, tlen) - m6502_seq_cycles(rule->cand, rule->cand_len);
-    int n = std::snprintf(buf, (size_t)cap,
-                          "{\"source_asm\":\"%s\",\"replacement_asm\":\"%s\",\"source_bytes\":%d,"
-                          "\"replacement_bytes\":%d,\"bytes_saved\":%d,\"cycles_saved\":%d",
-                          src.c_str(), rep.c_str(), sb, cb, sb - cb, cs);
-    if (n >= 0 && n < cap && run_dead_flags)
-        n += std::snprintf(buf + n, (size_t)(cap - n), ",\"dead_flags\":\"0x%02X\"", run_dead_flags);
-    if (n >= 0 && n < cap) n += std::snprintf(buf + n, (size_t)(cap - n), "}");
+    q = put_str(q, "\",\"source_bytes\":");
+    q = put_int(q, sb);
+    q = put_str(q, ",\"replacement_bytes\":");
+    q = put_int(q, cb);
+    q = put_str(q, ",\"bytes_saved\":");
+    q = put_int(q, sb - cb);
+    q = put_str(q, ",\"cycles_saved\":");
+    q = put_int(q, cs);
+    if (run_dead_flags) {
+        q = put_str(q, ",\"dead_flags\":\"0x");
+        *q++ = kHex[run_dead_flags >> 4];
+        *q++ = kHex[run_dead_flags & 15];
+        *q++ = '"';
+    }
+    *q++ = '}';
+    const int n = (int)(q - line);
+    const int k = n < cap ? n : cap - 1;
+    std::memcpy(buf, line, (size_t)k);
+    buf[k] = '\0';
     return n;
 }
 

@@ -164,6 +164,45 @@ def test_format_jsonl_matches_oracle():
                     "replacement_bytes": 2, "bytes_saved": 2, "cycles_saved": 4, "dead_flags": "0xC3"}
 
 
+def test_format_jsonl_random_rules_match_oracle():
+    """3,000 random rules (targets and candidates of 1-3 instructions, cycle
+    savings of either sign, four run masks): the library's JSONL line equals
+    the oracle's restatement of cuda/6502_search_v2.cu:912-930 byte for byte."""
+    from m6502.result import jsonl_line
+    rng = np.random.default_rng(11)
+    tab = oracle.insn_table()
+    for _ in range(3000):
+        t = [int(tab[k]) for k in rng.integers(0, 2863, size=int(rng.integers(1, 4)))]
+        c = [int(tab[k]) for k in rng.integers(0, 2863, size=int(rng.integers(1, 4)))]
+        dead = int(rng.choice([0x00, 0x01, 0xC3, 0xFF]))
+        row = np.zeros(1, dtype=_lib.RULE_DTYPE)[0]
+        row["cand"][:len(c)] = c
+        row["cand_len"] = len(c)
+        assert jsonl_line(t, row, dead) == oracle.format_jsonl(t, (0, tuple(c), 0), dead), (t, c, dead)
+
+
+def test_format_jsonl_long_target_and_short_buffer():
+    """A target longer than the writer's stack line (80 instructions) and a
+    buffer shorter than the line: the return value is the whole line's
+    length and the buffer holds its first cap - 1 characters, like snprintf."""
+    from m6502.inst import Disassemble, SeqByteSize, SeqCycles
+    t = [I.parse_assembly("LDA #$1F")[0], I.parse_assembly("ROL M")[0]] * 40
+    c = [I.parse_assembly("LDX #$0A")[0]]
+    sb, cb = SeqByteSize(t, _lib.SEM_CUDA), SeqByteSize(c, _lib.SEM_CUDA)
+    want = ('{"source_asm":"%s","replacement_asm":"%s","source_bytes":%d,"replacement_bytes":%d,'
+            '"bytes_saved":%d,"cycles_saved":%d,"dead_flags":"0x0C"}'
+            % (" : ".join(Disassemble(x) for x in t), Disassemble(c[0]), sb, cb, sb - cb,
+               SeqCycles(t) - SeqCycles(c)))
+    r = _lib.Rule()
+    r.cand_len, r.cand[0] = 1, c[0]
+    tt = _lib.u16(t)
+    for cap in (4096, 20, 1):
+        buf = ctypes.create_string_buffer(cap)
+        n = _lib.lib().m6502_format_jsonl(_lib.ptr(tt, ctypes.c_uint16), len(t), ctypes.byref(r), 0x0C, buf, cap)
+        assert n == len(want)
+        assert buf.value.decode() == want[:cap - 1]
+
+
 def test_draw_targets_matches_oracle_draw():
     """The library's seeded draw equals the oracle's for fixed lengths (the
     config-1 and length-3 workloads) and keeps lengths in range otherwise."""
