@@ -876,9 +876,10 @@ __global__ void __launch_bounds__(256) k_qc1(const uint64_t* __restrict__ tfp, c
 
 // QC (+ MidCheck) of targets x all length-1 candidates as an exact join:
 // the non-pruned candidates sorted by the hash of their 8 masked QuickCheck
-// outputs (skeys/sidx, built per dead-flags mask) sit in shared memory; a
-// warp takes one target, binary-searches its own key and checks only the
-// candidates with an equal key -- a superset of those QuickCheck passes.
+// outputs (skeys/sidx, built per dead-flags mask) sit in shared memory with
+// a directory of key buckets; a warp takes one target, finds its own key's
+// equal range and checks only those candidates -- a superset of those
+// QuickCheck passes.
 // Lane v checks vector v from the candidate-major fingerprints (cfp_cm,
 // 256 contiguous bytes per candidate).  Same survivors as k_qc1.
 template <bool GO>
