@@ -1,17 +1,18 @@
 // engine.cu -- B200 kernels and the C ABI of libm6502gpu.so.
 //
-// Pipeline of one device pass over a block of targets (all on one stream,
-// one host synchronisation per pass):
+// Pipeline of a search (all on one stream; a CUDA-semantics search with
+// length-1 candidates queues every pass and syncs once at the end):
 //
-//   k_fingerprint   warp per target, lane v runs the target on test vector v:
-//                   32 packed 64-bit output states per target (256 B).
-//   k_qc1           tile of 64 targets x all 2,863 candidates per CTA; the
-//                   candidates' vector-0 outputs stay in registers, the
-//                   targets' in shared memory; one masked 64-bit compare per
-//                   pair rejects almost everything; hits run the byte
-//                   filter, pruner, the other 7 QC vectors and the 24 mid
-//                   vectors, and survivors are appended with one atomic per
-//                   warp (ballot + popc).
+//   k_check_ops     every opcode of the targets, once per search.
+//   k_qc_join       (default) warp per target, lane v runs the target on
+//                   test vector v; the 8 masked QC outputs are hashed and
+//                   looked up in the candidates' sorted key table (shared
+//                   memory, bucket directory); only the equal range is
+//                   checked, on all 32 vectors (QuickCheck + MidCheck).
+//   k_fingerprint + k_qc1  (M6502_QC_SCAN) 32 packed output states per
+//                   target, then a tile of 64 targets x all 2,863
+//                   candidates per CTA with one masked 64-bit compare per
+//                   pair; the same survivors as the join.
 //   k_exhaustive    persistent; a warp takes one surviving pair from a
 //                   device ticket, derives the pair's swept input space
 //                   (reference rule) and the input cone of every output
