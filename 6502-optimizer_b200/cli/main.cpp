@@ -6,7 +6,7 @@
 //                     [--jsonl] [--semantics go|cuda] [--sweep full|reference]
 //                     [--first-op-start A] [--first-op-end B] [--no-exhaust]
 //                     [--gpu-id N] [--checkpoint FILE] [--workers N]
-//   6502opt target "LDA #$00 : TAX" [--max-candidate N] [--dead-flags M] [-v]
+//   6502opt target "LDA #$00 : TAX" [--max-candidate N<=2] [--dead-flags M] [-v]
 //   6502opt verify-jsonl FILE [--dead-flags M] [-v] [--sweep full|reference]
 //   6502opt stoke --target "PHA : TXA : PLA" [--chains N] [--iterations I] [--decay D]
 //                 [--output FILE] [-v] [--dead-flags M] [--cost ref|hamming] [--seed S]
@@ -179,12 +179,23 @@ int cmd_enumerate(const Args& a) {
     if (dead) std::fprintf(info, "  Dead flags: 0x%02X (%s)\n", dead, dead_desc(dead).c_str());
     std::fprintf(info, "\n");
 
-    // Resume watermark: a checkpoint file holds the next first-op index to run.
+    // Resume watermark: a checkpoint file holds "LEN NEXT", the target length
+    // being enumerated and the next first-op index of it to run (every length
+    // below LEN is complete).  The reference's only resume is the manual
+    // --first-op-start (cuda/6502_search_v2.cu:776); its gob checkpoint is
+    // never called (cmd/6502opt/main.go:74).
     std::string ckpt = a.get("--checkpoint", "");
+    int resume_len = 2;
+    uint32_t resume_at = first;
     if (!ckpt.empty()) {
         std::ifstream in(ckpt);
+        int l;
         uint32_t w;
-        if (in >> w && w > first) { first = std::min(w, last); std::fprintf(stderr, "resuming at first-op %u\n", first); }
+        if (in >> l >> w && l >= 2 && l <= max_target + 1) {
+            resume_len = l;
+            resume_at = std::max(first, std::min(w, last));
+            std::fprintf(stderr, "resuming at target length %d, first-op %u\n", resume_len, resume_at);
+        }
     }
     m6502_search_cfg cfg{};
     cfg.semantics = go ? M6502_SEM_GO : M6502_SEM_CUDA;
@@ -196,11 +207,13 @@ int cmd_enumerate(const Args& a) {
     cfg.dead_flags = dead;
     std::vector<OutRule> all;
     uint64_t total_rules = 0;
-    for (int len = 2; len <= max_target; len++) {
+    for (int len = resume_len; len <= max_target; len++) {
         if (verbose) std::fprintf(info, "=== Searching target length %d ===\n", len);
-        // Slices of first-op indices keep host buffers bounded and allow resume.
-        const uint32_t slice = len == 2 ? 2863 : 4;
-        for (uint32_t f = first; f < last; f += slice) {
+        const uint32_t start = len == resume_len ? resume_at : first;
+        // Slices of first-op indices keep host buffers bounded and allow resume:
+        // with --checkpoint the watermark advances every 64 first-ops.
+        const uint32_t slice = len == 2 ? (ckpt.empty() ? 2863u : 64u) : 4u;
+        for (uint32_t f = start; f < last; f += slice) {
             uint32_t f1 = std::min(last, f + slice);
             std::vector<m6502_rule> out(1u << 20);
             uint64_t n = 0;
@@ -243,7 +256,11 @@ int cmd_enumerate(const Args& a) {
                          len, f, f1, (unsigned long long)st.targets, (unsigned long long)st.qc_hits,
                          (unsigned long long)st.mid_hits, (unsigned long long)st.exh_checked,
                          (unsigned long long)n, st.ms_device);
-            if (!ckpt.empty()) { std::ofstream o(ckpt); o << f1 << "\n"; }
+            if (!ckpt.empty()) {   // written after the slice's rules are out
+                std::ofstream o(ckpt);
+                if (f1 < last) o << len << " " << f1 << "\n";
+                else o << len + 1 << " " << first << "\n";
+            }
         }
     }
     if (!jsonl) {
@@ -275,15 +292,21 @@ int cmd_target(const Args& a) {
     if (n > 3) { std::fprintf(stderr, "targets of more than 3 instructions: use `6502opt stoke`\n"); return 1; }
     uint8_t dead = 0;
     if (!parse_dead(a.get("--dead-flags", "none"), &dead)) { std::fprintf(stderr, "invalid --dead-flags\n"); return 1; }
-    long maxc = a.num("--max-candidate", 4);
+    // The Go CLI defaults to 4 (cmd/6502opt/main.go:130); the engine searches
+    // candidates of length 1 and 2, so this command defaults to 2 and refuses
+    // more rather than silently searching less than asked.
+    long maxc = a.num("--max-candidate", 2);
+    if (maxc > 2) {
+        std::fprintf(stderr, "--max-candidate %ld: the GPU engine searches candidates of length 1..2\n", maxc);
+        return 1;
+    }
     std::printf("Target: %s (%d bytes, %d cycles)\n", input.c_str(), m6502_seq_bytes(seq, n, M6502_SEM_GO),
                 m6502_seq_cycles(seq, n));
     m6502_ctx* ctx = open_ctx((int)a.num("--gpu-id", 0));
     m6502_search_cfg cfg{};
     cfg.semantics = M6502_SEM_GO;
     cfg.sweep = M6502_SWEEP_REFERENCE;
-    if (maxc > 2) std::fprintf(stderr, "note: candidates are searched up to length 2 (--max-candidate %ld)\n", maxc);
-    cfg.max_cand_len = (uint32_t)std::max(0L, std::min(maxc, 2L));
+    cfg.max_cand_len = (uint32_t)std::max(0L, maxc);
     cfg.dead_flags = dead;
     m6502_rule out[4];
     uint64_t k = 0;
@@ -329,7 +352,10 @@ int cmd_verify(const Args& a) {
     std::ifstream in(a.pos[0]);
     if (!in) { std::fprintf(stderr, "cannot open %s\n", a.pos[0].c_str()); return 1; }
     m6502_ctx* ctx = open_ctx((int)a.num("--gpu-id", 0));
-    uint64_t total = 0, passed = 0, failed = 0, skipped = 0;
+    // A rule whose sweep would exceed the engine's cone cap (bit 3 of
+    // m6502_check_pairs) was not decided: it is reported as UNDECIDED, not as
+    // a failure, and makes the command exit non-zero like a failure.
+    uint64_t total = 0, passed = 0, failed = 0, skipped = 0, undecided = 0;
     std::vector<uint16_t> ti, ci;
     std::vector<uint32_t> to{0}, co{0};
     std::vector<std::pair<uint64_t, std::string>> names;
@@ -344,6 +370,9 @@ int cmd_verify(const Args& a) {
             if (res[i] & M6502_CHECK_EXH) {
                 passed++;
                 if (verbose) std::printf("  [%llu] PASS: %s\n", (unsigned long long)names[i].first, names[i].second.c_str());
+            } else if (res[i] & 8) {
+                undecided++;
+                std::printf("  [%llu] UNDECIDED: %s\n", (unsigned long long)names[i].first, names[i].second.c_str());
             } else {
                 failed++;
                 std::printf("  [%llu] FAIL: %s\n", (unsigned long long)names[i].first, names[i].second.c_str());
@@ -382,12 +411,19 @@ int cmd_verify(const Args& a) {
         if (names.size() >= (1u << 20)) flush();
     }
     flush();
-    std::printf("\nVerification complete: %llu total, %llu passed, %llu failed, %llu skipped\n",
+    std::printf("\nVerification complete: %llu total, %llu passed, %llu failed, %llu skipped",
                 (unsigned long long)total, (unsigned long long)passed, (unsigned long long)failed,
                 (unsigned long long)skipped);
+    if (undecided) std::printf(", %llu undecided", (unsigned long long)undecided);
+    std::printf("\n");
     m6502_destroy(ctx);
     if (failed) {
         std::fprintf(stderr, "Error: %llu rules failed verification\n", (unsigned long long)failed);
+        return 1;
+    }
+    if (undecided) {
+        std::fprintf(stderr, "Error: %llu rules were not decided (sweep beyond the engine's cap)\n",
+                     (unsigned long long)undecided);
         return 1;
     }
     return 0;

@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUten
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = s_tmem;
 
+    int issued = 0;   // k blocks whose TMA loads the producer issued
     if (warp == 0 && lane == 0) {
         // producer: stage s of round r is free once the MMAs of round r-1 committed on empty[s]
         for (int kb = 0; kb < nk; kb++) {
@@ -153,6 +154,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUten
             mbar_expect_tx(&full[s], (uint32_t)kStageBytes);
             tma_load_2d(sa, &tmA, kb * kBK, m0, &full[s]);
             tma_load_2d(sa + kStageA, &tmB, kb * kBK, n0, &full[s]);
+            issued = kb + 1;
         }
     } else if (warp == 1 && lane == 0) {
         // MMA issuer
@@ -189,6 +191,12 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUten
     asm volatile("tcgen05.fence::after_thread_sync;");
     if (!ok) {
         if (threadIdx.x == 0) atomicExch(err, 1);
+        // Loads the MMA issuer never consumed may still be landing in shared
+        // memory: the producer waits (bounded) for the last phase it armed on
+        // each stage before the CTA releases its memory.
+        if (warp == 0 && lane == 0)
+            for (int kb = max(0, issued - kStages); kb < issued; kb++)
+                mbar_wait(&full[kb % kStages], (uint32_t)((kb / kStages) & 1));
     } else {
         // Epilogue: row = m0 + 32 * warp + lane; 16 columns per tcgen05.ld.
         const int row = m0 + 32 * warp + lane;

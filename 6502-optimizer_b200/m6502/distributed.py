@@ -50,12 +50,15 @@ def reduce_stats(stats, dist, group=None):
 
 
 def gather_rules(rules, dist, group=None, dst=0):
-    """All ranks' (globalized) rules concatenated on rank dst; None elsewhere."""
+    """All ranks' (globalized) rules concatenated on rank dst of the group
+    (a rank within `group`); None elsewhere."""
     world = dist.get_world_size(group)
     if world == 1:
         return rules
     parts = [None] * world if dist.get_rank(group) == dst else None
-    dist.gather_object(np.asarray(rules).tobytes(), parts, dst=dst, group=group)
+    # gather_object takes the destination as a global rank
+    gdst = dist.get_global_rank(group, dst) if group is not None else dst
+    dist.gather_object(np.asarray(rules).tobytes(), parts, dst=gdst, group=group)
     if parts is None:
         return None
     return np.concatenate([np.frombuffer(p, dtype=_lib.RULE_DTYPE) for p in parts]) if parts else rules

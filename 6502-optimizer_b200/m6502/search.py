@@ -6,6 +6,11 @@ target.  All candidate checking runs on the GPU engine; semantics follow the
 Go worker (first passing candidate in Go order, Go byte sizes, QuickCheck then
 ExhaustiveCheck, masked pass with DeadFlags = FlagDiff) unless ``semantics``
 selects the CUDA pipeline's (every passing candidate, MidCheck, CUDA sizes).
+
+Candidates have length 1..MaxCandLen with MaxCandLen at most 2: the engine
+joins targets against all 2,863 length-1 and 8,196,769 length-2 sequences.
+The Go CLI's ``target`` defaults to 4 (cmd/6502opt/main.go:130); asking for
+more than 2 here raises ValueError rather than searching less than asked.
 """
 from dataclasses import dataclass
 
@@ -36,16 +41,27 @@ def _decode_target(tid, tlen, tab):
     return out[::-1]
 
 
+MAX_CAND_LEN = 2
+
+
+def _cand_len(max_cand):
+    if max_cand > MAX_CAND_LEN:
+        raise ValueError(f"MaxCandLen {max_cand}: the engine searches candidates of length 1..{MAX_CAND_LEN}")
+    return max_cand
+
+
 def Run(cfg: Config, engine=None):
-    """search.Run: all target lengths 2..MaxTargetLen; returns sorted rules."""
+    """search.Run: all target lengths 2..MaxTargetLen; returns sorted rules.
+    MaxCandLen 0 means MaxTargetLen - 1 (search.go:26-28); under CUDA
+    semantics only length-1 candidates exist (cuda/6502_search_v2.cu:800-806)."""
+    max_cand = _cand_len(cfg.MaxCandLen or cfg.MaxTargetLen - 1)
+    if cfg.semantics == _lib.SEM_CUDA:
+        max_cand = 1
     eng = engine or default_engine()
-    max_cand = cfg.MaxCandLen or cfg.MaxTargetLen - 1
-    if max_cand != 1:
-        raise NotImplementedError("candidate length > 1 is not supported by this build")
     tab = insn_table(_lib.SEM_CUDA)
     rules = []
     for tlen in range(2, cfg.MaxTargetLen + 1):
-        found, st = eng.enumerate(tlen, cfg.DeadFlags, cfg.semantics, cfg.sweep)
+        found, st = eng.enumerate(tlen, cfg.DeadFlags, cfg.semantics, cfg.sweep, max_cand_len=max_cand)
         if cfg.Verbose:
             print(f"=== target length {tlen}: {st['targets']} targets, {len(found)} rules, "
                   f"{st['ms_device']:.1f} ms ===")
@@ -56,7 +72,7 @@ def Run(cfg: Config, engine=None):
     return sort_rules(rules)
 
 
-def SearchSingle(target, maxCandLen=1, verbose=False, engine=None):
+def SearchSingle(target, maxCandLen=MAX_CAND_LEN, verbose=False, engine=None):
     rules = _single(target, maxCandLen, 0, engine)
     return rules[0] if rules else None
 
@@ -67,12 +83,13 @@ def SearchSingleMasked(target, maxCandLen, deadFlags, verbose=False, engine=None
 
 
 def _single(target, max_cand, dead, engine):
-    eng = engine or default_engine()
+    max_cand = _cand_len(max_cand)
     if max_cand < 1:
         return []
+    eng = engine or default_engine()
     t = np.asarray([target], dtype=np.uint16)
     found, _ = eng.search(t, dead_flags=dead, semantics=_lib.SEM_GO, sweep=_lib.SWEEP_REFERENCE,
-                          max_cand_len=1)
+                          max_cand_len=max_cand)
     rules = [make_rule(list(target), [int(x) for x in r["cand"][:int(r["cand_len"])]], _lib.SEM_GO,
                        int(r["dead_flags"])) for r in found]
     return sort_rules(rules)

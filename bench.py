@@ -88,9 +88,26 @@ class ClockSampler:
         return out
 
 
+def cpu_model():
+    """The host CPU's model name and logical core count (from /proc/cpuinfo)."""
+    name = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    name = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": name, "logical_cores": os.cpu_count() or 1}
+
+
 def cpu_reference_rate(targets, budget_targets, nthreads):
     """The reference's own CPU path (oracle/_ref, else the C restatement) on a
-    strided sample of the workload's targets; returns pair-checks/s."""
+    strided sample of the workload's targets; returns pair-checks/s.  The
+    reference's host pipeline sweeps 32 representative values per register
+    once a pair reads three or more (its cpu_exhaustive_check has no full
+    sweep), so it does at most the work of the engine's full sweep."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     stride = max(1, len(targets) // budget_targets)
@@ -106,7 +123,23 @@ def cpu_reference_rate(targets, budget_targets, nthreads):
     return len(sample) * PAIRS_PER_TARGET / dt, kind, len(sample), stride, dt
 
 
+def oracle_targets(first=0, last=2863):
+    """All pruned length-2 targets, enumerated by the oracle's restatement of
+    the reference's enumeration and ShouldPrune (no engine code involved)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    return oracle.enumerate_targets(2, first, last)
+
+
+REF_SWEEP_NOTE = ("reference: 32 representative values per register for pairs reading >= 3 extra registers "
+                  "(cpu_exhaustive_check, the reference's only CPU sweep); engine: all 256 values")
+
+
 def run_reference(args):
+    """The reference's own host pipeline (oracle/_ref: h_fingerprint,
+    h_midcheck, should_prune, cpu_exhaustive_check built from its sources)
+    on a strided sample of the length-2 workload, all host threads.  Nothing
+    of the engine is loaded: the targets come from the oracle."""
     rank, world, _ = dist_env()
     if world > 1:
         import torch.distributed as dist
@@ -116,27 +149,34 @@ def run_reference(args):
             dist.barrier()
             dist.destroy_process_group()
             return
-    from m6502 import inst
-    targets = inst.enumerate_targets(2)
+    targets = oracle_targets(args.first_op, args.last_op)
     nthreads = os.cpu_count() or 1
     per_step = args.ref_sample
     for _ in range(args.warmup):
         cpu_reference_rate(targets, max(8, per_step // 8), nthreads)
-    rates, secs = [], 0.0
+    rates, secs, kind, stride = [], 0.0, None, 1
     for _ in range(args.steps):
         rate, kind, n, stride, dt = cpu_reference_rate(targets, per_step, nthreads)
         rates.append(rate)
         secs += dt
     value = len(rates) * per_step * PAIRS_PER_TARGET / secs
+    cpu = cpu_model()
+    workload = WORKLOAD if (args.first_op, args.last_op) == (0, 2863) else \
+        f"len2-enumerate-first-ops-{args.first_op}-{args.last_op}"
     line = {"metric": "pair-checks/s", "value": value, "unit": "pair-checks/s", "impl": "reference",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000 * secs / max(len(rates), 1), "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "u8", "data": "synthetic (exhaustive enumeration)",
-            "config": {"workload": WORKLOAD, "targets": int(len(targets)), "candidates": PAIRS_PER_TARGET,
-                       "dead_flags": "0x00", "sweep": "reference (32-value reduced sweep for >=3 extra registers)",
+            "config": {"workload": workload, "targets": int(len(targets)), "candidates": PAIRS_PER_TARGET,
+                       "dead_flags": "0x00", "semantics": "cuda-pipeline",
+                       "sweep": "reference (the only sweep the reference's CPU path has)",
+                       "engine_sweep": "full", "reference_sweep": "reduced for >= 3 extra registers",
+                       "sweep_note": REF_SWEEP_NOTE,
                        "sample": f"every {stride}th target, {per_step} targets per step"},
             "cpu_baseline": {"value": value, "unit": "pair-checks/s", "cores": nthreads, "kind": kind,
-                             "sample": f"{per_step} targets (every {stride}th) x 2863 candidates per step"},
+                             "cpu": cpu["model"],
+                             "sample": f"{per_step} targets (every {stride}th) x 2863 candidates per step, "
+                                       "reduced sweep for >= 3 extra registers"},
             "e2e": {"value": value, "unit": "pair-checks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     if world > 1:
@@ -145,23 +185,25 @@ def run_reference(args):
         dist.destroy_process_group()
 
 
-# Issue-slot utilisation (smsp__issue_active.avg.pct_of_peak_sustained_active)
-# of the committed ncu captures in profiles/ (k_exhaustive_len2.md,
-# k_qc_join_len2.md, k_exh_items_len2.md).
-ISSUE_ACTIVE = {"k_exhaustive": 0.676, "k_qc_join": 0.726, "k_exh_items": 0.204}
-
-
-def load_traffic():
-    """Per-launch DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of
-    each kernel from the committed ncu summary, profiles/traffic.txt."""
+def load_profile_figures():
+    """Per-kernel figures of the committed ncu summary profiles/traffic.txt:
+    DRAM bytes per full-workload launch (dram__bytes_read.sum +
+    dram__bytes_write.sum) and, where captured, the issue-slot utilisation
+    (smsp__issue_active.avg.pct_of_peak_sustained_active) of the same
+    capture.  Lines: `kernel bytes [issue_active]`; `# source:` names the
+    capture."""
     p = os.path.join(ROOT, "profiles", "traffic.txt")
-    out = {}
+    out, source = {}, None
     if os.path.exists(p):
         for line in open(p):
+            if line.startswith("# source:"):
+                source = line.split(":", 1)[1].strip()
+                continue
             parts = line.split()
-            if len(parts) == 2 and parts[1].isdigit():
-                out[parts[0]] = int(parts[1])
-    return out
+            if len(parts) >= 2 and not line.startswith("#") and parts[1].isdigit():
+                out[parts[0]] = {"traffic": int(parts[1]),
+                                 "issue_active": float(parts[2]) if len(parts) > 2 else None}
+    return out, source
 
 
 def run_engine(args):
@@ -264,11 +306,19 @@ def run_engine(args):
                   "emit_ms": avg("ms_emit")}
         dominant = max(("k_exhaustive", avg("ms_exhaustive")), ("k_exh_items", avg("ms_exh_items")),
                        ("k_qc_join", qc_ms), key=lambda kv: kv[1])[0]
-        traffic = load_traffic().get(dominant)
+        figs, figs_source = load_profile_figures()
+        exh_kernels = ("k_exhaustive", "k_exh_items")
         if dominant == "k_qc_join":
             achieved, alg = qc_achieved, "13 ops/pair + 31x13 ops per QC hit (QC+MidCheck)"
+            kernels, ktime = ("k_qc_join",), qc_ms
         else:
-            achieved, alg = exh_achieved, "accepted pairs x 2^(9+8k) states x (10 ops/instruction + 3)"
+            # states the two exhaustive kernels evaluated (cone sweeps, work items and
+            # the 64-state random probes) at the convention's 10 ops per executed
+            # instruction + 3 per compare
+            achieved, alg = exh_exec, ("states evaluated (cone sweeps + items + 64-state probes) x "
+                                       "(10 ops/instruction x 3 instructions + 3)")
+            kernels, ktime = exh_kernels, exh_ms
+        traffic = sum(figs[k]["traffic"] for k in kernels if k in figs) if all(k in figs for k in kernels) else None
         line = {
             "metric": "pair-checks/s", "value": value, "unit": "pair-checks/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
@@ -287,19 +337,25 @@ def run_engine(args):
             "stage_counts": {k: s0[k] for k in ("qc_hits", "mid_hits", "exh_checked", "exh_passed", "rules",
                                                   "exh_states", "exh_items", "exh_probe_rejects")},
             "stages_ms": stages,
-            "roofline": {"bound": "int-issue", "kernel": dominant, "achieved": achieved / 1e12,
+            "roofline": {"bound": "int-issue", "kernel": "+".join(kernels), "achieved": achieved / 1e12,
                          "peak": peak_lane_ops / 1e12, "unit": "Tlane-op/s",
                          "frac": achieved / peak_lane_ops if peak_lane_ops else None,
-                         "traffic": traffic, "traffic_unit": "DRAM bytes per launch (one 2^21-target pass)",
+                         "kernel_ms_per_step": ktime,
+                         "traffic": traffic, "traffic_unit": "DRAM bytes per launch (one 2^21-target pass), "
+                                                             "summed over the kernels named",
                          "algorithmic": alg,
                          "peak_basis": f"{sms} SMs x 128 int32 lanes x {f_mhz:.0f} MHz (median SM clock sampled)",
-                         "note": "exhaustive work is counted as the full product sweep; the cone "
-                                 "decomposition evaluates fewer states, so frac may exceed 1 "
-                                 "(emulation-equivalent)",
-                         # the states the kernels actually evaluated (cone sweeps + 64-state
-                         # probes) at the same 10 ops per instruction + 3 per compare
-                         "executed": exh_exec / 1e12, "executed_frac": exh_exec / peak_lane_ops,
-                         "issue_active_ncu": ISSUE_ACTIVE.get(dominant)},
+                         # the fixed convention: every accepted pair costs its whole product
+                         # sweep; the cone decomposition evaluates far fewer states, so this
+                         # figure exceeds the peak and is not a utilisation
+                         "convention": {"achieved": exh_achieved / 1e12,
+                                        "frac": exh_achieved / peak_lane_ops if peak_lane_ops else None,
+                                        "algorithmic": "accepted pairs x 2^(9+8k) states x "
+                                                       "(10 ops/instruction + 3)",
+                                        "note": "emulation-equivalent, not a utilisation"},
+                         "issue_active_from_profile": {k: figs[k]["issue_active"] for k in kernels
+                                                       if k in figs and figs[k]["issue_active"] is not None},
+                         "profile_source": figs_source},
             "roofline_qc": {"achieved": qc_achieved / 1e12, "unit": "Tlane-op/s",
                             "frac": qc_achieved / peak_lane_ops},
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]},
@@ -313,8 +369,10 @@ def run_engine(args):
         if world == 1 and not args.no_cpu_baseline:
             rate, kind, ns, stride, dt = cpu_reference_rate(all_targets, args.cpu_sample, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": rate, "unit": "pair-checks/s", "cores": os.cpu_count() or 1,
-                                    "kind": kind, "sample": f"{ns} targets (every {stride}th of the workload) "
-                                    f"x 2863 candidates, reference sweep, {dt:.1f} s"}
+                                    "kind": kind, "cpu": cpu_model()["model"],
+                                    "sample": f"{ns} targets (every {stride}th of the workload) "
+                                    f"x 2863 candidates, {dt:.1f} s",
+                                    "sweep": REF_SWEEP_NOTE}
         print(json.dumps(line), flush=True)
     eng.close()
     if dist:

@@ -189,14 +189,16 @@ int m6502_exec_batch(m6502_ctx *ctx, uint64_t n, const uint16_t *insns, const ui
  * as CSR (t_insns/t_offs, c_insns/c_offs, n + 1 offsets each, 1..16
  * instructions per sequence).  out[i] = 1 equivalent, 0 not equivalent, 0xFF
  * invalid pair (length or opcode out of range), 0xFE undecided (an output
- * cone beyond 2^28 states, which one warp cannot sweep in bounded time).  Runs asynchronously on
- * `stream` (a cudaStream_t; NULL = the legacy default stream); read `out`
- * after synchronising it.  Returns M6502_E_TOOBIG for n >
- * M6502_STATIC_MAX_PAIRS.  The first call on a device uploads the instruction
- * tables and looks up the scratch address; make that first call before any
- * stream capture.  Every call shares the one scratch array and leaves it
- * holding its own results, so calls that overlap on the GPU race: issue them
- * on one stream, or wait for one before the next. */
+ * cone beyond 2^28 states, which one warp cannot sweep in bounded time).
+ * Runs asynchronously on `stream` (a cudaStream_t; NULL = the legacy default
+ * stream); read `out` after synchronising it.  Returns M6502_E_TOOBIG for
+ * n > M6502_STATIC_MAX_PAIRS.  The first call on a device uploads the
+ * instruction tables and looks up the scratch address; make that first call
+ * before any stream capture.  That set-up is kept for the life of the
+ * process: a device reset (cudaDeviceReset) after the first call is not
+ * supported.  Every call shares the one scratch array and leaves it holding
+ * its own results, so calls that overlap on the GPU race: issue them on one
+ * stream, or wait for one before the next. */
 #define M6502_STATIC_MAX_PAIRS (1u << 20)
 int m6502_exhaustive_static(uint64_t n, const uint16_t *t_insns, const uint32_t *t_offs,
                             const uint16_t *c_insns, const uint32_t *c_offs, uint8_t dead_flags,

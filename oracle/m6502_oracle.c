@@ -544,15 +544,19 @@ static void set_reg(or_state *s, int off, uint8_t v) {
  * {A, P = carry, S = 0xFD}, the rest 0; every extra register read by either
  * sequence is swept over 256 values when at most 2 are read, else over the
  * 32 representative values (sweep = reference) or over 256 values
- * (sweep = full, the GPU engine's extension). */
-int or_exhaustive(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead, int sweep) {
+ * (sweep = full, the GPU engine's extension).  This helper sweeps the A
+ * values [a0, a1) and gives up early once *stop is set (another thread of
+ * or_exhaustive_mt found a differing state). */
+static int exhaustive_range(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead,
+                            int sweep, int a0, int a1, volatile int *stop) {
     int extra[6];
     int k = or_swept_regs(t, tn, c, cn, extra);
     int use_rep = (k >= 3 && sweep == OR_SWEEP_REFERENCE);
     int width = use_rep ? 32 : 256;
     uint64_t inner = 1;
     for (int i = 0; i < k; i++) inner *= (uint64_t)width;
-    for (int a = 0; a < 256; a++) {
+    for (int a = a0; a < a1; a++) {
+        if (stop && *stop) return 1;
         for (int carry = 0; carry <= 1; carry++) {
             for (uint64_t idx = 0; idx < inner; idx++) {
                 or_state s;
@@ -572,6 +576,52 @@ int or_exhaustive(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t 
         }
     }
     return 1;
+}
+
+int or_exhaustive(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead, int sweep) {
+    return exhaustive_range(t, tn, c, cn, dead, sweep, 0, 256, NULL);
+}
+
+typedef struct exh_part {
+    const uint16_t *t, *c;
+    int tn, cn, sweep, a0, a1, ok;
+    uint8_t dead;
+    volatile int *stop;
+} exh_part;
+
+static void *exh_part_main(void *arg) {
+    exh_part *p = (exh_part *)arg;
+    p->ok = exhaustive_range(p->t, p->tn, p->c, p->cn, p->dead, p->sweep, p->a0, p->a1, p->stop);
+    if (!p->ok) *p->stop = 1;
+    return NULL;
+}
+
+/* or_exhaustive with the 256 values of A dealt to nthreads threads (A value
+ * a to thread a mod nthreads, so every thread gets the same mix); the same
+ * states, the same verdict.  Lets tests decide full sweeps of 2^33 states. */
+int or_exhaustive_mt(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead, int sweep,
+                     int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    exh_part parts[256];
+    pthread_t th[256];
+    volatile int stop = 0;
+    /* Each thread sweeps runs of one A value: thread i takes a = i, i + n, ... */
+    int ok = 1;
+    for (int base = 0; base < 256 && ok; base += nthreads) {
+        int m = (256 - base) < nthreads ? (256 - base) : nthreads;
+        for (int i = 0; i < m; i++) {
+            exh_part *p = &parts[i];
+            p->t = t; p->c = c; p->tn = tn; p->cn = cn; p->sweep = sweep; p->dead = dead;
+            p->a0 = base + i; p->a1 = base + i + 1; p->stop = &stop; p->ok = 1;
+            pthread_create(&th[i], NULL, exh_part_main, p);
+        }
+        for (int i = 0; i < m; i++) {
+            pthread_join(th[i], NULL);
+            if (!parts[i].ok) ok = 0;
+        }
+    }
+    return ok;
 }
 
 /* A state of the full-sweep domain of (t, c) on which the two differ,

@@ -68,6 +68,9 @@ void or_fingerprint(const uint16_t *seq, int n, uint8_t out[64]);
 int  or_quickcheck(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead);
 int  or_midcheck(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead);
 int  or_exhaustive(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead, int sweep);
+/* The same sweep with the A values spread over nthreads threads. */
+int  or_exhaustive_mt(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead, int sweep,
+                      int nthreads);
 uint8_t or_flagdiff(const uint16_t *t, int tn, const uint16_t *c, int cn);
 int  or_swept_regs(const uint16_t *t, int tn, const uint16_t *c, int cn, int *extra);
 int  or_full_sweep_witness(const uint16_t *t, int tn, const uint16_t *c, int cn, uint8_t dead,

@@ -108,6 +108,11 @@ def exhaustive(t, c, dead=0, sweep=SWEEP_REFERENCE):
     return bool(_pair(lib().or_exhaustive, t, c, ctypes.c_uint8(dead), sweep))
 
 
+def exhaustive_mt(t, c, dead=0, sweep=SWEEP_REFERENCE, nthreads=None):
+    """exhaustive() with the sweep's A values spread over all host threads."""
+    return bool(_pair(lib().or_exhaustive_mt, t, c, ctypes.c_uint8(dead), sweep, nthreads or os.cpu_count() or 1))
+
+
 def flagdiff(t, c):
     return int(_pair(lib().or_flagdiff, t, c))
 

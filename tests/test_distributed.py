@@ -87,3 +87,32 @@ def test_reduce_stats_single_process():
             return 1
     st = reduce_stats({"targets": 3, "ms_qc": 2.5}, One())
     assert st["targets"] == 3 and st["ms_qc"] == 2.5 and st["rules"] == 0
+
+
+def _subgroup_main(rank, world, port, out_path):
+    """Ranks 1 and 2 form a group without global rank 0; the group's rank 0
+    (global rank 1) must receive both ranks' rules."""
+    import datetime
+    import torch.distributed as dist
+    from m6502.distributed import gather_rules
+    os.environ["MASTER_ADDR"], os.environ["MASTER_PORT"] = "127.0.0.1", str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        group = dist.new_group([1, 2])
+        if rank in (1, 2):
+            r = np.zeros(2, dtype=_lib.RULE_DTYPE)
+            r["target"] = [10 * rank, 10 * rank + 1]
+            got = gather_rules(r, dist, group=group, dst=0)
+            if rank == 1:
+                np.save(out_path, got)
+            else:
+                assert got is None
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gather_to_a_subgroup_rank(tmp_path):
+    out = str(tmp_path / "sub.npy")
+    mp.start_processes(_subgroup_main, args=(3, _free_port(), out), nprocs=3, join=True, start_method="spawn")
+    assert sorted(np.load(out)["target"].tolist()) == [10, 11, 20, 21]

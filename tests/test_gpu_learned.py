@@ -7,7 +7,8 @@ stopped on validation targets, and evaluated on held-out targets: (1) the
 moves a higher log-likelihood than the uniform proposal; (2) STOKE with the
 mixed proposal is run beside uniform STOKE on the same held-out targets and
 seeds, and every rewrite either finds passes the CPU oracle's QuickCheck and
-MidCheck (ExhaustiveCheck is the GPU's, pinned elsewhere).
+MidCheck, and the oracle's ExhaustiveCheck where its domain has at most
+2^25 states.
 """
 import numpy as np
 import pytest
@@ -17,6 +18,15 @@ from m6502 import _lib, inst as I
 from m6502.proposal import collect_trajectories, move_log_likelihood, train_proposal
 
 pytestmark = pytest.mark.gpu
+
+
+def _domain_bits(t, c):
+    """log2 of the reduced-sweep domain of (t, c) (the sweep these runs use)."""
+    reads = 0
+    for x in list(t) + list(c):
+        reads |= int(oracle.lib().or_op_reads(x & 0xFF))
+    k = bin(reads & 0xFC).count("1")
+    return 9 + k * (5 if k >= 3 else 8)
 
 
 def test_learned_proposal_gains_over_uniform(engine):
@@ -44,7 +54,12 @@ def test_learned_proposal_gains_over_uniform(engine):
         print(f"{name}: proved {len(st)} of {len(held)}; median steps {np.median(st) if st else None}, "
               f"median ms {np.median(ms) if ms else None}")
     for proofs, name in ((proofs_u, "uniform"), (proofs_l, "learned")):
+        seen = set()
         for p in proofs[:200]:
             t, c = held[p["target"]], p["cand"]
             assert oracle.quickcheck(t, c) and oracle.midcheck(t, c), name
+            key = (p["target"], tuple(c))
+            if key not in seen and _domain_bits(t, c) <= 25:
+                seen.add(key)
+                assert oracle.exhaustive_mt(t, c, 0, oracle.SWEEP_REFERENCE), (name, t, c)
     mlp.close()

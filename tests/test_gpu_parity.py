@@ -65,9 +65,19 @@ def test_pair_verdicts_golden(engine, exh_mode):
             assert bool(o & 4) == p["exh"], (p, exh_mode)
 
 
-def test_pairs_random_vs_oracle(engine):
+def _extra_regs(seq):
+    r = 0
+    for x in seq:
+        r |= int(oracle.lib().or_op_reads(int(x) & 0xFF))
+    return bin(r & 0xFC).count("1")
+
+
+@pytest.mark.parametrize("sweep", [_lib.SWEEP_REFERENCE, _lib.SWEEP_FULL])
+def test_pairs_random_vs_oracle(engine, sweep):
     """Random pairs (target 1..4, candidate 1..3 instructions): QC, MidCheck,
-    FlagDiff on all; ExhaustiveCheck on those passing QC (reference sweep)."""
+    FlagDiff on all; ExhaustiveCheck on those passing QC, in the reduced
+    (reference) and the full sweep.  Full-sweep pairs reading three extra
+    registers have 2^33 states; the oracle sweeps them on all host threads."""
     rng = np.random.default_rng(5)
     tab = oracle.insn_table()
     ts, cs = [], []
@@ -83,6 +93,7 @@ def test_pairs_random_vs_oracle(engine):
             c = [int(tab[k]) for k in rng.integers(0, 2863, size=int(rng.integers(1, 4)))]
         ts.append(t)
         cs.append(c)
+    n_k3 = 0
     for dead in (0x00, 0x01, 0xC3, 0xFF):
         out, fd = engine.check_pairs(ts, cs, dead, _lib.CHECK_QC | _lib.CHECK_MID, flagdiff=True)
         exh_idx = []
@@ -94,9 +105,18 @@ def test_pairs_random_vs_oracle(engine):
             if out[i] & 1:
                 exh_idx.append(i)
         sub_t, sub_c = [ts[i] for i in exh_idx], [cs[i] for i in exh_idx]
-        ex = engine.check_pairs(sub_t, sub_c, dead, _lib.CHECK_EXH, _lib.SWEEP_REFERENCE)
+        ex = engine.check_pairs(sub_t, sub_c, dead, _lib.CHECK_EXH, sweep)
+        assert not np.any(ex & 8)   # every pair decided
         for t, c, o in zip(sub_t, sub_c, ex):
-            assert bool(o & 4) == oracle.exhaustive(t, c, dead, oracle.SWEEP_REFERENCE), (t, c, dead)
+            k = _extra_regs(t + c)
+            if sweep == _lib.SWEEP_FULL and k >= 3:
+                n_k3 += 1
+                want = oracle.exhaustive_mt(t, c, dead, oracle.SWEEP_FULL)
+            else:
+                want = oracle.exhaustive(t, c, dead, sweep)
+            assert bool(o & 4) == want, (t, c, dead, sweep)
+    if sweep == _lib.SWEEP_FULL:
+        assert n_k3 > 0   # the set holds pairs whose full and reduced sweeps differ in size
 
 
 @pytest.mark.parametrize("mask", ["0x00", "0x01", "0xC3", "0xFF"])
@@ -119,6 +139,24 @@ def test_config1_cuda_semantics(engine, mask):
             assert st[k] == run["counts"][k], k
         lines = sorted(m6502.result.jsonl_line(targets[int(r["target"])], r, dead) for r in rules)
         assert lines == run["jsonl"]
+
+
+@pytest.mark.parametrize("mask", ["0x00", "0x01", "0xC3", "0xFF"])
+def test_config1_full_sweep_vs_oracle(engine, mask):
+    """The config-1 targets under the full sweep (all 256 values of every
+    swept register), cones and brute force, against the oracle's full sweep."""
+    cfg = READ("config1.json")
+    run = cfg["runs"][mask]
+    targets = np.array(cfg["targets"], dtype=np.uint16)[run["target_index"]]
+    dead = int(mask, 16)
+    want, wst = oracle.search_cuda(targets, dead=dead, sweep=oracle.SWEEP_FULL)
+    for exh_mode in (_lib.EXH_CONES, _lib.EXH_BRUTE):
+        rules, st = engine.search(targets, dead_flags=dead, semantics=_lib.SEM_CUDA,
+                                  sweep=_lib.SWEEP_FULL, exh_mode=exh_mode)
+        got = sorted((int(r["target"]), (int(r["cand"][0]),), int(r["dead_flags"])) for r in rules)
+        assert got == sorted(want)
+        for k in ("pairs", "qc_hits", "mid_hits", "exh_checked"):
+            assert st[k] == wst[k], k
 
 
 @pytest.mark.parametrize("dead,n", [(0x00, 256), (0x01, 256), (0xFF, 16)])

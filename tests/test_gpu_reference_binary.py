@@ -44,3 +44,28 @@ def test_rules_equal_reference_cuda_binary(engine, dead):
         ours.append(json.dumps(json.loads(jsonl_line(target, r, dead)), sort_keys=True))
     assert len(ref) > 0
     assert sorted(ours) == ref
+
+
+REF_FULL = os.path.join(ROOT, "tests", "golden", "ref_len2_0x00.json")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_FULL), reason="fixture not generated (tests/golden/make_ref_len2.py)")
+def test_full_enumeration_equals_reference_cuda_binary(engine):
+    """The whole length-2 enumeration at dead-flags 0x00 (reduced sweep):
+    the engine's JSONL rule set hashes to the one the unmodified reference
+    binary produced over all 2,863 first instructions, and the stage counts
+    are the binary's."""
+    import hashlib
+    want = json.load(open(REF_FULL))
+    rules, st = engine.enumerate(2, dead_flags=0, semantics=_lib.SEM_CUDA, sweep=_lib.SWEEP_REFERENCE)
+    tab = I.insn_table(_lib.SEM_CUDA)
+    lines = []
+    for r in rules:
+        tid = int(r["target"])
+        lines.append(json.dumps(json.loads(jsonl_line([int(tab[tid // 2863]), int(tab[tid % 2863])], r, 0)),
+                                sort_keys=True))
+    lines.sort()
+    assert len(lines) == want["rules"]
+    assert hashlib.sha256("\n".join(lines).encode()).hexdigest() == want["rules_sha256"]
+    for k in ("targets", "qc_hits", "mid_hits", "exh_checked"):
+        assert st[k] == want["counts"][k], k

@@ -27,6 +27,16 @@ def _oracle_sweep_ok(t, c):
     return bin(reads & 0xFC).count("1") <= 4
 
 
+def _domain_bits(t, c, sweep):
+    """log2 of the states ExhaustiveCheck sweeps for (t, c): A, carry and 8
+    bits per extra register read (5 under the reduced sweep from three on)."""
+    reads = 0
+    for x in list(t) + list(c):
+        reads |= int(oracle.lib().or_op_reads(x & 0xFF))
+    k = bin(reads & 0xFC).count("1")
+    return 9 + k * (5 if (sweep == oracle.SWEEP_REFERENCE and k >= 3) else 8)
+
+
 def _distinct(proofs):
     """(target, candidate) of every distinct proof, in first-found order."""
     seen = {}
@@ -88,6 +98,31 @@ def test_stoke_stop_on_proof_and_random_targets(engine):
             assert oracle.exhaustive(t, c, 0, oracle.SWEEP_REFERENCE)
             checked += 1
     assert checked >= min(len(proofs), 1) or not proofs
+
+
+def test_stoke_full_sweep_proofs_reprove_on_oracle(engine):
+    """The STOKE benchmark proves at the full sweep: seeded random targets of
+    length 4..8, Hamming cost, stop_on_proof, full sweep.  Every distinct
+    proof re-passes the oracle's QuickCheck and MidCheck, and its full-sweep
+    ExhaustiveCheck (every state of the domain, on all host threads) where
+    the domain has at most 2^30 states, plus the first two larger ones (2^33)."""
+    rng = np.random.default_rng(2)
+    tab = oracle.insn_table()
+    targets = [[int(tab[k]) for k in rng.integers(0, 2863, size=int(rng.integers(4, 9)))] for _ in range(24)]
+    res, proofs, st = engine.stoke(targets, chains_per_target=16, steps=30000, steps_per_epoch=1000, seed=11,
+                                   cost=_lib.COST_HAMMING, stop_on_proof=True, sweep=_lib.SWEEP_FULL)
+    assert proofs
+    checked, large = 0, 0
+    for i, c in _distinct(proofs):
+        t = targets[i]
+        assert _go_bytes(c) < _go_bytes(t)
+        assert oracle.quickcheck(t, c) and oracle.midcheck(t, c), (t, c)
+        bits = _domain_bits(t, c, oracle.SWEEP_FULL)
+        if bits <= 30 or (bits <= 33 and large < 2):
+            large += bits > 30
+            assert oracle.exhaustive_mt(t, c, 0, oracle.SWEEP_FULL), (t, c)
+            checked += 1
+    assert checked >= 1
 
 
 def test_stoke_dedupe_deterministic(engine):
