@@ -28,9 +28,14 @@
 #include <cub/block/block_scan.cuh>
 #include <cub/device/device_radix_sort.cuh>
 
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -197,12 +202,16 @@ struct Surv {
     uint32_t c;
 };
 constexpr uint32_t kSurvLen2 = 1u << 23, kSurvMasked = 1u << 24;
+// The join already ran the random-state probe on this pair and found no
+// difference (k_exhaustive skips its own probe).
+constexpr uint32_t kSurvProbed = 1u << 31;
 __host__ __device__ __forceinline__ uint32_t fd_pack(uint32_t fd) { return (fd & 0x0Fu) | ((fd >> 2) & 0x30u); }
 
 struct Counters {
     unsigned long long qc, mid, surv, exh_ticket, items, item_ticket, rules, exh_pass, states, algo, probe_rejects;
     unsigned long long round_n, max_ord;   // Go-order verification rounds
     unsigned long long join_items;         // chunks of long length-2 equal ranges
+    unsigned long long join_probe_rej;     // MidCheck survivors the join's probe rejected
 };
 
 struct Item {   // one chunk of a large cone sweep
@@ -245,6 +254,7 @@ struct SurvSource {
         }
         dead = go ? ((s.c & kSurvMasked) ? run_dead : 0u) : run_dead;
     }
+    __device__ bool probed(uint64_t p) const { return (surv[p].c & kSurvProbed) != 0; }
 };
 
 struct CsrSource {
@@ -262,6 +272,7 @@ struct CsrSource {
         if (lane < cn) sc[lane] = c_ins[c0 + lane];
         dead = dead_;
     }
+    __device__ bool probed(uint64_t) const { return false; }
 };
 
 // Decode parameters of one cone sweep.  State index bits: A (8, if in the
@@ -388,6 +399,15 @@ __device__ __forceinline__ St probe_state(uint32_t swept, bool rep, uint64_t z) 
     return in;
 }
 
+// The i-th random word of a probe with the given salt (splitmix64 output
+// mixing of salt + i * golden ratio).
+__device__ __forceinline__ uint64_t probe_z(uint64_t salt, int i) {
+    uint64_t z = salt + (uint64_t)i * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
 // Probe: 64 pseudo-random states of the pair's whole sweep domain (A and
 // carry always swept), all outputs compared.  A mismatch anywhere in the
 // domain decides the pair (not equivalent) without the cone analysis;
@@ -396,10 +416,7 @@ __device__ __forceinline__ bool probe_domain(const PairView& pv, uint32_t swept,
                                              uint64_t salt, int lane) {
     const OutMask m = out_mask(cmp_mask(dead));
     for (int it = 0; it < 2; it++) {   // 32 states at a time: most failing pairs fail in the first
-        uint64_t z = salt + (uint64_t)(lane + 32 * it) * 0x9E3779B97F4A7C15ull;
-        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-        z ^= z >> 31;
+        const uint64_t z = probe_z(salt, lane + 32 * it);
         if (__any_sync(kFull, state_diff_in(pv, m, probe_state(swept, rep, z)) != 0)) return false;
     }
     return true;
@@ -677,6 +694,8 @@ struct ExhArgs {
     uint32_t sweep;              // M6502_SWEEP_*
     uint32_t brute;
     uint32_t defer_bits;         // > 0: pairs with a cone above 2^defer_bits states get fail = 4 (deferred)
+    uint32_t ticket_batch;       // pairs a warp claims per ticket atomic (0 = kTicketBatch)
+    uint32_t chunk_log2;         // states per work item, at least (0 = kChunk)
 };
 
 // ---------------------------------------------------------------------------
@@ -884,13 +903,14 @@ __global__ void __launch_bounds__(256) k_qc1(const uint64_t* __restrict__ tfp, c
 // Lane v checks vector v from the candidate-major fingerprints (cfp_cm,
 // 256 contiguous bytes per candidate).  Same survivors as k_qc1.
 template <bool GO>
-__global__ void __launch_bounds__(256) k_qc_join(const uint16_t* __restrict__ targets, uint32_t tlen,
+__global__ void __launch_bounds__(256, 4) k_qc_join(const uint16_t* __restrict__ targets, uint32_t tlen,
                                                   uint32_t nt, const uint64_t* __restrict__ cfp_cm,
                                                   const uint8_t* __restrict__ cmeta, const uint64_t* __restrict__ skeys,
                                                   const uint16_t* __restrict__ sidx, uint32_t nsorted, uint32_t dead,
                                                   uint32_t stages, Surv* __restrict__ surv, uint64_t cap,
-                                                  Counters* __restrict__ cnt) {
+                                                  Counters* __restrict__ cnt, uint32_t probe) {
     __shared__ uint64_t s_key[kNumInsns];
+    __shared__ uint64_t s_tprobe[kWarpsPerBlock][2][32];   // target outputs on the probe states
     __shared__ uint16_t s_idx[kNumInsns];
     __shared__ uint8_t s_meta[kNumInsns];
     __shared__ uint16_t s_dir[(1u << kDirBits) + 1];
@@ -915,7 +935,7 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint16_t* __restrict__ ta
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t loose = cmp_mask(dead), exact = cmp_mask(0);
     const uint64_t vin = c_vec[lane];   // lane v's test vector, read once
-    unsigned long long nqc = 0, nmid = 0;
+    unsigned long long nqc = 0, nmid = 0, nprobe_rej = 0;
     const uint32_t stride = gridDim.x * kWarpsPerBlock;
     uint32_t t = blockIdx.x * kWarpsPerBlock + w;
     // Lane i holds instruction i of the warp's target (tlen <= 32); the next
@@ -951,6 +971,19 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint16_t* __restrict__ ta
             while (end < bhi && s_key[end] == key) end++;
         }
         if (lo == end) continue;
+        // Random-state probe of the MidCheck survivors (CUDA semantics, before
+        // ExhaustiveCheck; `probe` = 1 + the sweep mode, 0 = off).  Lane l
+        // takes domain states l and l + 32 drawn from this target's salt.  The
+        // target's outputs on them are computed once, on the first survivor,
+        // over the target's own domain (A, carry and the registers it reads)
+        // and reused by every candidate that reads no other register; a
+        // candidate that widens the domain runs the target again on the wider
+        // states.  A difference rejects the pair, as ExhaustiveCheck would
+        // (the states lie in its domain); under the reduced sweep, pairs
+        // reading three or more extra registers are left to k_exhaustive.
+        bool tp_ready = false;
+        uint32_t tp_sw = 0;
+        const uint64_t salt = (uint64_t)t * 0xD1B54A32D192ED03ull + 0x632BE59BD9B4E019ull;
         for (uint32_t i0 = lo; i0 < end; i0 += kJoinBatch) {
             // The rows of up to kJoinBatch candidates are loaded before any is
             // used, so their latencies overlap.
@@ -983,6 +1016,39 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint16_t* __restrict__ ta
                     nqc += lane == 0;
                     const bool mid = !(stages & M6502_CHECK_MID) || lo_eq == kFull;
                     if (mid) { nmid += lane == 0; pass = true; }
+                    if (pass && probe) {
+                        if (!tp_ready) {
+                            tp_sw = __reduce_or_sync(kFull, lane < (int)tlen ? (uint32_t)c_sweep[ins & 0xFFu] : 0u);
+                            for (int r = 0; r < 2; r++) {
+                                St ts = probe_state(tp_sw | LB(L_A) | LB(L_C), false, probe_z(salt, lane + 32 * r));
+                                for (uint32_t i = 0; i < tlen; i++) exec(ts, __shfl_sync(kFull, ins, (int)i));
+                                s_tprobe[w][r][lane] = pack(ts);
+                            }
+                            tp_ready = true;
+                        }
+                        const uint32_t cins = c_tab[c];
+                        const uint32_t swc = c_sweep[cins & 0xFFu], swu = tp_sw | swc;
+                        if (probe != 1u + M6502_SWEEP_REFERENCE || __popc(swu) < 3) {
+                            const bool same = (swc & ~tp_sw) == 0;   // uniform
+                            const uint64_t m = cmp_mask(dead);
+                            bool differ = false;
+                            for (int r = 0; r < 2 && !differ; r++) {
+                                const St in = probe_state(swu | LB(L_A) | LB(L_C), false, probe_z(salt, lane + 32 * r));
+                                uint64_t tout = s_tprobe[w][r][lane];
+                                St ps = in;
+                                // one exec site: the target (when the domain widened), then the candidate
+                                for (int i = same ? (int)tlen : 0; i <= (int)tlen; i++) {
+                                    uint32_t insn = cins;
+                                    if (i < (int)tlen) insn = __shfl_sync(kFull, ins, i);
+                                    else { if (!same) tout = pack(ps); ps = in; }
+                                    exec(ps, insn);
+                                }
+                                differ = __any_sync(kFull, ((tout ^ pack(ps)) & m) != 0);
+                            }
+                            if (differ) { pass = false; nprobe_rej += lane == 0; }
+                            else code |= kSurvProbed;
+                        }
+                    }
                 } else if ((ex_eq & 0xFFu) == 0xFFu) {           // processTask: unmasked QC passes
                     nqc += lane == 0; nmid += lane == 0; pass = true;
                 } else if (dead) {                               // processTaskMasked, FlagDiff != 0
@@ -1001,10 +1067,12 @@ __global__ void __launch_bounds__(256) k_qc_join(const uint16_t* __restrict__ ta
     for (int o = 16; o; o >>= 1) {
         nqc += __shfl_down_sync(kFull, nqc, o);
         nmid += __shfl_down_sync(kFull, nmid, o);
+        nprobe_rej += __shfl_down_sync(kFull, nprobe_rej, o);
     }
     if (lane == 0) {
         if (nqc) atomicAdd(&cnt->qc, nqc);
         if (nmid) atomicAdd(&cnt->mid, nmid);
+        if (nprobe_rej) atomicAdd(&cnt->join_probe_rej, nprobe_rej);
     }
 }
 
@@ -1199,9 +1267,11 @@ __global__ void __launch_bounds__(256) k_qc_join2_items(Join2Args a) {
 }
 
 // Exhaustive check, one pair per warp (persistent, device ticket).
-template <class Src>
-__global__ void __launch_bounds__(256, 4) k_exhaustive(Src src, const unsigned long long* n_pairs_ptr,
-                                                     uint64_t n_cap, ExhArgs a) {
+// MINB: resident 256-thread blocks per SM the register cap is set for (4:
+// 64 registers, 3: 80, 2: 128); the autotuner picks the variant.
+template <class Src, int MINB = 4>
+__global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigned long long* n_pairs_ptr,
+                                                        uint64_t n_cap, ExhArgs a) {
     __shared__ uint16_t s_t[kWarpsPerBlock][kMaxSeq], s_c[kWarpsPerBlock][kMaxSeq];
     __shared__ uint16_t s_dep[NUM_OPS][NUM_LOCS];
     for (int i = threadIdx.x; i < NUM_OPS * NUM_LOCS; i += blockDim.x) (&s_dep[0][0])[i] = (&c_dep[0][0])[i];
@@ -1210,15 +1280,17 @@ __global__ void __launch_bounds__(256, 4) k_exhaustive(Src src, const unsigned l
     const uint64_t n = min((uint64_t)*n_pairs_ptr, n_cap);
     unsigned long long nstates = 0, probe_rej = 0;
     unsigned long long next = 0, lim = 0;   // this warp's batch of tickets
+    const unsigned long long tbatch = a.ticket_batch ? a.ticket_batch : kTicketBatch;
+    const uint64_t chunk_min = a.chunk_log2 ? (1ull << a.chunk_log2) : kChunk;
     // Lane 0 claims the following batch while the warp works on the current
     // one, so the atomic's latency is hidden behind a batch of pairs.
     unsigned long long ahead = 0;
-    if (lane == 0) ahead = atomicAdd(&a.cnt->exh_ticket, (unsigned long long)kTicketBatch);
+    if (lane == 0) ahead = atomicAdd(&a.cnt->exh_ticket, tbatch);
     for (;;) {
         if (next >= lim) {
             next = __shfl_sync(kFull, ahead, 0);
-            lim = next + kTicketBatch;
-            if (lane == 0 && next < n) ahead = atomicAdd(&a.cnt->exh_ticket, (unsigned long long)kTicketBatch);
+            lim = next + tbatch;
+            if (lane == 0 && next < n) ahead = atomicAdd(&a.cnt->exh_ticket, tbatch);
         }
         const unsigned long long p = next++;
         if (p >= n) break;
@@ -1226,7 +1298,7 @@ __global__ void __launch_bounds__(256, 4) k_exhaustive(Src src, const unsigned l
         pv.t = s_t[w]; pv.c = s_c[w];
         src.load(p, s_t[w], s_c[w], pv.tn, pv.cn, pv.dead, lane);
         __syncwarp();
-        {
+        if (!src.probed(p)) {
             uint32_t sw = 0;
             for (int i = 0; i < pv.tn; i++) sw |= c_sweep[pv.t[i] & 0xFFu];
             for (int i = 0; i < pv.cn; i++) sw |= c_sweep[pv.c[i] & 0xFFu];
@@ -1279,7 +1351,7 @@ __global__ void __launch_bounds__(256, 4) k_exhaustive(Src src, const unsigned l
                 else next_group(lg, rem, lane, o, bits, cone, mask);
                 rem &= ~(1u << o);
                 const uint64_t total = 1ull << bits;
-                const uint64_t chunk = max(kChunk, (total + kMaxItemsPerCone - 1) / kMaxItemsPerCone);
+                const uint64_t chunk = max(chunk_min, (total + kMaxItemsPerCone - 1) / kMaxItemsPerCone);
                 const uint64_t nitems = (total - kProbe + chunk - 1) / chunk;
                 unsigned long long base = 0;
                 if (lane == 0) base = atomicAdd(&a.cnt->items, (unsigned long long)nitems);
@@ -1716,6 +1788,8 @@ struct m6502_ctx {
     std::mutex mu;
     int sms = 148;
     int exh_blocks = 0, exh_item_blocks = 0, qc_blocks = 0, fp_blocks = 0;
+    int exh_occ[5] = {};       // resident blocks per SM of k_exhaustive<SurvSource, MINB>, by MINB
+    m6502_tune tune{4, 4, 11, 1, {0, 0, 0, 0}};   // scheduling knobs (m6502_tune_set / m6502_autotune)
     uint64_t pass_targets = 1ull << 21;
     bool ready = false;
     DevBuf cfp1, cmeta1, targets, ids, tfp, tmeta, surv, fail, items, rules, cnt, best, pins, poffs,
@@ -1780,6 +1854,34 @@ int ensure(m6502_ctx* ctx, DevBuf& b, size_t bytes) {
         if (rc_ != M6502_OK) return rc_; \
     } while (0)
 
+// The exhaustive kernel over survivors with the context's knobs: ticket
+// batch and work-item size in the arguments, the register-cap variant and
+// its persistent grid (SMs x resident blocks).
+int launch_exh(m6502_ctx* ctx, const SurvSource& src, const unsigned long long* n_ptr, uint64_t cap, ExhArgs ea) {
+    ea.ticket_batch = ctx->tune.ticket_batch;
+    ea.chunk_log2 = ctx->tune.chunk_log2;
+    const int minb = (int)ctx->tune.exh_minb;
+    const unsigned grid = (unsigned)(ctx->sms * ctx->exh_occ[minb >= 2 && minb <= 4 ? minb : 4]);
+    if (minb == 2)
+        k_exhaustive<SurvSource, 2><<<grid, 256, 0, ctx->stream>>>(src, n_ptr, cap, ea);
+    else if (minb == 3)
+        k_exhaustive<SurvSource, 3><<<grid, 256, 0, ctx->stream>>>(src, n_ptr, cap, ea);
+    else
+        k_exhaustive<SurvSource, 4><<<grid, 256, 0, ctx->stream>>>(src, n_ptr, cap, ea);
+    CKL("k_exhaustive");
+    return M6502_OK;
+}
+
+// Items of survivor pairs, with the work-item size of the knobs (the items
+// were cut by launch_exh with the same size).
+int launch_items(m6502_ctx* ctx, const SurvSource& src, ExhArgs ea) {
+    ea.ticket_batch = ctx->tune.ticket_batch;
+    ea.chunk_log2 = ctx->tune.chunk_log2;
+    k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
+    CKL("k_exh_items");
+    return M6502_OK;
+}
+
 int init_ctx(m6502_ctx* ctx) {
     if (ctx->ready) return M6502_OK;
     CK(cudaSetDevice(ctx->device));
@@ -1814,6 +1916,11 @@ int init_ctx(m6502_ctx* ctx) {
     int occ = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_exhaustive<SurvSource>, 256, 0));
     ctx->exh_blocks = ctx->sms * std::max(occ, 1);
+    ctx->exh_occ[4] = std::max(occ, 1);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_exhaustive<SurvSource, 3>, 256, 0));
+    ctx->exh_occ[3] = std::max(occ, 1);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_exhaustive<SurvSource, 2>, 256, 0));
+    ctx->exh_occ[2] = std::max(occ, 1);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_exh_items<SurvSource>, 256, 0));
     ctx->exh_item_blocks = ctx->sms * std::max(occ, 1);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_qc1<false>, 256, 0));
@@ -1947,6 +2054,8 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
         }
         CK(cudaEventRecord(ctx->sev[1], ctx->stream));
         uint32_t qgrid = (uint32_t)std::min<uint64_t>(ctx->qc_blocks, (nt + kQcTile - 1) / kQcTile);
+        const bool count_only = (cfg.flags & M6502_COUNT_ONLY) != 0;
+        const uint64_t rlim = count_only ? 0 : rcap;   // emit kernels count past rlim without writing
         if (!scan) {
             TRY(join_table(ctx, dead));
             uint32_t jgrid = (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8, (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
@@ -1956,12 +2065,14 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
                 k_qc_join<true><<<jgrid, 256, 0, ctx->stream>>>(d_targets, tlen,
                                                                 (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p,
                                                                 (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
-                                                                dead, stages, (Surv*)ctx->surv.p, scap, cnt);
+                                                                dead, stages, (Surv*)ctx->surv.p, scap, cnt, 0u);
             else
                 k_qc_join<false><<<jgrid, 256, 0, ctx->stream>>>(d_targets, tlen,
                                                                  (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p,
                                                                  (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
-                                                                 dead, stages, (Surv*)ctx->surv.p, scap, cnt);
+                                                                 dead, stages, (Surv*)ctx->surv.p, scap, cnt,
+                                                                 (ctx->tune.join_probe && (stages & M6502_CHECK_EXH))
+                                                                     ? 1u + cfg.sweep : 0u);
         } else if (go)
             k_qc1<true><<<qgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
                                                         (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
@@ -2027,10 +2138,8 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
                     CK(cudaMemsetAsync(&cnt->exh_ticket, 0, 3 * sizeof(unsigned long long), ctx->stream));
                     ExhArgs ra{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep,
                                cfg.exh_mode == M6502_EXH_BRUTE};
-                    k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(rs, &cnt->round_n, ns, ra);
-                    CKL("k_exhaustive");
-                    k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(rs, ra);
-                    CKL("k_exh_items");
+                    TRY(launch_exh(ctx, rs, &cnt->round_n, ns, ra));
+                    TRY(launch_items(ctx, rs, ra));
                     CK(cudaMemcpyAsync(&cnts[0], &cnt->items, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                        ctx->stream));
                     CK(cudaMemcpyAsync(&cnts[1], &cnt->round_n, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
@@ -2054,19 +2163,13 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             return M6502_OK;
         };
         if (go) CK(cudaMemsetAsync(ctx->best.p, 0xFF, 2 * nt * sizeof(uint32_t), ctx->stream));
-        if (exh && !rounds) {
-            k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &cnt->surv, scap, ea);
-            CKL("k_exhaustive");
-        }
+        if (exh && !rounds) TRY(launch_exh(ctx, src, &cnt->surv, scap, ea));
         if (rounds) {
             TRY(go_rounds());
             if (grow) continue;
         }
         CK(cudaEventRecord(ctx->sev[3], ctx->stream));
-        if (exh && !rounds) {
-            k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
-            CKL("k_exh_items");
-        }
+        if (exh && !rounds) TRY(launch_items(ctx, src, ea));
         CK(cudaEventRecord(ctx->sev[4], ctx->stream));
         // Passing survivors -> Go winners (best) or rules (CUDA semantics).
         auto select_or_emit = [&]() -> int {
@@ -2081,7 +2184,7 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             } else {
                 k_emit_all<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
                                                                   (const uint32_t*)ctx->fail.p, d_ids, 0, dead,
-                                                                  (m6502_rule*)ctx->rules.p, rcap, &cnt->rules, cnt,
+                                                                  (m6502_rule*)ctx->rules.p, rlim, &cnt->rules, cnt,
                                                                   exh ? 1 : 0, d_targets, tlen, cfg.sweep);
                 CKL("k_emit_all");
             }
@@ -2099,7 +2202,7 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             CK(cudaStreamSynchronize(ctx->stream));
             if (hc.surv > scap) { scap = hc.surv + hc.surv / 4 + 1024; redo = true; }
             if (hc.items > icap) { icap = hc.items + hc.items / 4 + 1024; redo = true; }
-            if (hc.rules > rcap) { rcap = hc.rules + hc.rules / 4 + 1024; redo = true; }
+            if (hc.rules > rlim && !count_only) { rcap = hc.rules + hc.rules / 4 + 1024; redo = true; }
             if (redo) continue;
             surv1 = hc.surv;
             items1 = hc.items;
@@ -2128,19 +2231,13 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             }
             CKL("k_qc_join2");
             CK(cudaEventRecord(ctx->sev2[1], ctx->stream));
-            if (exh && !rounds) {
-                k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &cnt->surv, scap, ea);
-                CKL("k_exhaustive");
-            }
+            if (exh && !rounds) TRY(launch_exh(ctx, src, &cnt->surv, scap, ea));
             if (rounds) {
                 TRY(go_rounds());
                 if (grow) continue;
             }
             CK(cudaEventRecord(ctx->sev2[2], ctx->stream));
-            if (exh && !rounds) {
-                k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
-                CKL("k_exh_items");
-            }
+            if (exh && !rounds) TRY(launch_items(ctx, src, ea));
             CK(cudaEventRecord(ctx->sev2[3], ctx->stream));
             TRY(select_or_emit());
             CK(cudaEventRecord(ctx->sev2[4], ctx->stream));
@@ -2149,7 +2246,7 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
         if (go) {
             k_go_emit<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const uint32_t*)ctx->best.p, (uint32_t)nt,
                                                              d_targets, tlen, d_ids,
-                                                             (m6502_rule*)ctx->rules.p, rcap, cnt);
+                                                             (m6502_rule*)ctx->rules.p, rlim, cnt);
             CKL("k_go_emit");
         }
         CK(cudaEventRecord(ctx->sev2[5], ctx->stream));
@@ -2157,12 +2254,12 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
         CK(cudaStreamSynchronize(ctx->stream));
         if (hc.surv > scap) { scap = hc.surv + hc.surv / 4 + 1024; redo = true; }
         if (hc.items > icap) { icap = hc.items + hc.items / 4 + 1024; redo = true; }
-        if (hc.rules > rcap) { rcap = hc.rules + hc.rules / 4 + 1024; redo = true; }
+        if (hc.rules > rlim && !count_only) { rcap = hc.rules + hc.rules / 4 + 1024; redo = true; }
         if (hc.join_items > jcap) { jcap = hc.join_items + hc.join_items / 4 + 1024; redo = true; }
         if (redo) continue;
         size_t old = ctx->staging.size();
-        ctx->staging.resize(old + hc.rules);
-        if (hc.rules)
+        if (!count_only) ctx->staging.resize(old + hc.rules);
+        if (hc.rules && !count_only)
             CK(cudaMemcpyAsync(ctx->staging.data() + old, ctx->rules.p, hc.rules * sizeof(m6502_rule),
                                cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
@@ -2173,13 +2270,13 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             st->pairs += nt * ((uint64_t)kNumInsns + (phase2 ? (uint64_t)kNumInsns * kNumInsns : 0u));
             st->qc_hits += hc.qc;
             st->mid_hits += hc.mid;
-            st->exh_checked += !exh ? 0 : rounds ? round_checked : hc.surv + surv1;
+            st->exh_checked += !exh ? 0 : rounds ? round_checked : hc.surv + surv1 + hc.join_probe_rej;
             st->exh_passed += hc.exh_pass;
             st->rules += hc.rules;
             st->exh_states += hc.states;
             st->exh_items += rounds ? round_items : hc.items + items1;
             st->exh_algo_ops += hc.algo;
-            st->exh_probe_rejects += hc.probe_rejects;
+            st->exh_probe_rejects += hc.probe_rejects + hc.join_probe_rej;
             float ms[5];
             for (int i = 0; i < 5; i++) cudaEventElapsedTime(&ms[i], ctx->sev[i], ctx->sev[i + 1]);
             st->ms_fingerprint += ms[0];
@@ -2221,6 +2318,7 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
     const uint32_t dead = cfg.dead_flags;
     const bool exh = (stages & M6502_CHECK_EXH) != 0;
     const bool scan = (cfg.flags & M6502_QC_SCAN) != 0;
+    const bool count_only = (cfg.flags & M6502_COUNT_ONLY) != 0;
     const uint64_t pmax = std::min(P, n);
     uint64_t scap = std::max<uint64_t>(ctx->surv.bytes / sizeof(Surv), pmax * 4 + 4096);
     uint64_t icap = std::max<uint64_t>(ctx->items.bytes / sizeof(Item), 1u << 16);
@@ -2273,27 +2371,23 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
                     k_qc_join<false><<<jgrid, 256, 0, ctx->stream>>>(
                         d_t, tlen, (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p, (uint8_t*)ctx->cmeta1.p,
                         (const uint64_t*)ctx->join_keys[dead].p, (const uint16_t*)ctx->join_idx[dead].p,
-                        ctx->join_n[dead], dead, stages, (Surv*)ctx->surv.p, scap, cnt);
+                        ctx->join_n[dead], dead, stages, (Surv*)ctx->surv.p, scap, cnt,
+                        (ctx->tune.join_probe && exh) ? 1u + cfg.sweep : 0u);
                     CKL("k_qc_join");
                 }
                 CK(rec(ev[2]));
                 SurvSource src{(const Surv*)ctx->surv.p, d_t, tlen, dead, 0};
                 ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep,
                            cfg.exh_mode == M6502_EXH_BRUTE};
-                if (exh) {
-                    k_exhaustive<SurvSource><<<ctx->exh_blocks, 256, 0, ctx->stream>>>(src, &cnt->surv, scap, ea);
-                    CKL("k_exhaustive");
-                }
+                if (exh) TRY(launch_exh(ctx, src, &cnt->surv, scap, ea));
                 CK(rec(ev[3]));
-                if (exh) {
-                    k_exh_items<SurvSource><<<ctx->exh_item_blocks, 256, 0, ctx->stream>>>(src, ea);
-                    CKL("k_exh_items");
-                }
+                if (exh) TRY(launch_items(ctx, src, ea));
                 CK(rec(ev[4]));
                 k_emit_all<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap,
                                                                   (const uint32_t*)ctx->fail.p, nullptr, b, dead,
-                                                                  (m6502_rule*)ctx->rules.p, rcap, &slots[0].rules, cnt,
-                                                                  exh ? 1 : 0, d_t, tlen, cfg.sweep);
+                                                                  (m6502_rule*)ctx->rules.p, count_only ? 0 : rcap,
+                                                                  &slots[0].rules, cnt, exh ? 1 : 0, d_t, tlen,
+                                                                  cfg.sweep);
                 CKL("k_emit_all");
                 CK(rec(ev[5]));
             }
@@ -2308,7 +2402,8 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
                 (uint64_t)(uintptr_t)ctx->fail.p, (uint64_t)(uintptr_t)ctx->items.p,
                 (uint64_t)(uintptr_t)ctx->rules.p, (uint64_t)(uintptr_t)ctx->cnt_slots.p,
                 (uint64_t)(uintptr_t)ctx->tfp.p, (uint64_t)(uintptr_t)ctx->tmeta.p,
-                (uint64_t)(uintptr_t)ctx->join_keys[dead].p};
+                (uint64_t)(uintptr_t)ctx->join_keys[dead].p, ctx->tune.exh_minb, ctx->tune.ticket_batch,
+                ctx->tune.chunk_log2, ctx->tune.join_probe};
             if (!(ctx->graph.exec && ctx->graph.key == key)) {
                 if (ctx->graph.exec) { cudaGraphExecDestroy(ctx->graph.exec); ctx->graph.exec = nullptr; }
                 // Record; if recording or instantiation fails, this context stops
@@ -2350,9 +2445,11 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
             if (c.items > icap) { icap = std::max<uint64_t>(icap, c.items + c.items / 4 + 1024); redo = true; }
         }
         const uint64_t nrules = hc[0].rules;
-        if (nrules > rcap) { rcap = nrules + nrules / 4 + 1024; redo = true; }
+        if (nrules > rcap && !count_only) { rcap = nrules + nrules / 4 + 1024; redo = true; }
         if (redo) continue;
-        if (out && nrules <= out_cap && ctx->staging.empty()) {   // straight into the caller's buffer
+        if (count_only) {
+            *delivered = true;   // counted, nothing to hand over
+        } else if (out && nrules <= out_cap && ctx->staging.empty()) {   // straight into the caller's buffer
             if (nrules)
                 CK(cudaMemcpyAsync(out, ctx->rules.p, nrules * sizeof(m6502_rule), cudaMemcpyDeviceToHost,
                                    ctx->stream));
@@ -2373,12 +2470,12 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
                 st->pairs += nt * (uint64_t)kNumInsns;
                 st->qc_hits += c.qc;
                 st->mid_hits += c.mid;
-                st->exh_checked += exh ? c.surv : 0;
+                st->exh_checked += exh ? c.surv + c.join_probe_rej : 0;   // the join's probe is part of the check
                 st->exh_passed += c.exh_pass;
                 st->exh_states += c.states;
                 st->exh_items += c.items;
                 st->exh_algo_ops += c.algo;
-                st->exh_probe_rejects += c.probe_rejects;
+                st->exh_probe_rejects += c.probe_rejects + c.join_probe_rej;
                 float ms[5];
                 for (int i = 0; i < 5; i++) cudaEventElapsedTime(&ms[i], ctx->aev[6 * p + i], ctx->aev[6 * p + i + 1]);
                 st->ms_fingerprint += ms[0];
@@ -2442,6 +2539,80 @@ int check_ops_device(m6502_ctx* ctx, const uint16_t* d_ins, uint64_t n) {
 
 }  // namespace
 
+// ---- tuning knobs and their cache file ----
+bool tune_valid(const m6502_tune& t) {
+    return t.exh_minb >= 2 && t.exh_minb <= 4 && t.ticket_batch >= 1 && t.ticket_batch <= 32 &&
+           t.chunk_log2 >= 9 && t.chunk_log2 <= 16 && t.join_probe <= 1;
+}
+
+std::string device_tag(const m6502_ctx* ctx) {
+    cudaDeviceProp prop;
+    std::string name = "unknown";
+    if (cudaGetDeviceProperties(&prop, ctx->device) == cudaSuccess) name = prop.name;
+    for (char& c : name)
+        if (!std::isalnum((unsigned char)c)) c = '_';
+    return name + "-sm" + std::to_string(ctx->sms);
+}
+
+// $M6502_TUNE_CACHE, else $XDG_CACHE_HOME/m6502/ or ~/.cache/m6502/ plus a
+// file per device; "" when none of these is set.
+std::string tune_cache_path(const m6502_ctx* ctx) {
+    if (const char* e = std::getenv("M6502_TUNE_CACHE")) return e;
+    std::string dir;
+    if (const char* x = std::getenv("XDG_CACHE_HOME")) dir = std::string(x) + "/m6502";
+    else if (const char* h = std::getenv("HOME")) dir = std::string(h) + "/.cache/m6502";
+    else return "";
+    return dir + "/tune-" + device_tag(ctx) + ".txt";
+}
+
+const char* kTuneVersion = "m6502-b200 1.0 (sm_100a) tune 1";
+
+// Reads a cache written by tune_save for this device; false when the file is
+// missing, for another device or library, or out of range.
+bool tune_load(const m6502_ctx* ctx, const std::string& path, m6502_tune* out) {
+    FILE* f = std::fopen(path.c_str(), "r");
+    if (!f) return false;
+    char line[256];
+    m6502_tune t{};
+    std::string device, version;
+    int seen = 0;
+    while (std::fgets(line, sizeof line, f)) {
+        std::string l(line);
+        while (!l.empty() && (l.back() == '\n' || l.back() == '\r')) l.pop_back();
+        const size_t eq = l.find('=');
+        if (l.empty() || l[0] == '#' || eq == std::string::npos) continue;
+        const std::string k = l.substr(0, eq), v = l.substr(eq + 1);
+        const uint32_t u = (uint32_t)std::strtoul(v.c_str(), nullptr, 10);
+        if (k == "device") device = v;
+        else if (k == "version") version = v;
+        else if (k == "exh_minb") { t.exh_minb = u; seen |= 1; }
+        else if (k == "ticket_batch") { t.ticket_batch = u; seen |= 2; }
+        else if (k == "chunk_log2") { t.chunk_log2 = u; seen |= 4; }
+        else if (k == "join_probe") { t.join_probe = u; seen |= 8; }
+    }
+    std::fclose(f);
+    if (seen != 15 || device != device_tag(ctx) || version != kTuneVersion || !tune_valid(t)) return false;
+    *out = t;
+    return true;
+}
+
+void tune_save(const m6502_ctx* ctx, const std::string& path, const m6502_tune& t, double ms) {
+    const size_t slash = path.rfind('/');
+    if (slash != std::string::npos && slash > 0) {   // create the directory chain
+        for (size_t p = path.find('/', 1); p != std::string::npos && p <= slash; p = path.find('/', p + 1))
+            mkdir(path.substr(0, p).c_str(), 0755);
+    }
+    const std::string tmp = path + ".tmp" + std::to_string((long)getpid());
+    FILE* f = std::fopen(tmp.c_str(), "w");
+    if (!f) return;
+    std::fprintf(f, "# m6502 tuning cache (m6502_autotune)\ndevice=%s\nversion=%s\n", device_tag(ctx).c_str(),
+                 kTuneVersion);
+    std::fprintf(f, "exh_minb=%u\nticket_batch=%u\nchunk_log2=%u\njoin_probe=%u\nms=%.4f\n", t.exh_minb,
+                 t.ticket_batch, t.chunk_log2, t.join_probe, ms);
+    std::fclose(f);
+    std::rename(tmp.c_str(), path.c_str());   // readers see the old file or the whole new one
+}
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
@@ -2486,6 +2657,11 @@ int m6502_create(m6502_ctx** out, const m6502_opts* opts) {
         fprintf(stderr, "m6502_create: %s\n", ctx->err.c_str());
         m6502_destroy(ctx);
         return rc;
+    }
+    {   // knobs an earlier m6502_autotune chose for this device
+        const std::string path = tune_cache_path(ctx);
+        m6502_tune t;
+        if (!path.empty() && tune_load(ctx, path, &t)) ctx->tune = t;
     }
     *out = ctx;
     return M6502_OK;
@@ -2711,7 +2887,7 @@ int m6502_search(m6502_ctx* ctx, const m6502_search_cfg* cfg, const uint16_t* ta
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     st.ms_device = ms;
     if (stats) *stats = st;
-    if (delivered) {
+    if (delivered || (cfg->flags & M6502_COUNT_ONLY)) {
         if (n_out) *n_out = st.rules;
         return M6502_OK;
     }
@@ -2761,7 +2937,111 @@ int m6502_enumerate(m6502_ctx* ctx, const m6502_search_cfg* cfg, uint32_t tlen, 
     cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
     st.ms_device = ms;
     if (stats) *stats = st;
+    if (cfg->flags & M6502_COUNT_ONLY) {
+        if (n_out) *n_out = st.rules;
+        return M6502_OK;
+    }
     return finish(ctx, out, cap, n_out);
+}
+
+int m6502_tune_get(m6502_ctx* ctx, m6502_tune* out) {
+    if (!ctx || !out) return M6502_E_INVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    *out = ctx->tune;
+    return M6502_OK;
+}
+
+int m6502_tune_set(m6502_ctx* ctx, const m6502_tune* t) {
+    if (!ctx || !t) return M6502_E_INVAL;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    if (!tune_valid(*t)) return set_err(ctx, M6502_E_INVAL, "tuning knob out of range");
+    ctx->tune = *t;
+    return M6502_OK;
+}
+
+int m6502_autotune(m6502_ctx* ctx, const char* cache_path, uint32_t flags, m6502_tune* chosen, double* ms_out) {
+    if (!ctx) return M6502_E_INVAL;
+    std::string path = cache_path ? std::string(cache_path) : tune_cache_path(ctx);
+    if (ms_out) *ms_out = 0.0;
+    if (!(flags & M6502_TUNE_FORCE)) {
+        m6502_tune t;
+        if (!path.empty() && tune_load(ctx, path, &t)) {
+            TRY(m6502_tune_set(ctx, &t));
+            if (chosen) *chosen = t;
+            return M6502_OK;
+        }
+    }
+    // Calibration workload: every pruned length-2 target, enumerated on the device.
+    DevBuf tg, ids, count;
+    const uint64_t span = (uint64_t)kNumInsns * kNumInsns;
+    unsigned long long nt = 0;
+    {
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        CK(cudaSetDevice(ctx->device));
+        TRY(ensure(ctx, tg, span * 2 * sizeof(uint16_t)));
+        TRY(ensure(ctx, ids, span * sizeof(uint64_t)));
+        TRY(ensure(ctx, count, sizeof(unsigned long long)));
+        CK(cudaMemsetAsync(count.p, 0, sizeof(unsigned long long), ctx->stream));
+        const uint32_t grid = (uint32_t)std::min<uint64_t>((span + 255) / 256, (uint64_t)ctx->sms * 16);
+        k_enum_targets<<<grid, 256, 0, ctx->stream>>>(0, span, 2, (uint16_t*)tg.p, (uint64_t*)ids.p, span,
+                                                       (unsigned long long*)count.p);
+        CKL("k_enum_targets");
+        CK(cudaMemcpyAsync(&nt, count.p, sizeof nt, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        cudaFree(ids.p);
+        cudaFree(count.p);
+        ids.p = count.p = nullptr;
+    }
+    m6502_search_cfg cfg{};
+    cfg.semantics = M6502_SEM_CUDA;
+    cfg.sweep = M6502_SWEEP_FULL;
+    cfg.exh_mode = M6502_EXH_CONES;
+    cfg.max_cand_len = 1;
+    cfg.flags = M6502_TARGETS_ON_DEVICE | M6502_COUNT_ONLY;
+    // median of three timed runs after one untimed run (which records the graph)
+    auto measure = [&](const m6502_tune& t, double* ms) -> int {
+        TRY(m6502_tune_set(ctx, &t));
+        double v[3];
+        for (int r = -1; r < 3; r++) {
+            m6502_stats st;
+            uint64_t n = 0;
+            TRY(m6502_search(ctx, &cfg, (const uint16_t*)tg.p, nt, 2, nullptr, 0, &n, &st));
+            if (r >= 0) v[r] = st.ms_device;
+        }
+        std::sort(v, v + 3);
+        *ms = v[1];
+        return M6502_OK;
+    };
+    m6502_tune best = ctx->tune;
+    best.exh_minb = 4; best.ticket_batch = 4; best.chunk_log2 = 11; best.join_probe = 1;
+    double best_ms = 0;
+    int rc = measure(best, &best_ms);
+    // Coordinate descent: each knob in turn over its candidates, the others held.
+    const uint32_t probe_v[] = {0, 1}, minb_v[] = {2, 3, 4}, tb_v[] = {2, 4, 8, 16}, ck_v[] = {10, 11, 12, 13};
+    using Field = uint32_t m6502_tune::*;
+    struct Knob { Field f; const uint32_t* v; int n; };
+    const Knob knobs[] = {{&m6502_tune::join_probe, probe_v, 2}, {&m6502_tune::exh_minb, minb_v, 3},
+                          {&m6502_tune::ticket_batch, tb_v, 4}, {&m6502_tune::chunk_log2, ck_v, 4}};
+    for (const Knob& k : knobs) {
+        if (rc != M6502_OK) break;
+        const m6502_tune base = best;
+        for (int i = 0; i < k.n && rc == M6502_OK; i++) {
+            if (base.*k.f == k.v[i]) continue;
+            m6502_tune t = base;
+            t.*k.f = k.v[i];
+            double ms = 0;
+            rc = measure(t, &ms);
+            if (rc == M6502_OK && ms < best_ms) { best = t; best_ms = ms; }
+        }
+    }
+    cudaFree(tg.p);
+    tg.p = nullptr;
+    TRY(rc);
+    TRY(m6502_tune_set(ctx, &best));
+    if (!path.empty()) tune_save(ctx, path, best, best_ms);   // a cache that cannot be written is not an error
+    if (chosen) *chosen = best;
+    if (ms_out) *ms_out = best_ms;
+    return M6502_OK;
 }
 
 

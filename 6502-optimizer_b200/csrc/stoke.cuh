@@ -381,6 +381,7 @@ struct StokeSource {
         if (lane < cn) sc[lane] = e.ins[lane];
         dead = dead_;
     }
+    __device__ bool probed(uint64_t) const { return false; }
 };
 
 // Over the vec_ok entries sorted by key (one CTA, chunks of 1,024): rep[i] =

@@ -31,6 +31,7 @@ CHECK_QC, CHECK_MID, CHECK_EXH, CHECK_ALL = 1, 2, 4, 7
 TARGETS_ON_DEVICE = 1
 QC_SCAN = 2
 NO_GRAPH = 4
+COUNT_ONLY = 8
 
 
 class M6502Error(RuntimeError):
@@ -120,6 +121,24 @@ assert ctypes.sizeof(MlpExample) == 64
 MLP_OUT = 330
 
 
+class Tune(ctypes.Structure):
+    """m6502_tune: scheduling knobs of the device path (no verdict depends on them)."""
+    _fields_ = [("exh_minb", ctypes.c_uint32), ("ticket_batch", ctypes.c_uint32), ("chunk_log2", ctypes.c_uint32),
+                ("join_probe", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 4)]
+    KNOBS = ("exh_minb", "ticket_batch", "chunk_log2", "join_probe")
+
+    def as_dict(self):
+        return {n: int(getattr(self, n)) for n in self.KNOBS}
+
+
+assert ctypes.sizeof(Tune) == 32
+TUNE_FORCE = 1
+TUNE_DEFAULT = {"exh_minb": 4, "ticket_batch": 4, "chunk_log2": 11, "join_probe": 1}
+# the candidate values m6502_autotune tries for each knob
+TUNE_CANDIDATES = {"join_probe": (0, 1), "exh_minb": (2, 3, 4), "ticket_batch": (2, 4, 8, 16),
+                   "chunk_log2": (10, 11, 12, 13)}
+
+
 _lib = None
 _lock = threading.Lock()
 
@@ -132,7 +151,7 @@ SYMBOLS = (
     "m6502_seq_bytes", "m6502_seq_cycles", "m6502_op_deps", "m6502_format_jsonl",
     "m6502_exhaustive_static", "m6502_stoke_run", "m6502_mlp_param_count", "m6502_mlp_create",
     "m6502_mlp_destroy", "m6502_mlp_last_error", "m6502_mlp_params", "m6502_mlp_predict", "m6502_mlp_gradients",
-    "m6502_mlp_train", "m6502_gemm_bf16",
+    "m6502_mlp_train", "m6502_gemm_bf16", "m6502_tune_get", "m6502_tune_set", "m6502_autotune",
 )
 
 
@@ -195,6 +214,9 @@ def lib():
         L.m6502_gemm_bf16.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
         L.m6502_exhaustive_static.argtypes = [ctypes.c_uint64, vp, vp, vp, vp, ctypes.c_uint8, ctypes.c_uint32,
                                               vp, vp]
+        L.m6502_tune_get.argtypes = [vp, P(Tune)]
+        L.m6502_tune_set.argtypes = [vp, P(Tune)]
+        L.m6502_autotune.argtypes = [vp, ctypes.c_char_p, ctypes.c_uint32, P(Tune), P(ctypes.c_double)]
         _lib = L
         return L
 

@@ -57,6 +57,38 @@ class Engine:
     def stream(self):
         return self._L.m6502_stream(self._ctx)
 
+    # ---- scheduling knobs (m6502_tune) ----
+    @property
+    def tune(self):
+        """The context's knobs as a dict (exh_minb, ticket_batch, chunk_log2, join_probe)."""
+        t = _lib.Tune()
+        with self._lock:
+            self._check(self._L.m6502_tune_get(self._ctx, ctypes.byref(t)))
+        return t.as_dict()
+
+    @tune.setter
+    def tune(self, knobs):
+        t = _lib.Tune()
+        with self._lock:
+            self._check(self._L.m6502_tune_get(self._ctx, ctypes.byref(t)))
+            for k, v in dict(knobs).items():
+                if k not in _lib.Tune.KNOBS:
+                    raise KeyError(k)
+                setattr(t, k, int(v))
+            self._check(self._L.m6502_tune_set(self._ctx, ctypes.byref(t)))
+
+    def autotune(self, cache_path=None, force=False):
+        """Picks the knobs for this device by timing them (or reads them from the
+        device's tuning cache); returns (knobs, ms of the chosen configuration on
+        the calibration run, 0 when the cache was used)."""
+        t = _lib.Tune()
+        ms = ctypes.c_double(0.0)
+        path = cache_path.encode() if cache_path else None
+        with self._lock:
+            self._check(self._L.m6502_autotune(self._ctx, path, _lib.TUNE_FORCE if force else 0, ctypes.byref(t),
+                                               ctypes.byref(ms)))
+        return t.as_dict(), ms.value
+
     # ---- pairwise verifier ----
     def check_pairs(self, targets, candidates, dead_flags=0, checks=_lib.CHECK_ALL,
                     sweep=_lib.SWEEP_REFERENCE, exh_mode=_lib.EXH_CONES, flagdiff=False):
@@ -123,6 +155,13 @@ class Engine:
                 pass
         return np.empty(max(cap, 1), dtype=_lib.RULE_DTYPE)
 
+    def _count(self, fn, *args):
+        """A COUNT_ONLY call: (rule count, stats), no rules copied."""
+        st = _lib.Stats()
+        n_out = ctypes.c_uint64(0)
+        self._check(fn(*args, None, 0, ctypes.byref(n_out), ctypes.byref(st)))
+        return int(n_out.value), st.as_dict()
+
     def _run(self, fn, cap, *args):
         st = _lib.Stats()
         n_out = ctypes.c_uint64(0)
@@ -145,9 +184,10 @@ class Engine:
 
     def search(self, targets, dead_flags=0, semantics=_lib.SEM_CUDA, sweep=_lib.SWEEP_FULL,
                exh_mode=_lib.EXH_CONES, stages=_lib.CHECK_ALL, max_cand_len=1, cap=None,
-               device_ptr=None, qc_scan=False, graph=True):
+               device_ptr=None, qc_scan=False, graph=True, count_only=False):
         """Searches targets (n x tlen array of packed insns, or a device pointer with
-        device_ptr=(ptr, n, tlen)) for shorter replacements.  Returns (rules, stats)."""
+        device_ptr=(ptr, n, tlen)) for shorter replacements.  Returns (rules, stats),
+        or (rule count, stats) with count_only."""
         if device_ptr is not None:
             tptr, n, tlen = device_ptr
             flags = _lib.TARGETS_ON_DEVICE
@@ -163,20 +203,29 @@ class Engine:
             flags |= _lib.QC_SCAN
         if not graph:   # queued searches are otherwise recorded once and replayed as a CUDA graph
             flags |= _lib.NO_GRAPH
+        if count_only:
+            flags |= _lib.COUNT_ONLY
         cfg = self._cfg(semantics, dead_flags, sweep, exh_mode, stages, max_cand_len, flags)
         cap = cap if cap is not None else max(1024, n // 2)
         with self._lock:
-            rules, st = self._run(self._L.m6502_search, cap, self._ctx, ctypes.byref(cfg), tptr, n, tlen)
+            if count_only:
+                rules, st = self._count(self._L.m6502_search, self._ctx, ctypes.byref(cfg), tptr, n, tlen)
+            else:
+                rules, st = self._run(self._L.m6502_search, cap, self._ctx, ctypes.byref(cfg), tptr, n, tlen)
         del keep
         return rules, st
 
     def enumerate(self, target_len=2, dead_flags=0, semantics=_lib.SEM_CUDA, sweep=_lib.SWEEP_FULL,
                   exh_mode=_lib.EXH_CONES, stages=_lib.CHECK_ALL, first=0, last=2863, cap=1 << 21,
-                  max_cand_len=1):
+                  max_cand_len=1, count_only=False):
         """All length-target_len targets whose first instruction has CUDA index in
-        [first, last), searched against candidates of length 1..max_cand_len."""
-        cfg = self._cfg(semantics, dead_flags, sweep, exh_mode, stages, max_cand_len)
+        [first, last), searched against candidates of length 1..max_cand_len.
+        Returns (rules, stats), or (rule count, stats) with count_only."""
+        cfg = self._cfg(semantics, dead_flags, sweep, exh_mode, stages, max_cand_len,
+                        _lib.COUNT_ONLY if count_only else 0)
         with self._lock:
+            if count_only:
+                return self._count(self._L.m6502_enumerate, self._ctx, ctypes.byref(cfg), target_len, first, last)
             return self._run(self._L.m6502_enumerate, cap, self._ctx, ctypes.byref(cfg), target_len,
                              first, last)
 

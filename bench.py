@@ -224,6 +224,14 @@ def run_engine(args):
     shard = np.ascontiguousarray(all_targets[shard_indices(len(all_targets), rank, world)])
     n = len(shard)
     eng = m6502.Engine(device=local)
+    # the scheduling knobs for this device: the tuning cache if one exists,
+    # else timed now (m6502_autotune), before anything is measured
+    if args.tune == "default":
+        eng.tune = _lib.TUNE_DEFAULT
+        tuned, tune_ms, tune_source = eng.tune, 0.0, "default"
+    else:
+        tuned, tune_ms = eng.autotune(force=args.tune == "force")
+        tune_source = "timed" if tune_ms > 0 else "cache"
     stream = torch.cuda.ExternalStream(eng.stream, device=local)
     d_targets = torch.from_numpy(shard.view(np.int16)).to(f"cuda:{local}")
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=f"cuda:{local}")   # > 126 MB L2
@@ -366,6 +374,9 @@ def run_engine(args):
             # opcode check of the targets
             "gpu_launches": int((4 * s0["passes"] + 1) * args.steps),
         }
+        line["config"]["tuning"] = dict(tuned, source=tune_source, calibration_ms=tune_ms)
+        if world == 1 and not args.no_mask_ff:
+            line["mask_ff"] = mask_ff_run(eng, stream, d_targets, n, sweep)
         if world == 1 and not args.no_cpu_baseline:
             rate, kind, ns, stride, dt = cpu_reference_rate(all_targets, args.cpu_sample, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": rate, "unit": "pair-checks/s", "cores": os.cpu_count() or 1,
@@ -378,6 +389,35 @@ def run_engine(args):
     if dist:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def mask_ff_run(eng, stream, d_targets, n, sweep):
+    """The same enumeration at dead-flags 0xFF (every flag dead): 482 M pairs
+    survive MidCheck and go to ExhaustiveCheck.  The rules are counted on the
+    device, not copied out.  One warm-up run, then one run timed with CUDA
+    events on the engine's stream."""
+    import torch
+    from m6502 import _lib
+
+    def run():
+        return eng.search(None, dead_flags=0xFF, semantics=_lib.SEM_CUDA, sweep=sweep,
+                          device_ptr=(d_targets.data_ptr(), n, 2), count_only=True)
+    run()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    nrules, st = run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    return {"dead_flags": "0xFF", "ms": ms, "pair_checks_per_s": n * PAIRS_PER_TARGET / (ms / 1e3),
+            "rules": nrules, "qc_hits": st["qc_hits"], "mid_hits": st["mid_hits"],
+            "exh_checked": st["exh_checked"], "exh_passed": st["exh_passed"],
+            "exh_probe_rejects": st["exh_probe_rejects"], "exh_states": st["exh_states"],
+            "exh_items": st["exh_items"],
+            "stages_ms": {"qc_mid_ms": st["ms_qc"], "exhaustive_ms": st["ms_exhaustive"],
+                          "exh_items_ms": st["ms_exh_items"], "emit_ms": st["ms_emit"]},
+            "note": "rules counted on the device (M6502_COUNT_ONLY), not copied to the host"}
 
 
 def stoke_once(eng, targets, args, model=None):
@@ -655,6 +695,10 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=1500, help="targets in the CPU baseline sample")
     ap.add_argument("--ref-sample", type=int, default=600, help="targets per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mask-ff", action="store_true", help="skip the dead-flags 0xFF run of the default line")
+    ap.add_argument("--tune", choices=["auto", "force", "default"], default="auto",
+                    help="scheduling knobs: the device's tuning cache or a timed tuning (auto), a new timed "
+                         "tuning (force), or the built-in defaults")
     ap.add_argument("--workload", choices=["len2", "len3", "stoke", "stoke-learned", "gemm"], default="len2")
     ap.add_argument("--gemm-n", type=int, default=8192, help="GEMM workload: M = N = K")
     ap.add_argument("--first-op", type=int, default=0,

@@ -74,7 +74,10 @@ enum {
                                     opcodes are checked on the device */
     M6502_QC_SCAN = 2,           /* QuickCheck by scanning every pair instead of the
                                     exact join on vector-0 outputs (same survivors) */
-    M6502_NO_GRAPH = 4           /* do not record or replay the search as a CUDA graph */
+    M6502_NO_GRAPH = 4,          /* do not record or replay the search as a CUDA graph */
+    M6502_COUNT_ONLY = 8         /* rules are counted, not returned: *n_out and the stats
+                                    get the counts, `out` is not written (stage statistics
+                                    of runs whose rule sets do not fit host memory) */
 };
 
 typedef struct m6502_ctx m6502_ctx;
@@ -109,7 +112,8 @@ typedef struct m6502_search_cfg {
                               sorted QuickCheck-key table per mask; Go semantics try
                               length 2 only where length 1 found nothing
                               (pkg/search/worker.go:122-176). */
-    uint32_t flags;        /* M6502_TARGETS_ON_DEVICE */
+    uint32_t flags;        /* M6502_TARGETS_ON_DEVICE, M6502_QC_SCAN, M6502_NO_GRAPH,
+                              M6502_COUNT_ONLY */
     uint8_t dead_flags;    /* dead-flags mask of the run */
     uint8_t reserved[7];
 } m6502_search_cfg;
@@ -137,6 +141,42 @@ typedef struct m6502_stats {
                               candidates; host targets are first copied to the
                               device), else 0 */
 } m6502_stats;
+
+/* ---- tuning ----
+ * No counterpart in the reference, whose launch shapes are compile-time
+ * constants (BATCH_SIZE, BLOCK_SIZE, EXHAUST_BLOCK at
+ * cuda/6502_search_v2.cu:28-34).  Knobs of the device path; none changes a
+ * verdict or a rule, only how the work is scheduled. */
+typedef struct m6502_tune {
+    uint32_t exh_minb;      /* 2, 3 or 4: resident 256-thread blocks per SM that the
+                               exhaustive kernel's register cap is set for (128, 80 or
+                               64 registers per thread) */
+    uint32_t ticket_batch;  /* 1..32: pairs an exhaustive warp claims per ticket */
+    uint32_t chunk_log2;    /* 9..16: states per work item of a large cone, log2 */
+    uint32_t join_probe;    /* 0 or 1: the random-state probe of MidCheck survivors runs
+                               inside the QuickCheck join (CUDA semantics, length-1
+                               candidates) instead of in the exhaustive kernel */
+    uint32_t reserved[4];
+} m6502_tune;               /* 32 bytes */
+
+/* The knobs a context uses.  A new context starts from the defaults
+ * {4, 4, 11, 1} or, when a tuning cache for its device exists (see
+ * m6502_autotune), from the cached choice. */
+int m6502_tune_get(m6502_ctx *ctx, m6502_tune *out);
+/* Sets the knobs; M6502_E_INVAL for a value out of range. */
+int m6502_tune_set(m6502_ctx *ctx, const m6502_tune *t);
+enum { M6502_TUNE_FORCE = 1 /* tune even when a cache for this device exists */ };
+/* Picks the knobs for this device by timing them on the device (full
+ * length-2 enumeration, CUDA semantics, full sweep, mask 0x00: coordinate
+ * descent over join_probe, exh_minb, ticket_batch and chunk_log2, median of
+ * three timed runs each, about a second), sets them on ctx and writes them to
+ * `cache_path` (NULL: $M6502_TUNE_CACHE, else $XDG_CACHE_HOME/m6502/ or
+ * ~/.cache/m6502/, one file per device name and SM count).  Without
+ * M6502_TUNE_FORCE a readable cache for the device is used instead of
+ * timing.  *ms (optional) gets the chosen configuration's time on the
+ * calibration run (0 when the cache was used).  Other calls must not use
+ * ctx while it runs. */
+int m6502_autotune(m6502_ctx *ctx, const char *cache_path, uint32_t flags, m6502_tune *chosen, double *ms);
 
 /* ---- context ---- */
 const char *m6502_version(void);

@@ -19,6 +19,7 @@ REF_BIN = os.path.join(HERE, "_ref", "6502search_v2")
 SEM_CUDA, SEM_GO = 0, 1
 SWEEP_REFERENCE, SWEEP_FULL = 0, 1
 STAGE_QC, STAGE_MID, STAGE_EXH = 1, 2, 4
+REF_COUNT_ONLY = 8   # ref_search: stage counts only, no rule list
 
 
 class State(ctypes.Structure):
@@ -220,6 +221,18 @@ def ref():
         R.ref_op_writes.restype = ctypes.c_uint16
         _ref = R
     return _ref
+
+
+def ref_stage_counts(targets, dead=0, stages=STAGE_QC | STAGE_MID, nthreads=None):
+    """Stage counts of the reference host pipeline (no rule list kept)."""
+    t = np.ascontiguousarray(np.asarray(targets, dtype=np.uint16))
+    n, tlen = t.shape
+    cnt = (ctypes.c_uint64 * 4)()
+    k = ref().ref_search(t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), n, tlen, dead, stages | REF_COUNT_ONLY,
+                         None, 0, cnt, nthreads or os.cpu_count() or 1)
+    out = dict(zip(("pairs", "qc_hits", "mid_hits", "exh_checked"), (int(x) for x in cnt)))
+    out["passed"] = int(k)
+    return out
 
 
 def ref_search(targets, dead=0, stages=7, nthreads=None):

@@ -74,6 +74,7 @@ void* ref_job_main(void* arg) {
                 j->exh++;
                 if (!cpu_exhaustive_check(ops, imms, j->tlen, co, cm, 1, j->dead)) continue;
             }
+            if (j->stages & 8) continue;   // counts only
             j->rules.push_back((uint32_t)ti);
             j->rules.push_back((uint32_t)ci);
         }
@@ -137,6 +138,8 @@ int ref_instructions(uint16_t* out) {
 // nthreads threads.  Writes (target, candidate index) pairs of passing
 // rules into out (2 * cap entries) and the stage counters into counts[4]
 // = {pairs, qc_hits, mid_hits, exh_checked}.  Returns the rule count.
+// stages: bit 0 QuickCheck, 1 MidCheck, 2 ExhaustiveCheck; bit 3 counts
+// only (no pair is kept: for runs with hundreds of millions of survivors).
 uint64_t ref_search(const uint16_t* targets, uint64_t n, int tlen, uint8_t dead, int stages,
                     uint32_t* out, uint64_t cap, uint64_t* counts, int nthreads) {
     init_tables();

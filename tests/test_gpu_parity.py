@@ -236,6 +236,36 @@ def test_enumerate_length2_published_counts(engine):
     assert len({int(r["target"]) * 65536 + int(r["cand"][0]) for r in rules}) == len(rules)
 
 
+@pytest.mark.parametrize("mask", ["0x00", "0xFF"])
+def test_enumerate_length2_stage_counts_at_mask(engine, mask):
+    """Full length-2 enumeration through QuickCheck and MidCheck at
+    dead-flags 0x00 and 0xFF: the counts equal those of the reference's own
+    host pipeline over the same targets (tests/golden/len2_counts.json).  At
+    0xFF 482 M pairs survive MidCheck; they are counted on the device, not
+    returned."""
+    want = READ("len2_counts.json")
+    ref = want["masks"][mask]
+    n, st = engine.enumerate(2, dead_flags=int(mask, 16), sweep=_lib.SWEEP_REFERENCE,
+                             stages=_lib.CHECK_QC | _lib.CHECK_MID, count_only=True)
+    assert st["targets"] == want["targets"]
+    assert st["pairs"] == ref["pairs"]
+    assert st["qc_hits"] == ref["qc_hits"]
+    assert st["mid_hits"] == ref["mid_hits"]
+    assert n == st["rules"] == ref["mid_hits"]   # without ExhaustiveCheck the survivors are the rules
+
+
+def test_enumerate_length2_mask_ff_full_pipeline(engine):
+    """The whole pipeline at 0xFF, full sweep, counted on the device: every
+    MidCheck survivor reaches ExhaustiveCheck (the reference binary drops
+    QuickCheck hits beyond 131,072 per batch here, cuda/6502_search_v2.cu:
+    874-876)."""
+    ref = READ("len2_counts.json")["masks"]["0xFF"]
+    n, st = engine.enumerate(2, dead_flags=0xFF, sweep=_lib.SWEEP_FULL, count_only=True)
+    assert st["qc_hits"] == ref["qc_hits"] and st["mid_hits"] == ref["mid_hits"]
+    assert st["exh_checked"] == ref["mid_hits"]
+    assert 0 < n == st["rules"] == st["exh_passed"] <= st["exh_checked"]
+
+
 def test_enumerate_slices_union_equals_whole(engine):
     whole, _ = engine.enumerate(2, sweep=_lib.SWEEP_REFERENCE, first=100, last=160)
     parts = []
