@@ -1811,7 +1811,7 @@ struct m6502_ctx {
     DevBuf c2_keys_in, c2_idx_in, c2_sort_tmp;
     uint32_t join_n[256] = {};
     DevBuf st_tins, st_toffs, st_tout, st_tbytes, st_chains, st_entries, st_vidx, st_proven, st_cnt, st_pidx,
-        st_mex, st_probs, st_traj;
+        st_mex, st_probs, st_traj, st_row;
     DevBuf st_keys, st_keys2, st_vals2, st_rep, st_ord, st_verdict, st_vlist, st_vpos, st_sort_tmp, st_vphase,
         st_pphase;
 };
@@ -2680,7 +2680,7 @@ void m6502_destroy(m6502_ctx* ctx) {
                       &ctx->pins, &ctx->poffs, &ctx->cins, &ctx->coffs, &ctx->pout, &ctx->pfd,
                       &ctx->enum_count, &ctx->st_tins, &ctx->st_toffs, &ctx->st_tout, &ctx->st_tbytes,
                       &ctx->st_chains, &ctx->st_entries, &ctx->st_vidx, &ctx->st_proven, &ctx->st_cnt,
-                      &ctx->st_pidx, &ctx->st_mex, &ctx->st_probs, &ctx->st_traj, &ctx->st_keys,
+                      &ctx->st_pidx, &ctx->st_mex, &ctx->st_probs, &ctx->st_traj, &ctx->st_row, &ctx->st_keys,
                       &ctx->st_keys2, &ctx->st_vals2, &ctx->st_rep, &ctx->st_ord, &ctx->st_verdict,
                       &ctx->st_vlist, &ctx->st_vpos, &ctx->st_sort_tmp, &ctx->c2_keys_in, &ctx->c2_idx_in,
                       &ctx->c2_sort_tmp, &ctx->go_keys, &ctx->go_keys2, &ctx->go_ord, &ctx->go_round,

@@ -42,6 +42,7 @@ struct StokeCounters {
     unsigned long long max_ord;   // largest per-target ordinal of a distinct pair
     unsigned long long round_n;   // pairs verified in the current round
     unsigned long long verified;  // pairs verified this epoch (all rounds)
+    unsigned long long ex_rows;   // chains given a row of the learned proposal this epoch
 };
 
 constexpr uint32_t kVerifyBatch = 8;   // distinct candidates per target per round under stop_on_proof
@@ -81,7 +82,8 @@ struct StokeParams {
     float t_start;
     const uint32_t* proven; // per target: 1 once proved (stop_on_proof)
     uint32_t stop_on_proof;
-    const float* cdf;       // PROPOSAL_MIXED: per chain 330 cumulative probabilities (3 heads)
+    const float* cdf;       // PROPOSAL_MIXED: 330 cumulative probabilities (3 heads) per row
+    const uint32_t* row;    // per chain: its row of cdf, or kNoRow (uniform moves only)
     float learned_frac;
     m6502_mlp_example* traj;   // improving moves as labelled examples (optional)
     uint64_t traj_cap;
@@ -145,17 +147,32 @@ __device__ __forceinline__ int cdf_sample(const float* cdf, int a, int b, uint64
     return lo - a;
 }
 
-// The model's input for every chain: target, current candidate and its
-// vector mismatch mask (a chain about to (re)start uses the target itself).
+constexpr uint32_t kNoRow = 0xFFFFFFFFu;
+
+// The model's input for every chain still searching: target, current
+// candidate and its vector mismatch mask (a chain about to (re)start uses
+// the target itself).  Chains of proved targets under stop_on_proof get no
+// row; the others get consecutive rows (row[ci]), so the forward pass runs
+// over the live chains only.
 __global__ void k_stoke_examples(const StokeChain* __restrict__ chains, uint32_t n_chains, uint32_t cpt,
-                                 StokeTargets tg, m6502_mlp_example* __restrict__ ex) {
+                                 StokeTargets tg, const uint32_t* __restrict__ proven, uint32_t stop_on_proof,
+                                 m6502_mlp_example* __restrict__ ex, uint32_t* __restrict__ row,
+                                 StokeCounters* __restrict__ sc) {
     const int lane = threadIdx.x & 31;
     for (uint32_t ci = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); ci < n_chains;
          ci += gridDim.x * kWarpsPerBlock) {
         const StokeChain& ch = chains[ci];
         const uint32_t t = ci / cpt, t0 = tg.off[t], tlen = tg.off[t + 1] - t0;
+        if (ch.status == 2 || (stop_on_proof && proven[t])) {
+            if (lane == 0) row[ci] = kNoRow;
+            continue;
+        }
+        unsigned long long r = 0;
+        if (lane == 0) r = atomicAdd(&sc->ex_rows, 1ull);
+        r = __shfl_sync(kFull, r, 0);
+        if (lane == 0) row[ci] = (uint32_t)r;
         const bool fresh = ch.status != 1;
-        m6502_mlp_example& x = ex[ci];
+        m6502_mlp_example& x = ex[r];
         if (lane < 8) x.target[lane] = lane < (int)tlen ? tg.ins[t0 + lane] : 0;
         if (lane < 16) x.cand[lane] = fresh ? (lane < (int)tlen ? tg.ins[t0 + lane] : 0) : ch.cur[lane];
         if (lane == 0) {
@@ -212,7 +229,8 @@ __global__ void __launch_bounds__(256) k_stoke_epoch(StokeChain* __restrict__ ch
     uint64_t rng, step = ch.step, since = ch.since;
     uint32_t accepted = 0, diff = 0;
     bool zero;
-    const float* cdf = prm.cdf ? prm.cdf + (size_t)ci * 330 : nullptr;
+    const uint32_t crow = prm.cdf ? prm.row[ci] : kNoRow;
+    const float* cdf = crow != kNoRow ? prm.cdf + (size_t)crow * 330 : nullptr;
     if (status == 0) {   // NewChain (mcmc.go:28-49): start from the target
         if (lane < (int)tlen) { cur[lane] = tg.ins[t0 + lane]; best[lane] = cur[lane]; }
         __syncwarp();
@@ -576,6 +594,7 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
     prm.stop_on_proof = cfg->stop_on_proof;
     prm.proven = (const uint32_t*)ctx->st_proven.p;
     prm.cdf = nullptr;
+    prm.row = nullptr;
     prm.learned_frac = cfg->learned_frac > 0 ? cfg->learned_frac : 0.5f;
     prm.traj = nullptr;
     prm.traj_cap = 0;
@@ -583,7 +602,7 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
     if (mixed) {
         TRY(ensure(ctx, ctx->st_mex, (size_t)n_chains * sizeof(m6502_mlp_example)));
         TRY(ensure(ctx, ctx->st_probs, (size_t)n_chains * 330 * sizeof(float)));
-        prm.cdf = (const float*)ctx->st_probs.p;
+        TRY(ensure(ctx, ctx->st_row, (size_t)n_chains * sizeof(uint32_t)));
     }
     uint64_t traj_total = 0;
     if (cfg->trajectories && cfg->traj_cap) {
@@ -613,20 +632,34 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
     uint32_t proven_targets = 0;
     uint32_t epoch_len = cfg->first_epoch ? std::min(cfg->first_epoch, spe) : spe;
     for (uint64_t done = 0; done < steps;) {
+        // The first epoch runs uniform moves only: a target the first random
+        // moves rewrite costs no forward pass; from the second epoch on the
+        // model is refreshed for the chains still searching.
+        const bool use_model = mixed && done > 0;
         const uint32_t e_steps = (uint32_t)std::min<uint64_t>(epoch_len, steps - done);
         epoch_len = (uint32_t)std::min<uint64_t>((uint64_t)epoch_len * 2, spe);
         prm.steps = e_steps;
         CK(cudaMemsetAsync(sc, 0, sizeof(StokeCounters), ctx->stream));
         CK(cudaEventRecord(ctx->sev[0], ctx->stream));
-        if (mixed) {   // refresh the learned proposal of every chain
+        prm.cdf = nullptr;
+        if (use_model) {   // refresh the learned proposal of the chains still searching
             k_stoke_examples<<<(n_chains + kWarpsPerBlock - 1) / kWarpsPerBlock, 256, 0, ctx->stream>>>(
-                (const StokeChain*)ctx->st_chains.p, n_chains, cpt, tg, (m6502_mlp_example*)ctx->st_mex.p);
+                (const StokeChain*)ctx->st_chains.p, n_chains, cpt, tg, (const uint32_t*)ctx->st_proven.p,
+                cfg->stop_on_proof, (m6502_mlp_example*)ctx->st_mex.p, (uint32_t*)ctx->st_row.p, sc);
             CKL("k_stoke_examples");
-            int mrc = m6502_mlp_forward_device(cfg->model, (const m6502_mlp_example*)ctx->st_mex.p, n_chains,
-                                               (float*)ctx->st_probs.p, ctx->stream);
-            if (mrc != M6502_OK) return set_err(ctx, mrc, "learned proposal forward pass failed");
-            k_cdf<<<(n_chains + 255) / 256, 256, 0, ctx->stream>>>((float*)ctx->st_probs.p, n_chains);
-            CKL("k_cdf");
+            unsigned long long rows = 0;
+            CK(cudaMemcpyAsync(&rows, &sc->ex_rows, sizeof rows, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            if (rows) {
+                int mrc = m6502_mlp_forward_device(cfg->model, (const m6502_mlp_example*)ctx->st_mex.p, rows,
+                                                   (float*)ctx->st_probs.p, ctx->stream);
+                if (mrc != M6502_OK) return set_err(ctx, mrc, "learned proposal forward pass failed");
+                k_cdf<<<(uint32_t)((rows + 255) / 256), 256, 0, ctx->stream>>>((float*)ctx->st_probs.p,
+                                                                             (uint32_t)rows);
+                CKL("k_cdf");
+                prm.cdf = (const float*)ctx->st_probs.p;
+                prm.row = (const uint32_t*)ctx->st_row.p;
+            }
         }
         k_stoke_epoch<<<(n_chains + kWarpsPerBlock - 1) / kWarpsPerBlock, 256, 0, ctx->stream>>>(
             (StokeChain*)ctx->st_chains.p, n_chains, tg, prm, (StokeEntry*)ctx->st_entries.p, ecap, sc);

@@ -377,6 +377,9 @@ def run_engine(args):
         line["config"]["tuning"] = dict(tuned, source=tune_source, calibration_ms=tune_ms)
         if world == 1 and not args.no_mask_ff:
             line["mask_ff"] = mask_ff_run(eng, stream, d_targets, n, sweep)
+        if world == 1 and not args.no_stoke:   # configs 4 and 5, beside the headline
+            main, extra = stoke_compare(eng, args, learned=True)
+            line["stoke"] = {"config": stoke_config(args, True), "learned": main, **extra}
         if world == 1 and not args.no_cpu_baseline:
             rate, kind, ns, stride, dt = cpu_reference_rate(all_targets, args.cpu_sample, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": rate, "unit": "pair-checks/s", "cores": os.cpu_count() or 1,
@@ -460,28 +463,48 @@ def hard_target_speedup(res_u, res_l, min_steps, budget):
             "median_step_ratio": statistics.median(ratios) if ratios else None}
 
 
-def run_stoke(args):
-    """STOKE benchmark workloads on 512 seeded targets of length 4..8 (seed 2),
-    128 chains each (65,536 chains), Hamming cost over the 32 MidCheck
-    vectors, temperature 1.0 -> 0.1; every shorter zero-cost best is proved on
-    the GPU (full sweep).  Metric: median time-to-proof over the proved
-    targets.  `stoke`: the uniform proposal.  `stoke-learned`: the 50/50
-    mixed proposal of a model trained first on the GPU (training targets
-    seed 20, validation seed 22, disjoint draws), reported beside a uniform
-    run with the same seeds."""
-    import torch
-    import m6502
+def hard_target_times(res_u, res_l, first_epoch, ms_u, ms_l):
+    """Time-to-proof on the targets uniform STOKE did not prove within its
+    first epoch (the same seeds make that epoch identical under both
+    proposals, since the model is first used in the second).  A target a
+    proposal never proved counts at that run's whole device time (censored,
+    so its true time is at least that); targets neither proved are left
+    out.  Returns both medians, their ratio and the median per-target
+    ratio."""
+    tu, tl, ratios, cens_u, cens_l = [], [], [], 0, 0
+    for ru, rl in zip(res_u, res_l):
+        if ru["first_proof_ms"] >= 0 and ru["first_proof_step"] < first_epoch:
+            continue
+        if ru["first_proof_ms"] < 0 and rl["first_proof_ms"] < 0:
+            continue
+        a = ru["first_proof_ms"] if ru["first_proof_ms"] >= 0 else ms_u
+        b = rl["first_proof_ms"] if rl["first_proof_ms"] >= 0 else ms_l
+        cens_u += ru["first_proof_ms"] < 0
+        cens_l += rl["first_proof_ms"] < 0
+        tu.append(a)
+        tl.append(b)
+        ratios.append(a / b if b > 0 else None)
+    ratios = [r for r in ratios if r is not None]
+    mu, ml = (statistics.median(tu) if tu else None), (statistics.median(tl) if tl else None)
+    return {"targets": len(tu), "definition": f"uniform first proof at step >= {first_epoch} or never",
+            "median_ms_uniform": mu, "median_ms_learned": ml,
+            "speedup_median_ms": mu / ml if mu and ml else None,
+            "median_per_target_ratio": statistics.median(ratios) if ratios else None,
+            "censored_uniform": cens_u, "censored_learned": cens_l}
+
+
+def stoke_compare(eng, args, learned):
+    """The 512-target STOKE workload (seed 2) with the uniform proposal and,
+    when `learned`, with the 50/50 mixed proposal of a model first trained on
+    the GPU (training targets seed 20, validation seed 22, disjoint draws).
+    Returns (summary of the main run, extra keys)."""
     from m6502 import inst, _lib
     from m6502.proposal import train_proposal
-    rank, world, local = dist_env()
-    torch.cuda.set_device(local)
     targets = inst.draw_targets(2, 4, 8, 512, reject_pruned=False)
-    eng = m6502.Engine(device=local)
     # warm-up at full size (every device buffer allocated before the timed runs)
     eng.stoke(targets, chains_per_target=128, steps=4 * args.stoke_first_epoch, steps_per_epoch=args.stoke_epoch,
               first_epoch=args.stoke_first_epoch, seed=1, cost=_lib.COST_HAMMING, sweep=_lib.SWEEP_FULL,
               stop_on_proof=True)
-    learned = args.workload == "stoke-learned"
     model, train_info, train_s = None, None, None
     if learned:
         t0 = time.perf_counter()
@@ -489,36 +512,60 @@ def run_stoke(args):
                                            inst.draw_targets(22, 4, 8, 64, reject_pruned=False),
                                            steps=3000, chunk=500)
         train_s = time.perf_counter() - t0
+    res_u, uni = stoke_once(eng, targets, args)
+    extra = {}
+    if not learned:
+        return uni, extra
+    res_l, lrn = stoke_once(eng, targets, args, model)
+    extra["uniform"] = uni
+    extra["train"] = dict(train_info, seconds=train_s)
+    if uni["median_ms"] and lrn["median_ms"]:
+        extra["speedup_median_ms"] = uni["median_ms"] / lrn["median_ms"]
+    if uni["median_steps"] is not None and lrn["median_steps"] is not None:
+        extra["speedup_median_steps"] = (uni["median_steps"] + 1) / (lrn["median_steps"] + 1)
+    extra["hard_targets"] = hard_target_times(res_u, res_l, args.stoke_first_epoch, uni["ms_device"],
+                                              lrn["ms_device"])
+    extra["hard_targets_steps"] = hard_target_speedup(res_u, res_l, 1000, args.stoke_steps)
+    model.close()
+    return lrn, extra
+
+
+def run_stoke(args):
+    """STOKE benchmark workloads on 512 seeded targets of length 4..8 (seed 2),
+    128 chains each (65,536 chains), Hamming cost over the 32 MidCheck
+    vectors, temperature 1.0 -> 0.1; every shorter zero-cost best is proved on
+    the GPU (full sweep).  Metric: median time-to-proof over the proved
+    targets.  `stoke`: the uniform proposal.  `stoke-learned`: the 50/50
+    mixed proposal of a model trained first on the GPU, reported beside a
+    uniform run with the same seeds."""
+    import torch
+    import m6502
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    eng = m6502.Engine(device=local)
+    learned = args.workload == "stoke-learned"
     clocks = ClockSampler(local)
     clocks.start()
-    res_u, uni = stoke_once(eng, targets, args)
-    res_l, lrn = stoke_once(eng, targets, args, model) if learned else (None, None)
+    main, extra = stoke_compare(eng, args, learned)
     clk = clocks.stop()
-    main = lrn if learned else uni
     line = {"metric": "STOKE time-to-proof (median over proved targets)", "value": main["median_ms"], "unit": "ms",
             "higher_is_better": False, "n_gpus": 1, "steps": args.stoke_steps, "warmup": 1,
             "dtype": "u8", "data": "synthetic (512 seeded random targets, length 4-8, seed 2)",
-            "config": {"workload": "stoke-512x128" + ("-learned" if learned else ""), "targets": len(targets),
-                       "chains_per_target": 128, "steps_per_chain": args.stoke_steps,
-                       "steps_per_epoch": args.stoke_epoch, "first_epoch": args.stoke_first_epoch,
-                       "cost": "hamming over 32 vectors + bytes + cycles/100", "temperature": "1.0 -> 0.1",
-                       "proposal": "mixed 50/50 learned + uniform" if learned else "uniform",
-                       "sweep": "full", "stop_on_proof": True},
+            "config": stoke_config(args, learned),
             "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}}
     line.update(main)
-    if learned:
-        line["uniform"] = uni
-        line["train"] = dict(train_info, seconds=train_s)
-        if uni["median_ms"] and main["median_ms"]:
-            line["speedup_median_ms"] = uni["median_ms"] / main["median_ms"]
-        if uni["median_steps"] and main["median_steps"]:
-            line["speedup_median_steps"] = uni["median_steps"] / main["median_steps"]
-        # most targets fall to the first random delete under either proposal;
-        # the proposal matters on the rest
-        line["hard_targets"] = hard_target_speedup(res_u, res_l, 1000, args.stoke_steps)
-        model.close()
+    line.update(extra)
     print(json.dumps(line), flush=True)
     eng.close()
+
+
+def stoke_config(args, learned):
+    return {"workload": "stoke-512x128" + ("-learned" if learned else ""), "targets": 512,
+            "chains_per_target": 128, "steps_per_chain": args.stoke_steps,
+            "steps_per_epoch": args.stoke_epoch, "first_epoch": args.stoke_first_epoch,
+            "cost": "hamming over 32 vectors + bytes + cycles/100", "temperature": "1.0 -> 0.1",
+            "proposal": "mixed 50/50 learned + uniform (model from the second epoch on)" if learned else "uniform",
+            "sweep": "full", "stop_on_proof": True}
 
 
 def run_gemm(args):
@@ -696,6 +743,7 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=600, help="targets per reference-arm step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mask-ff", action="store_true", help="skip the dead-flags 0xFF run of the default line")
+    ap.add_argument("--no-stoke", action="store_true", help="skip the STOKE runs (configs 4, 5) of the default line")
     ap.add_argument("--tune", choices=["auto", "force", "default"], default="auto",
                     help="scheduling knobs: the device's tuning cache or a timed tuning (auto), a new timed "
                          "tuning (force), or the built-in defaults")
