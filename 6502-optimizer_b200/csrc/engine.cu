@@ -212,6 +212,7 @@ struct Counters {
     unsigned long long round_n, max_ord;   // Go-order verification rounds
     unsigned long long join_items;         // chunks of long length-2 equal ranges
     unsigned long long join_probe_rej;     // MidCheck survivors the join's probe rejected
+    unsigned long long undecided;          // pairs left undecided (a cone beyond the sweep cap)
 };
 
 struct Item {   // one chunk of a large cone sweep
@@ -1427,10 +1428,11 @@ __global__ void k_emit_all(const Surv* __restrict__ surv, const unsigned long lo
                            const uint16_t* __restrict__ targets, uint32_t tlen, uint32_t sweep_mode) {
     const uint64_t n = min((uint64_t)*n_ptr, n_cap);
     const int lane = threadIdx.x & 31;
-    unsigned long long npass = 0, algo = 0;
+    unsigned long long npass = 0, algo = 0, nund = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t p = base + threadIdx.x;
         bool pass = p < n && (!check_exh || fail[p] == 0);
+        nund += (p < n && check_exh && fail[p] == 3u) ? 1u : 0u;   // left undecided: counted, not a rule
         m6502_rule r;
         memset(&r, 0, sizeof r);
         if (pass) {
@@ -1458,9 +1460,11 @@ __global__ void k_emit_all(const Surv* __restrict__ surv, const unsigned long lo
     for (int o = 16; o; o >>= 1) {
         npass += __shfl_down_sync(kFull, npass, o);
         algo += __shfl_down_sync(kFull, algo, o);
+        nund += __shfl_down_sync(kFull, nund, o);
     }
     if (lane == 0 && npass) atomicAdd(&cnt->exh_pass, npass);
     if (lane == 0 && algo) atomicAdd(&cnt->algo, algo);
+    if (lane == 0 && nund) atomicAdd(&cnt->undecided, nund);
 }
 
 // Go-order rank of a survivor's candidate; length-2 candidates (bit 28)
@@ -1478,9 +1482,9 @@ __global__ void k_go_select(const Surv* __restrict__ surv, const unsigned long l
                             Counters* cnt, const uint16_t* __restrict__ targets, uint32_t tlen,
                             uint32_t sweep_mode) {
     const uint64_t n = min((uint64_t)*n_ptr, n_cap);
-    unsigned long long npass = 0, algo = 0;
+    unsigned long long npass = 0, algo = 0, nund = 0;
     for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
-        if (fail[p]) continue;
+        if (fail[p]) { nund += fail[p] == 3u; continue; }   // undecided pairs count as not passing
         npass++;
         Surv s = surv[p];
         const uint32_t idx = s.c & 0x7FFFFFu, key = go_rank_of(s.c);
@@ -1495,6 +1499,7 @@ __global__ void k_go_select(const Surv* __restrict__ surv, const unsigned long l
     }
     if (npass) atomicAdd(&cnt->exh_pass, npass);
     if (algo) atomicAdd(&cnt->algo, algo);
+    if (nund) atomicAdd(&cnt->undecided, nund);
 }
 
 __global__ void k_go_emit(const uint32_t* __restrict__ best, uint32_t nt, const uint16_t* __restrict__ targets,
@@ -2277,6 +2282,7 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             st->exh_items += rounds ? round_items : hc.items + items1;
             st->exh_algo_ops += hc.algo;
             st->exh_probe_rejects += hc.probe_rejects + hc.join_probe_rej;
+            st->exh_undecided += hc.undecided;
             float ms[5];
             for (int i = 0; i < 5; i++) cudaEventElapsedTime(&ms[i], ctx->sev[i], ctx->sev[i + 1]);
             st->ms_fingerprint += ms[0];
@@ -2476,6 +2482,7 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
                 st->exh_items += c.items;
                 st->exh_algo_ops += c.algo;
                 st->exh_probe_rejects += c.probe_rejects + c.join_probe_rej;
+                st->exh_undecided += c.undecided;
                 float ms[5];
                 for (int i = 0; i < 5; i++) cudaEventElapsedTime(&ms[i], ctx->aev[6 * p + i], ctx->aev[6 * p + i + 1]);
                 st->ms_fingerprint += ms[0];

@@ -68,7 +68,7 @@ class Stats(ctypes.Structure):
                  "rules", "exh_states", "exh_items", "exh_algo_ops", "passes", "exh_probe_rejects")] + \
                [(n, ctypes.c_double) for n in ("ms_device", "ms_fingerprint", "ms_qc", "ms_exhaustive",
                                                "ms_exh_items", "ms_emit")] + \
-               [("graph_replays", ctypes.c_uint64)]
+               [("graph_replays", ctypes.c_uint64), ("exh_undecided", ctypes.c_uint64)]
 
     def as_dict(self):
         return {n: getattr(self, n) for n, _ in self._fields_}

@@ -15,7 +15,7 @@ import numpy as np
 from . import _lib
 
 STAT_SUM = ("targets", "pairs", "qc_hits", "mid_hits", "exh_checked", "exh_passed", "rules", "exh_states",
-            "exh_items", "exh_algo_ops", "exh_probe_rejects", "passes")
+            "exh_items", "exh_algo_ops", "exh_probe_rejects", "passes", "exh_undecided")
 STAT_MAX = ("ms_device", "ms_fingerprint", "ms_qc", "ms_exhaustive", "ms_exh_items", "ms_emit")
 
 

@@ -140,6 +140,9 @@ typedef struct m6502_stats {
                               earlier identical call (CUDA semantics, length-1
                               candidates; host targets are first copied to the
                               device), else 0 */
+    uint64_t exh_undecided; /* pairs ExhaustiveCheck left undecided: an output cone
+                              beyond 2^34 states (long sequences reading many
+                              registers under the full sweep); they yield no rule */
 } m6502_stats;
 
 /* ---- tuning ----

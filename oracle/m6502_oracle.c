@@ -858,6 +858,15 @@ uint64_t or_search_go(const uint16_t *targets, uint64_t n, int tlen, uint8_t dea
                     nthreads);
 }
 
+/* The Go worker with the ExhaustiveCheck sweep chosen (the reference's
+ * reduced sweep, or the full sweep of the GPU engine). */
+uint64_t or_search_go_sweep(const uint16_t *targets, uint64_t n, int tlen, uint8_t dead,
+                            int max_cand_len, int sweep, or_rule *out, uint64_t cap,
+                            or_stats *stats, int nthreads) {
+    return run_jobs(targets, n, tlen, dead, sweep, OR_STAGE_QC | OR_STAGE_EXH, OR_SEM_GO,
+                    max_cand_len, out, cap, stats, nthreads);
+}
+
 /* Target enumeration (cuda/6502_search_v2.cu:985-1037). */
 uint64_t or_enumerate_targets(int len, int first, int last, uint16_t *out, uint64_t cap) {
     uint16_t tab[OR_NUM_INSNS];

@@ -108,6 +108,10 @@ uint64_t or_search_cuda(const uint16_t *targets, uint64_t n, int tlen, uint8_t d
 uint64_t or_search_go(const uint16_t *targets, uint64_t n, int tlen, uint8_t dead,
                       int max_cand_len, or_rule *out, uint64_t cap, or_stats *stats,
                       int nthreads);
+/* The same with the sweep chosen (OR_SWEEP_REFERENCE or OR_SWEEP_FULL). */
+uint64_t or_search_go_sweep(const uint16_t *targets, uint64_t n, int tlen, uint8_t dead,
+                            int max_cand_len, int sweep, or_rule *out, uint64_t cap,
+                            or_stats *stats, int nthreads);
 
 /* All pruned length-L sequences in CUDA order whose first instruction index
  * lies in [first, last) (cuda/6502_search_v2.cu:985-1037).  Returns count;

@@ -61,6 +61,10 @@ def lib():
                                      ctypes.c_int, ctypes.c_int, ctypes.POINTER(Rule), ctypes.c_uint64,
                                      ctypes.POINTER(Stats), ctypes.c_int]
         L.or_search_go.restype = ctypes.c_uint64
+        L.or_search_go_sweep.restype = ctypes.c_uint64
+        L.or_search_go_sweep.argtypes = [u16p, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint8, ctypes.c_int,
+                                         ctypes.c_int, ctypes.POINTER(Rule), ctypes.c_uint64, ctypes.POINTER(Stats),
+                                         ctypes.c_int]
         L.or_search_go.argtypes = [u16p, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint8, ctypes.c_int,
                                    ctypes.POINTER(Rule), ctypes.c_uint64, ctypes.POINTER(Stats), ctypes.c_int]
         L.or_enumerate_targets.restype = ctypes.c_uint64
@@ -177,15 +181,15 @@ def search_cuda(targets, dead=0, sweep=SWEEP_REFERENCE, stages=7, max_cand_len=1
     return _rules_to_list(buf, k), st.as_dict()
 
 
-def search_go(targets, dead=0, max_cand_len=1, nthreads=None):
+def search_go(targets, dead=0, max_cand_len=1, nthreads=None, sweep=SWEEP_REFERENCE):
     t = np.ascontiguousarray(np.asarray(targets, dtype=np.uint16))
     n, tlen = t.shape
     nthreads = nthreads or os.cpu_count() or 1
     st = Stats()
     cap = 2 * n + 16
     buf = (Rule * cap)()
-    k = lib().or_search_go(t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), n, tlen, dead, max_cand_len,
-                           buf, cap, ctypes.byref(st), nthreads)
+    k = lib().or_search_go_sweep(t.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16)), n, tlen, dead, max_cand_len,
+                                 sweep, buf, cap, ctypes.byref(st), nthreads)
     return _rules_to_list(buf, min(k, cap)), st.as_dict()
 
 
