@@ -213,6 +213,10 @@ struct Counters {
     unsigned long long join_items;         // chunks of long length-2 equal ranges
     unsigned long long join_probe_rej;     // MidCheck survivors the join's probe rejected
     unsigned long long undecided;          // pairs left undecided (a cone beyond the sweep cap)
+    unsigned long long round_checked, round_items;   // Go-order rounds: pairs and work items, summed
+    unsigned long long surv1, items1;      // phase-1 survivors and work items (length-2 phase runs after)
+    unsigned long long surv_need, items_need;   // largest survivor / work-item counts seen, for the
+                                                // overflow check after the pass
 };
 
 struct Item {   // one chunk of a large cone sweep
@@ -1545,17 +1549,22 @@ __global__ void k_go_emit(const uint32_t* __restrict__ best, uint32_t nt, const 
 
 // Sort key of a survivor: target << 30 | masked pass << 29 | go_rank_of.
 
-__global__ void k_go_keys(const Surv* __restrict__ surv, const unsigned long long* n_ptr, uint64_t* __restrict__ keys) {
-    const uint64_t n = *n_ptr;
-    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+// Entries from the survivor count up to the capacity get `pad`, which sorts
+// after every real key.
+__global__ void k_go_keys(const Surv* __restrict__ surv, const unsigned long long* n_ptr, uint64_t cap, uint64_t pad,
+                          uint64_t* __restrict__ keys) {
+    const uint64_t n = min((uint64_t)*n_ptr, cap);
+    for (uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; p < cap; p += (uint64_t)gridDim.x * blockDim.x) {
+        if (p >= n) { keys[p] = pad; continue; }
         const Surv s = surv[p];
         keys[p] = ((uint64_t)s.t << 30) | ((uint64_t)((s.c & kSurvMasked) ? 1u : 0u) << 29) | go_rank_of(s.c);
     }
 }
 
 // Ordinal of each sorted survivor within its (target, kind) group.
-__global__ void k_go_ord(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* __restrict__ ord,
-                         Counters* __restrict__ cnt) {
+__global__ void k_go_ord(const uint64_t* __restrict__ keys, const unsigned long long* n_ptr, uint64_t cap,
+                         uint32_t* __restrict__ ord, Counters* __restrict__ cnt) {
+    const uint64_t n = min((uint64_t)*n_ptr, cap);
     unsigned long long mx = 0;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t g = keys[i] >> 29;
@@ -1572,9 +1581,13 @@ __global__ void k_go_ord(const uint64_t* __restrict__ keys, uint64_t n, uint32_t
 }
 
 // The survivors of one round, rebuilt as Surv records from their keys.
-__global__ void k_go_round(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ ord, uint64_t n,
-                           uint32_t lo, uint32_t hi, const uint32_t* __restrict__ best, uint32_t nt,
-                           Surv* __restrict__ out, Counters* __restrict__ cnt) {
+// A round whose first ordinal lies past the largest one finds nothing.
+__global__ void k_go_round(const uint64_t* __restrict__ keys, const uint32_t* __restrict__ ord,
+                           const unsigned long long* n_ptr, uint64_t cap, uint32_t lo, uint32_t hi,
+                           const uint32_t* __restrict__ best, uint32_t nt, Surv* __restrict__ out,
+                           Counters* __restrict__ cnt) {
+    if ((unsigned long long)lo > cnt->max_ord) return;
+    const uint64_t n = min((uint64_t)*n_ptr, cap);
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t o = ord[i];
         if (o < lo || o >= hi) continue;
@@ -1591,6 +1604,23 @@ __global__ void k_go_round(const uint64_t* __restrict__ keys, const uint32_t* __
         if (kind) code |= kSurvMasked;
         out[atomicAdd(&cnt->round_n, 1ull)] = Surv{t, code};
     }
+}
+
+// After a round: its pairs and work items join the totals; the largest
+// item count is kept for the overflow check after the pass.
+__global__ void k_go_tally(Counters* cnt) {
+    cnt->round_checked += cnt->round_n;
+    cnt->round_items += cnt->items;
+    cnt->items_need = max(cnt->items_need, cnt->items);
+}
+
+// Before the length-2 phase resets the survivor and item counters: the
+// first phase's counts are kept.
+__global__ void k_mark_phase(Counters* cnt) {
+    cnt->surv1 = cnt->surv;
+    cnt->items1 = cnt->items;
+    cnt->surv_need = max(cnt->surv_need, cnt->surv);
+    cnt->items_need = max(cnt->items_need, cnt->items);
 }
 
 // Pairwise QC / MidCheck / FlagDiff: warp per pair, lane = vector.
@@ -1786,6 +1816,13 @@ struct m6502_ctx {
         bool broken = false;         // recording failed once: launch directly from then on
         std::string why;             // the error that stopped recording
     } graph;
+    struct PassGraph {         // one recorded pass of the pass-by-pass path (Go semantics,
+        cudaGraphExec_t exec = nullptr;   // length-2 candidates, enumeration)
+        std::vector<uint64_t> key;
+        uint64_t stamp = 0;
+    };
+    PassGraph pass_graphs[8];
+    uint64_t pass_graph_clock = 0;
     DevBuf cnt_slots;          // Counters of the queued passes
     DevBuf tall;               // host targets of a queued search, copied to the device at once
     DevBuf opflag;             // k_check_ops result
@@ -2042,27 +2079,59 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
     uint64_t icap = std::max<uint64_t>(ctx->items.bytes / sizeof(Item), 1u << 16);
     uint64_t rcap = std::max<uint64_t>(ctx->rules.bytes / sizeof(m6502_rule), nt / 2 + 4096);
     uint64_t jcap = std::max<uint64_t>(ctx->jitems.bytes / sizeof(JoinItem), 1u << 16);
+    m6502_ctx::Cand2Table *c2 = nullptr, *c2e = nullptr;   // sorted length-2 candidate keys (cached per mask)
+    if (cfg.max_cand_len >= 2) {
+        if (go && dead) TRY(cand2_table(ctx, 0, &c2e));   // unmasked table for targets with only that pass open
+        TRY(cand2_table(ctx, dead, &c2));
+        if (!c2e) c2e = c2;
+    }
+    const bool scan = (cfg.flags & M6502_QC_SCAN) != 0;
+    const bool count_only = (cfg.flags & M6502_COUNT_ONLY) != 0;
+    const bool exh = (stages & M6502_CHECK_EXH) != 0;
+    const bool rounds = go && exh;   // Go semantics: verify in Go order, stop at the first pass
+    const bool phase2 = cfg.max_cand_len >= 2;
+    if (!scan) TRY(join_table(ctx, dead));
     for (int attempt = 0; attempt < 6; attempt++) {
+        // Every buffer the pass uses is allocated here, so that the launches
+        // below can be recorded as one CUDA graph and replayed.
         TRY(ensure(ctx, ctx->surv, scap * sizeof(Surv)));
         TRY(ensure(ctx, ctx->fail, scap * sizeof(uint32_t)));
         TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
         TRY(ensure(ctx, ctx->rules, rcap * sizeof(m6502_rule)));
         if (go) TRY(ensure(ctx, ctx->best, 2 * nt * sizeof(uint32_t)));
+        int end_bit = 30;   // Go-order sort keys: target << 30 | pass << 29 | rank
+        while (end_bit < 63 && (nt >> (end_bit - 30)) != 0) end_bit++;
+        if (rounds) {
+            TRY(ensure(ctx, ctx->go_keys, scap * 8));
+            TRY(ensure(ctx, ctx->go_keys2, scap * 8));
+            TRY(ensure(ctx, ctx->go_ord, scap * 4));
+            TRY(ensure(ctx, ctx->go_round, scap * sizeof(Surv)));
+            size_t tb = 0;
+            CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, (const uint64_t*)nullptr, (uint64_t*)nullptr, (int)scap, 0,
+                                              end_bit, ctx->stream));
+            TRY(ensure(ctx, ctx->go_sort_tmp, tb));
+        }
+        if (phase2) TRY(ensure(ctx, ctx->jitems, jcap * sizeof(JoinItem)));
+        const uint64_t rlim = count_only ? 0 : rcap;   // emit kernels count past rlim without writing
         Counters* cnt = (Counters*)ctx->cnt.p;
+        bool capturing = false;
+        // Stage events: inside a capture they must be external record nodes.
+        auto rec = [&](cudaEvent_t e) -> cudaError_t {
+            return capturing ? cudaEventRecordWithFlags(e, ctx->stream, cudaEventRecordExternal)
+                             : cudaEventRecord(e, ctx->stream);
+        };
+        // All launches of one pass, with no host read-back in between.
+        auto enqueue = [&]() -> int {
         CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), ctx->stream));
-        CK(cudaEventRecord(ctx->sev[0], ctx->stream));
-        const bool scan = (cfg.flags & M6502_QC_SCAN) != 0;
+        CK(rec(ctx->sev[0]));
         if (scan || cfg.max_cand_len >= 2) {   // the join computes its targets' outputs itself
             k_fingerprint<FixedSeqs><<<ctx->fp_blocks, 256, 0, ctx->stream>>>(
                 FixedSeqs{d_targets, tlen}, nt, (uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p);
             CKL("k_fingerprint(targets)");
         }
-        CK(cudaEventRecord(ctx->sev[1], ctx->stream));
+        CK(rec(ctx->sev[1]));
         uint32_t qgrid = (uint32_t)std::min<uint64_t>(ctx->qc_blocks, (nt + kQcTile - 1) / kQcTile);
-        const bool count_only = (cfg.flags & M6502_COUNT_ONLY) != 0;
-        const uint64_t rlim = count_only ? 0 : rcap;   // emit kernels count past rlim without writing
         if (!scan) {
-            TRY(join_table(ctx, dead));
             uint32_t jgrid = (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8, (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
             const uint64_t* jk = (const uint64_t*)ctx->join_keys[dead].p;
             const uint16_t* ji = (const uint16_t*)ctx->join_idx[dead].p;
@@ -2089,93 +2158,60 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
                                                          (uint8_t*)ctx->cmeta1.p, dead, stages,
                                                          (Surv*)ctx->surv.p, scap, cnt);
         CKL("k_qc1");
-        CK(cudaEventRecord(ctx->sev[2], ctx->stream));
-        const bool exh = (stages & M6502_CHECK_EXH) != 0;
-        const bool rounds = go && exh;   // Go semantics: verify in Go order, stop at the first pass
+        CK(rec(ctx->sev[2]));
         SurvSource src{(const Surv*)ctx->surv.p, d_targets, tlen, dead, go ? 1 : 0};
         ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep, cfg.exh_mode == M6502_EXH_BRUTE};
-        uint64_t round_checked = 0, round_items = 0;
-        bool grow = false;
         // Go-order verification rounds over the survivors in ctx->surv; on
         // return `best` holds the first passing candidate per target and pass.
-        auto go_rounds = [&]() -> int {
-            unsigned long long ns = 0;
-            CK(cudaMemcpyAsync(&ns, &cnt->surv, sizeof ns, cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
-            if (ns > scap) { scap = ns + ns / 4 + 1024; grow = true; return M6502_OK; }
-            if (ns == 0) return M6502_OK;
-            TRY(ensure(ctx, ctx->go_keys, ns * 8));
-            TRY(ensure(ctx, ctx->go_keys2, ns * 8));
-            TRY(ensure(ctx, ctx->go_ord, ns * 4));
-            TRY(ensure(ctx, ctx->go_round, ns * sizeof(Surv)));
-            int end_bit = 30;
-            while (end_bit < 64 && (nt >> (end_bit - 30)) != 0) end_bit++;
-            size_t tb = 0;
-            CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, (const uint64_t*)nullptr, (uint64_t*)nullptr, (int)ns, 0,
-                                              end_bit, ctx->stream));
-            TRY(ensure(ctx, ctx->go_sort_tmp, tb));
-            k_go_keys<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv,
+        // Go-order verification rounds over the survivors in ctx->surv, queued
+        // with no read-back: the survivors are sorted over the buffer's whole
+        // capacity (entries past the device's count get a key that sorts last),
+        // and every round a group of `bound` candidates could need is launched;
+        // a round past the largest ordinal finds nothing to do.  On return
+        // `best` holds the first passing candidate per target and pass; the
+        // rounds' pair and item counts are summed on the device.
+        auto go_rounds = [&](uint64_t bound) -> int {
+            const uint64_t pad = (1ull << end_bit) - 1;   // above every real key (target < nt)
+            k_go_keys<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->surv.p, &cnt->surv, scap, pad,
                                                              (uint64_t*)ctx->go_keys.p);
             CKL("k_go_keys");
-            tb = ctx->go_sort_tmp.bytes;
+            size_t tb = ctx->go_sort_tmp.bytes;
             CK(cub::DeviceRadixSort::SortKeys(ctx->go_sort_tmp.p, tb, (const uint64_t*)ctx->go_keys.p,
-                                              (uint64_t*)ctx->go_keys2.p, (int)ns, 0, end_bit, ctx->stream));
+                                              (uint64_t*)ctx->go_keys2.p, (int)scap, 0, end_bit, ctx->stream));
             CK(cudaMemsetAsync(&cnt->max_ord, 0, sizeof(unsigned long long), ctx->stream));
-            k_go_ord<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const uint64_t*)ctx->go_keys2.p, ns,
+            k_go_ord<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const uint64_t*)ctx->go_keys2.p, &cnt->surv, scap,
                                                             (uint32_t*)ctx->go_ord.p, cnt);
             CKL("k_go_ord");
-            unsigned long long max_ord = 0;
-            CK(cudaMemcpyAsync(&max_ord, &cnt->max_ord, sizeof max_ord, cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
             SurvSource rs{(const Surv*)ctx->go_round.p, d_targets, tlen, dead, 1};
-            uint64_t lo = 0, blk = 64;
-            while (lo <= max_ord) {
-                const uint64_t hi = lo + blk;
+            for (uint64_t lo = 0, blk = 64; lo < bound; lo += blk, blk = std::min<uint64_t>(blk * 2, 1ull << 22)) {
+                const uint64_t hi = std::min<uint64_t>(lo + blk, 0xFFFFFFFFull);
                 CK(cudaMemsetAsync(&cnt->round_n, 0, sizeof(unsigned long long), ctx->stream));
                 k_go_round<<<ctx->sms * 8, 256, 0, ctx->stream>>>(
-                    (const uint64_t*)ctx->go_keys2.p, (const uint32_t*)ctx->go_ord.p, ns, (uint32_t)lo,
-                    (uint32_t)std::min<uint64_t>(hi, 0xFFFFFFFFull), (const uint32_t*)ctx->best.p, (uint32_t)nt,
-                    (Surv*)ctx->go_round.p, cnt);
+                    (const uint64_t*)ctx->go_keys2.p, (const uint32_t*)ctx->go_ord.p, &cnt->surv, scap, (uint32_t)lo,
+                    (uint32_t)hi, (const uint32_t*)ctx->best.p, (uint32_t)nt, (Surv*)ctx->go_round.p, cnt);
                 CKL("k_go_round");
-                unsigned long long cnts[2] = {0, 0};
-                for (int attempt = 0;; attempt++) {
-                    // exhaustive tickets, work items and item tickets restart each round
-                    CK(cudaMemsetAsync(&cnt->exh_ticket, 0, 3 * sizeof(unsigned long long), ctx->stream));
-                    ExhArgs ra{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep,
-                               cfg.exh_mode == M6502_EXH_BRUTE};
-                    TRY(launch_exh(ctx, rs, &cnt->round_n, ns, ra));
-                    TRY(launch_items(ctx, rs, ra));
-                    CK(cudaMemcpyAsync(&cnts[0], &cnt->items, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                                       ctx->stream));
-                    CK(cudaMemcpyAsync(&cnts[1], &cnt->round_n, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
-                                       ctx->stream));
-                    CK(cudaStreamSynchronize(ctx->stream));
-                    if (cnts[0] <= icap) break;
-                    if (attempt >= 4) return set_err(ctx, M6502_E_NOMEM, "work-item queue kept overflowing");
-                    icap = cnts[0] + cnts[0] / 4 + 1024;
-                    TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
-                }
-                k_go_select<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->go_round.p, &cnt->round_n, ns,
+                // exhaustive tickets, work items and item tickets restart each round
+                CK(cudaMemsetAsync(&cnt->exh_ticket, 0, 3 * sizeof(unsigned long long), ctx->stream));
+                ExhArgs ra{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep,
+                           cfg.exh_mode == M6502_EXH_BRUTE};
+                TRY(launch_exh(ctx, rs, &cnt->round_n, scap, ra));
+                TRY(launch_items(ctx, rs, ra));
+                k_go_select<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const Surv*)ctx->go_round.p, &cnt->round_n, scap,
                                                                    (const uint32_t*)ctx->fail.p, (uint32_t)nt,
                                                                    (uint32_t*)ctx->best.p, cnt, d_targets, tlen,
                                                                    cfg.sweep);
                 CKL("k_go_select");
-                round_checked += cnts[1];
-                round_items += cnts[0];
-                lo = hi;
-                blk = std::min<uint64_t>(blk * 2, 1ull << 22);
+                k_go_tally<<<1, 1, 0, ctx->stream>>>(cnt);
+                CKL("k_go_tally");
             }
             return M6502_OK;
         };
         if (go) CK(cudaMemsetAsync(ctx->best.p, 0xFF, 2 * nt * sizeof(uint32_t), ctx->stream));
         if (exh && !rounds) TRY(launch_exh(ctx, src, &cnt->surv, scap, ea));
-        if (rounds) {
-            TRY(go_rounds());
-            if (grow) continue;
-        }
-        CK(cudaEventRecord(ctx->sev[3], ctx->stream));
+        if (rounds) TRY(go_rounds(kNumInsns));   // a target has at most 2,863 length-1 candidates
+        CK(rec(ctx->sev[3]));
         if (exh && !rounds) TRY(launch_items(ctx, src, ea));
-        CK(cudaEventRecord(ctx->sev[4], ctx->stream));
+        CK(rec(ctx->sev[4]));
         // Passing survivors -> Go winners (best) or rules (CUDA semantics).
         auto select_or_emit = [&]() -> int {
             if (rounds) return M6502_OK;   // the rounds selected already
@@ -2196,32 +2232,19 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             return M6502_OK;
         };
         TRY(select_or_emit());
-        CK(cudaEventRecord(ctx->sev[5], ctx->stream));
-        const bool phase2 = cfg.max_cand_len >= 2;
-        Counters hc;
-        bool redo = false;
-        uint64_t surv1 = 0, items1 = 0;   // phase-1 survivors and work items
+        CK(rec(ctx->sev[5]));
         if (phase2) {
-            // Length-2 candidates (worker.go:122: candidate lengths 1..max).
-            CK(cudaMemcpyAsync(&hc, cnt, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream));
-            CK(cudaStreamSynchronize(ctx->stream));
-            if (hc.surv > scap) { scap = hc.surv + hc.surv / 4 + 1024; redo = true; }
-            if (hc.items > icap) { icap = hc.items + hc.items / 4 + 1024; redo = true; }
-            if (hc.rules > rlim && !count_only) { rcap = hc.rules + hc.rules / 4 + 1024; redo = true; }
-            if (redo) continue;
-            surv1 = hc.surv;
-            items1 = hc.items;
-            m6502_ctx::Cand2Table *c2 = nullptr, *c2e = nullptr;
-            if (go && dead) TRY(cand2_table(ctx, 0, &c2e));   // unmasked table for targets with only that pass open
-            TRY(cand2_table(ctx, dead, &c2));
-            if (!c2e) c2e = c2;
+            // Length-2 candidates (worker.go:122: candidate lengths 1..max).  The
+            // phase-1 counts are kept on the device; buffer overflows of either
+            // phase are checked once, after the pass.
+            k_mark_phase<<<1, 1, 0, ctx->stream>>>(cnt);
+            CKL("k_mark_phase");
             // survivor, exhaustive-ticket and work-item counters restart for this phase
             CK(cudaMemsetAsync(&cnt->surv, 0, 4 * sizeof(unsigned long long), ctx->stream));
-            CK(cudaEventRecord(ctx->sev2[0], ctx->stream));
+            CK(rec(ctx->sev2[0]));
             const uint32_t jgrid2 =
                 (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8, (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
             const uint32_t n2 = (uint32_t)kNumInsns * (uint32_t)kNumInsns;
-            TRY(ensure(ctx, ctx->jitems, jcap * sizeof(JoinItem)));
             CK(cudaMemsetAsync(&cnt->join_items, 0, sizeof(unsigned long long), ctx->stream));
             Join2Args ja{(const uint64_t*)ctx->tfp.p, (const uint8_t*)ctx->tmeta.p, (uint32_t)nt,
                          (const uint64_t*)c2->keys.p, (const uint32_t*)c2->idx.p, (const uint64_t*)c2e->keys.p,
@@ -2235,30 +2258,86 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
                 k_qc_join2_items<false><<<ctx->sms * 8, 256, 0, ctx->stream>>>(ja);
             }
             CKL("k_qc_join2");
-            CK(cudaEventRecord(ctx->sev2[1], ctx->stream));
+            CK(rec(ctx->sev2[1]));
             if (exh && !rounds) TRY(launch_exh(ctx, src, &cnt->surv, scap, ea));
-            if (rounds) {
-                TRY(go_rounds());
-                if (grow) continue;
-            }
-            CK(cudaEventRecord(ctx->sev2[2], ctx->stream));
+            if (rounds) TRY(go_rounds((uint64_t)kNumInsns * kNumInsns));
+            CK(rec(ctx->sev2[2]));
             if (exh && !rounds) TRY(launch_items(ctx, src, ea));
-            CK(cudaEventRecord(ctx->sev2[3], ctx->stream));
+            CK(rec(ctx->sev2[3]));
             TRY(select_or_emit());
-            CK(cudaEventRecord(ctx->sev2[4], ctx->stream));
+            CK(rec(ctx->sev2[4]));
         }
-        if (!phase2) CK(cudaEventRecord(ctx->sev2[4], ctx->stream));
+        if (!phase2) CK(rec(ctx->sev2[4]));
         if (go) {
             k_go_emit<<<ctx->sms * 8, 256, 0, ctx->stream>>>((const uint32_t*)ctx->best.p, (uint32_t)nt,
                                                              d_targets, tlen, d_ids,
                                                              (m6502_rule*)ctx->rules.p, rlim, cnt);
             CKL("k_go_emit");
         }
-        CK(cudaEventRecord(ctx->sev2[5], ctx->stream));
+        CK(rec(ctx->sev2[5]));
+        return M6502_OK;
+        };   // enqueue
+        // One recorded graph per pass configuration (a few kept); an identical
+        // later pass replays it.
+        bool launched = false;
+        if (!(cfg.flags & M6502_NO_GRAPH) && !ctx->graph.broken) {
+            const std::vector<uint64_t> key = {
+                (uint64_t)(uintptr_t)d_targets, nt, tlen, (uint64_t)(uintptr_t)d_ids, cfg.semantics, cfg.sweep,
+                cfg.exh_mode, stages, cfg.flags, dead, cfg.max_cand_len, scap, icap, rcap, jcap,
+                (uint64_t)(uintptr_t)ctx->surv.p, (uint64_t)(uintptr_t)ctx->fail.p, (uint64_t)(uintptr_t)ctx->items.p,
+                (uint64_t)(uintptr_t)ctx->rules.p, (uint64_t)(uintptr_t)ctx->cnt.p, (uint64_t)(uintptr_t)ctx->best.p,
+                (uint64_t)(uintptr_t)ctx->tfp.p, (uint64_t)(uintptr_t)ctx->tmeta.p,
+                (uint64_t)(uintptr_t)ctx->go_keys.p, (uint64_t)(uintptr_t)ctx->go_keys2.p,
+                (uint64_t)(uintptr_t)ctx->go_ord.p, (uint64_t)(uintptr_t)ctx->go_round.p,
+                (uint64_t)(uintptr_t)ctx->go_sort_tmp.p, ctx->go_sort_tmp.bytes, (uint64_t)(uintptr_t)ctx->jitems.p,
+                (uint64_t)(uintptr_t)ctx->join_keys[dead].p, c2 ? (uint64_t)(uintptr_t)c2->keys.p : 0,
+                c2e ? (uint64_t)(uintptr_t)c2e->keys.p : 0, ctx->tune.exh_minb, ctx->tune.ticket_batch,
+                ctx->tune.chunk_log2, ctx->tune.join_probe};
+            m6502_ctx::PassGraph* pg = nullptr;
+            for (m6502_ctx::PassGraph& g : ctx->pass_graphs)
+                if (g.exec && g.key == key) pg = &g;
+            if (!pg) {   // record: the least recently used slot is replaced
+                pg = &ctx->pass_graphs[0];
+                for (m6502_ctx::PassGraph& g : ctx->pass_graphs)
+                    if (g.stamp < pg->stamp) pg = &g;
+                if (pg->exec) { cudaGraphExecDestroy(pg->exec); pg->exec = nullptr; }
+                cudaGraph_t g = nullptr;
+                bool ok = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+                if (ok) {
+                    capturing = true;
+                    const int rc = enqueue();
+                    capturing = false;
+                    ok = cudaStreamEndCapture(ctx->stream, &g) == cudaSuccess && rc == M6502_OK && g;
+                    ok = ok && cudaGraphInstantiate(&pg->exec, g, 0) == cudaSuccess;
+                    if (g) cudaGraphDestroy(g);
+                }
+                if (!ok) {
+                    pg->exec = nullptr;
+                    ctx->graph.broken = true;
+                    ctx->graph.why = cudaGetErrorString(cudaGetLastError());   // clears the launch error
+                    set_err(ctx, M6502_OK, "CUDA graph recording failed (" + ctx->graph.why +
+                                               "); passes are launched directly");
+                } else {
+                    pg->key = key;
+                }
+            } else if (st) {
+                st->graph_replays = 1;
+            }
+            if (pg->exec) {
+                pg->stamp = ++ctx->pass_graph_clock;
+                CK(cudaGraphLaunch(pg->exec, ctx->stream));
+                launched = true;
+            }
+        }
+        if (!launched) TRY(enqueue());
+        Counters hc;
+        bool redo = false;
         CK(cudaMemcpyAsync(&hc, cnt, sizeof hc, cudaMemcpyDeviceToHost, ctx->stream));
         CK(cudaStreamSynchronize(ctx->stream));
-        if (hc.surv > scap) { scap = hc.surv + hc.surv / 4 + 1024; redo = true; }
-        if (hc.items > icap) { icap = hc.items + hc.items / 4 + 1024; redo = true; }
+        const uint64_t surv_need = std::max<uint64_t>(hc.surv, hc.surv_need);
+        const uint64_t items_need = std::max<uint64_t>(hc.items, hc.items_need);
+        if (surv_need > scap) { scap = surv_need + surv_need / 4 + 1024; redo = true; }
+        if (items_need > icap) { icap = items_need + items_need / 4 + 1024; redo = true; }
         if (hc.rules > rlim && !count_only) { rcap = hc.rules + hc.rules / 4 + 1024; redo = true; }
         if (hc.join_items > jcap) { jcap = hc.join_items + hc.join_items / 4 + 1024; redo = true; }
         if (redo) continue;
@@ -2275,11 +2354,11 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             st->pairs += nt * ((uint64_t)kNumInsns + (phase2 ? (uint64_t)kNumInsns * kNumInsns : 0u));
             st->qc_hits += hc.qc;
             st->mid_hits += hc.mid;
-            st->exh_checked += !exh ? 0 : rounds ? round_checked : hc.surv + surv1 + hc.join_probe_rej;
+            st->exh_checked += !exh ? 0 : rounds ? hc.round_checked : hc.surv + hc.surv1 + hc.join_probe_rej;
             st->exh_passed += hc.exh_pass;
             st->rules += hc.rules;
             st->exh_states += hc.states;
-            st->exh_items += rounds ? round_items : hc.items + items1;
+            st->exh_items += rounds ? hc.round_items : hc.items + hc.items1;
             st->exh_algo_ops += hc.algo;
             st->exh_probe_rejects += hc.probe_rejects + hc.join_probe_rej;
             st->exh_undecided += hc.undecided;
@@ -2698,6 +2777,8 @@ void m6502_destroy(m6502_ctx* ctx) {
     for (cudaEvent_t e : ctx->sev2) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->aev) if (e) cudaEventDestroy(e);
     if (ctx->graph.exec) cudaGraphExecDestroy(ctx->graph.exec);
+    for (m6502_ctx::PassGraph& g : ctx->pass_graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
     for (auto& t : ctx->cand2) {
         if (t.keys.p) cudaFree(t.keys.p);
         if (t.idx.p) cudaFree(t.idx.p);
