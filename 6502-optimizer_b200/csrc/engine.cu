@@ -907,7 +907,10 @@ __global__ void __launch_bounds__(256) k_qc1(const uint64_t* __restrict__ tfp, c
 // QuickCheck passes.
 // Lane v checks vector v from the candidate-major fingerprints (cfp_cm,
 // 256 contiguous bytes per candidate).  Same survivors as k_qc1.
-template <bool GO>
+// PROBE: the random-state probe of MidCheck survivors runs here (CUDA
+// semantics only; a separate instantiation, so that the join without it
+// keeps its registers).
+template <bool GO, bool PROBE = false>
 __global__ void __launch_bounds__(256, 4) k_qc_join(const uint16_t* __restrict__ targets, uint32_t tlen,
                                                   uint32_t nt, const uint64_t* __restrict__ cfp_cm,
                                                   const uint8_t* __restrict__ cmeta, const uint64_t* __restrict__ skeys,
@@ -915,7 +918,7 @@ __global__ void __launch_bounds__(256, 4) k_qc_join(const uint16_t* __restrict__
                                                   uint32_t stages, Surv* __restrict__ surv, uint64_t cap,
                                                   Counters* __restrict__ cnt, uint32_t probe) {
     __shared__ uint64_t s_key[kNumInsns];
-    __shared__ uint64_t s_tprobe[kWarpsPerBlock][2][32];   // target outputs on the probe states
+    __shared__ uint64_t s_tprobe[PROBE ? kWarpsPerBlock : 1][2][32];   // target outputs on the probe states
     __shared__ uint16_t s_idx[kNumInsns];
     __shared__ uint8_t s_meta[kNumInsns];
     __shared__ uint16_t s_dir[(1u << kDirBits) + 1];
@@ -1021,7 +1024,7 @@ __global__ void __launch_bounds__(256, 4) k_qc_join(const uint16_t* __restrict__
                     nqc += lane == 0;
                     const bool mid = !(stages & M6502_CHECK_MID) || lo_eq == kFull;
                     if (mid) { nmid += lane == 0; pass = true; }
-                    if (pass && probe) {
+                    if (PROBE && pass && probe) {
                         if (!tp_ready) {
                             tp_sw = __reduce_or_sync(kFull, lane < (int)tlen ? (uint32_t)c_sweep[ins & 0xFFu] : 0u);
                             for (int r = 0; r < 2; r++) {
@@ -1914,6 +1917,25 @@ int launch_exh(m6502_ctx* ctx, const SurvSource& src, const unsigned long long* 
     return M6502_OK;
 }
 
+// The length-1 QuickCheck join under CUDA semantics, with the probe of its
+// MidCheck survivors when `probe` (1 + the sweep mode) is set.
+int launch_join1(m6502_ctx* ctx, const uint16_t* d_t, uint32_t tlen, uint64_t nt, uint32_t dead, uint32_t stages,
+                 uint64_t scap, Counters* cnt, uint32_t probe) {
+    const uint32_t jgrid = (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8, (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
+    const uint64_t* jk = (const uint64_t*)ctx->join_keys[dead].p;
+    const uint16_t* ji = (const uint16_t*)ctx->join_idx[dead].p;
+    if (probe)
+        k_qc_join<false, true><<<jgrid, 256, 0, ctx->stream>>>(d_t, tlen, (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p,
+                                                                 (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
+                                                                 dead, stages, (Surv*)ctx->surv.p, scap, cnt, probe);
+    else
+        k_qc_join<false, false><<<jgrid, 256, 0, ctx->stream>>>(d_t, tlen, (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p,
+                                                                  (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
+                                                                  dead, stages, (Surv*)ctx->surv.p, scap, cnt, 0u);
+    CKL("k_qc_join");
+    return M6502_OK;
+}
+
 // Items of survivor pairs, with the work-item size of the knobs (the items
 // were cut by launch_exh with the same size).
 int launch_items(m6502_ctx* ctx, const SurvSource& src, ExhArgs ea) {
@@ -2141,12 +2163,8 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
                                                                 (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
                                                                 dead, stages, (Surv*)ctx->surv.p, scap, cnt, 0u);
             else
-                k_qc_join<false><<<jgrid, 256, 0, ctx->stream>>>(d_targets, tlen,
-                                                                 (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p,
-                                                                 (uint8_t*)ctx->cmeta1.p, jk, ji, ctx->join_n[dead],
-                                                                 dead, stages, (Surv*)ctx->surv.p, scap, cnt,
-                                                                 (ctx->tune.join_probe && (stages & M6502_CHECK_EXH))
-                                                                     ? 1u + cfg.sweep : 0u);
+                TRY(launch_join1(ctx, d_targets, tlen, nt, dead, stages, scap, cnt,
+                                 (ctx->tune.join_probe && exh) ? 1u + cfg.sweep : 0u));
         } else if (go)
             k_qc1<true><<<qgrid, 256, 0, ctx->stream>>>((uint64_t*)ctx->tfp.p, (uint8_t*)ctx->tmeta.p,
                                                         (uint32_t)nt, (uint64_t*)ctx->cfp1.p,
@@ -2451,14 +2469,8 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
                                                                  (Surv*)ctx->surv.p, scap, cnt);
                     CKL("k_qc1");
                 } else {
-                    const uint32_t jgrid = (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8,
-                                                                        (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
-                    k_qc_join<false><<<jgrid, 256, 0, ctx->stream>>>(
-                        d_t, tlen, (uint32_t)nt, (uint64_t*)ctx->cfp1cm.p, (uint8_t*)ctx->cmeta1.p,
-                        (const uint64_t*)ctx->join_keys[dead].p, (const uint16_t*)ctx->join_idx[dead].p,
-                        ctx->join_n[dead], dead, stages, (Surv*)ctx->surv.p, scap, cnt,
-                        (ctx->tune.join_probe && exh) ? 1u + cfg.sweep : 0u);
-                    CKL("k_qc_join");
+                    TRY(launch_join1(ctx, d_t, tlen, nt, dead, stages, scap, cnt,
+                                     (ctx->tune.join_probe && exh) ? 1u + cfg.sweep : 0u));
                 }
                 CK(rec(ev[2]));
                 SurvSource src{(const Surv*)ctx->surv.p, d_t, tlen, dead, 0};

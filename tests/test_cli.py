@@ -187,10 +187,11 @@ def test_verify_jsonl_rejects_a_corrupted_rule(cli, full_jsonl, tmp_path):
 @pytest.mark.gpu
 def test_verify_jsonl_reports_undecided(cli, tmp_path):
     """A rule whose full sweep exceeds the engine's per-cone cap is reported
-    UNDECIDED, not FAIL, and the command exits non-zero.  Here A ends up
-    depending on A, carry, X, Y, M, S and S0 (2^49 states under the full
-    sweep); the replacement appends a NOP, so no sampled state differs."""
-    src = "TXA : ADC M : STA M : TYA : ADC M : STA M : PLA : ADC M"
+    UNDECIDED, not FAIL, and the command exits non-zero.  Here the final A
+    depends on A, X, Y, M, S0 and carry (a cone of 2^41 states under the full
+    sweep, above the 2^34 cap); the replacement appends a NOP, so no sampled
+    state differs."""
+    src = "ADC M : STA M : TXA : ADC M : STA M : TYA : ADC M : STA M : PLA : ADC M"
     f = tmp_path / "u.jsonl"
     f.write_text(json.dumps({"source_asm": src, "replacement_asm": src + " : NOP"}) + "\n")
     r = run(cli, "verify-jsonl", str(f), "--sweep", "full")
