@@ -2694,7 +2694,8 @@ bool tune_load(const m6502_ctx* ctx, const std::string& path, m6502_tune* out) {
     return true;
 }
 
-void tune_save(const m6502_ctx* ctx, const std::string& path, const m6502_tune& t, double ms) {
+void tune_save(const m6502_ctx* ctx, const std::string& path, const m6502_tune& t, double ms,
+               const std::vector<std::pair<m6502_tune, double>>& tried) {
     const size_t slash = path.rfind('/');
     if (slash != std::string::npos && slash > 0) {   // create the directory chain
         for (size_t p = path.find('/', 1); p != std::string::npos && p <= slash; p = path.find('/', p + 1))
@@ -2707,6 +2708,9 @@ void tune_save(const m6502_ctx* ctx, const std::string& path, const m6502_tune& 
                  kTuneVersion);
     std::fprintf(f, "exh_minb=%u\nticket_batch=%u\nchunk_log2=%u\njoin_probe=%u\nms=%.4f\n", t.exh_minb,
                  t.ticket_batch, t.chunk_log2, t.join_probe, ms);
+    for (const auto& tr : tried)   // every configuration timed, in order
+        std::fprintf(f, "# tried exh_minb=%u ticket_batch=%u chunk_log2=%u join_probe=%u ms=%.4f\n",
+                     tr.first.exh_minb, tr.first.ticket_batch, tr.first.chunk_log2, tr.first.join_probe, tr.second);
     std::fclose(f);
     std::rename(tmp.c_str(), path.c_str());   // readers see the old file or the whole new one
 }
@@ -3098,6 +3102,7 @@ int m6502_autotune(m6502_ctx* ctx, const char* cache_path, uint32_t flags, m6502
     cfg.exh_mode = M6502_EXH_CONES;
     cfg.max_cand_len = 1;
     cfg.flags = M6502_TARGETS_ON_DEVICE | M6502_COUNT_ONLY;
+    std::vector<std::pair<m6502_tune, double>> tried;
     // median of three timed runs after one untimed run (which records the graph)
     auto measure = [&](const m6502_tune& t, double* ms) -> int {
         TRY(m6502_tune_set(ctx, &t));
@@ -3110,6 +3115,7 @@ int m6502_autotune(m6502_ctx* ctx, const char* cache_path, uint32_t flags, m6502
         }
         std::sort(v, v + 3);
         *ms = v[1];
+        tried.emplace_back(t, v[1]);
         return M6502_OK;
     };
     m6502_tune best = ctx->tune;
@@ -3138,7 +3144,7 @@ int m6502_autotune(m6502_ctx* ctx, const char* cache_path, uint32_t flags, m6502
     tg.p = nullptr;
     TRY(rc);
     TRY(m6502_tune_set(ctx, &best));
-    if (!path.empty()) tune_save(ctx, path, best, best_ms);   // a cache that cannot be written is not an error
+    if (!path.empty()) tune_save(ctx, path, best, best_ms, tried);   // a cache that cannot be written is not an error
     if (chosen) *chosen = best;
     if (ms_out) *ms_out = best_ms;
     return M6502_OK;

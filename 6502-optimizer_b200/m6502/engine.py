@@ -77,6 +77,21 @@ class Engine:
                 setattr(t, k, int(v))
             self._check(self._L.m6502_tune_set(self._ctx, ctypes.byref(t)))
 
+    @staticmethod
+    def tune_trace(cache_path):
+        """The configurations m6502_autotune timed, as written to its cache
+        file: a list of dicts (the knobs and the median ms of each)."""
+        out = []
+        try:
+            with open(cache_path) as f:
+                for line in f:
+                    if line.startswith("# tried "):
+                        out.append({k: (float(v) if k == "ms" else int(v))
+                                    for k, v in (x.split("=") for x in line[8:].split())})
+        except OSError:
+            pass
+        return out
+
     def autotune(self, cache_path=None, force=False):
         """Picks the knobs for this device by timing them (or reads them from the
         device's tuning cache); returns (knobs, ms of the chosen configuration on

@@ -226,11 +226,14 @@ def run_engine(args):
     eng = m6502.Engine(device=local)
     # the scheduling knobs for this device: the tuning cache if one exists,
     # else timed now (m6502_autotune), before anything is measured
+    tune_path = os.environ.get("M6502_TUNE_CACHE") or os.path.expanduser(
+        "~/.cache/m6502/bench-tune-" + "".join(c if c.isalnum() else "_" for c in
+                                              torch.cuda.get_device_properties(local).name) + ".txt")
     if args.tune == "default":
         eng.tune = _lib.TUNE_DEFAULT
         tuned, tune_ms, tune_source = eng.tune, 0.0, "default"
     else:
-        tuned, tune_ms = eng.autotune(force=args.tune == "force")
+        tuned, tune_ms = eng.autotune(cache_path=tune_path, force=args.tune == "force")
         tune_source = "timed" if tune_ms > 0 else "cache"
     stream = torch.cuda.ExternalStream(eng.stream, device=local)
     d_targets = torch.from_numpy(shard.view(np.int16)).to(f"cuda:{local}")
@@ -374,7 +377,8 @@ def run_engine(args):
             # opcode check of the targets
             "gpu_launches": int((4 * s0["passes"] + 1) * args.steps),
         }
-        line["config"]["tuning"] = dict(tuned, source=tune_source, calibration_ms=tune_ms)
+        line["config"]["tuning"] = dict(tuned, source=tune_source, calibration_ms=tune_ms,
+                                        trace=m6502.Engine.tune_trace(tune_path) if args.tune != "default" else [])
         if world == 1 and not args.no_mask_ff:
             line["mask_ff"] = mask_ff_run(eng, stream, d_targets, n, sweep)
         if world == 1 and not args.no_stoke:   # configs 4 and 5, beside the headline
