@@ -80,3 +80,21 @@ def test_cuda_semantics_len2_rules_reprove(engine, cfg3):
     for i in rng.choice(len(cheap), size=min(40, len(cheap)), replace=False):
         t, c = cheap[i]
         assert oracle.exhaustive(list(targets[t]), list(c), 0, oracle.SWEEP_REFERENCE), (t, c)
+
+
+@pytest.mark.parametrize("mask", ["0x00", "0x01", "0xC3", "0xFF"])
+def test_go_semantics_full_sweep_match_oracle(engine, mask):
+    """The batched length-3 workload as benchmarked (Go semantics, length-1
+    and length-2 candidates, full sweep): 96 seeded length-3 targets against
+    the oracle's Go worker with its full sweep, under every mask.  A pair
+    the engine leaves undecided (an output cone beyond 2^34 states) would
+    count as not equivalent; none may occur here."""
+    targets = oracle.draw_targets(1, 3, 96)
+    dead = int(mask, 16)
+    want, wst = oracle.search_go(targets, dead=dead, max_cand_len=2, sweep=oracle.SWEEP_FULL)
+    rules, st = engine.search(targets, dead_flags=dead, semantics=_lib.SEM_GO, sweep=_lib.SWEEP_FULL,
+                              max_cand_len=2)
+    got = sorted((int(r["target"]), tuple(int(x) for x in r["cand"][:r["cand_len"]]), int(r["dead_flags"]))
+                 for r in rules)
+    assert got == sorted(want)
+    assert st["exh_undecided"] == 0
