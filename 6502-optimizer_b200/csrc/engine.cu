@@ -205,6 +205,8 @@ constexpr uint32_t kSurvLen2 = 1u << 23, kSurvMasked = 1u << 24;
 // The join already ran the random-state probe on this pair and found no
 // difference (k_exhaustive skips its own probe).
 constexpr uint32_t kSurvProbed = 1u << 31;
+// target_id of a pair source whose pairs do not share targets.
+constexpr uint64_t kNoTarget = ~0ull;
 __host__ __device__ __forceinline__ uint32_t fd_pack(uint32_t fd) { return (fd & 0x0Fu) | ((fd >> 2) & 0x30u); }
 
 struct Counters {
@@ -260,6 +262,8 @@ struct SurvSource {
         dead = go ? ((s.c & kSurvMasked) ? run_dead : 0u) : run_dead;
     }
     __device__ bool probed(uint64_t p) const { return (surv[p].c & kSurvProbed) != 0; }
+    // Pairs with the same id share their target (the probe reuses its outputs).
+    __device__ uint64_t target_id(uint64_t p) const { return surv[p].t; }
 };
 
 struct CsrSource {
@@ -278,6 +282,7 @@ struct CsrSource {
         dead = dead_;
     }
     __device__ bool probed(uint64_t) const { return false; }
+    __device__ uint64_t target_id(uint64_t) const { return kNoTarget; }
 };
 
 // Decode parameters of one cone sweep.  State index bits: A (8, if in the
@@ -423,6 +428,50 @@ __device__ __forceinline__ bool probe_domain(const PairView& pv, uint32_t swept,
     for (int it = 0; it < 2; it++) {   // 32 states at a time: most failing pairs fail in the first
         const uint64_t z = probe_z(salt, lane + 32 * it);
         if (__any_sync(kFull, state_diff_in(pv, m, probe_state(swept, rep, z)) != 0)) return false;
+    }
+    return true;
+}
+
+// The probe with the target's outputs kept per warp: consecutive pairs of
+// one target (a warp's ticket batch holds consecutive survivors, and the
+// join appends a target's survivors together) draw the same states, from
+// the target's salt.  The target's outputs on the states of its own domain
+// (A, carry and the registers it reads) are computed once and reused by
+// every candidate that reads no other register: one candidate instruction
+// per state instead of the whole pair.  A candidate that widens the domain
+// runs the target again on the wider states.  False when a state differs.
+struct TargetProbe {
+    uint64_t id = kNoTarget;   // target whose outputs `out` holds (uniform)
+    uint32_t sw = 0;           // its swept locations (uniform)
+    uint64_t out[2];           // this lane's target outputs on states lane, lane + 32
+};
+
+__device__ __forceinline__ bool probe_cached(const PairView& pv, uint32_t sw_t, uint32_t sw_c, uint64_t tid,
+                                             TargetProbe& tp, int lane) {
+    const uint64_t salt = tid * 0xD1B54A32D192ED03ull + 0x632BE59BD9B4E019ull;
+    if (tp.id != tid) {   // warp-uniform
+        tp.id = tid;
+        tp.sw = sw_t;
+        for (int r = 0; r < 2; r++) {
+            St ts = probe_state(sw_t | LB(L_A) | LB(L_C), false, probe_z(salt, lane + 32 * r));
+            for (int i = 0; i < pv.tn; i++) exec(ts, pv.t[i]);
+            tp.out[r] = pack(ts);
+        }
+    }
+    const bool same = (sw_c & ~tp.sw) == 0;   // uniform
+    const uint32_t swu = sw_t | sw_c | LB(L_A) | LB(L_C);
+    const uint64_t m = cmp_mask(pv.dead);
+    const int n = pv.tn + pv.cn;   // pv.cn >= 1 for every source with target ids
+    for (int r = 0; r < 2; r++) {   // 32 states at a time: most failing pairs fail in the first
+        const St in = probe_state(swu, false, probe_z(salt, lane + 32 * r));
+        uint64_t tout = tp.out[r];
+        St ps = in;
+        // one exec site: the target (when the domain widened), then the candidate
+        for (int i = same ? pv.tn : 0; i < n; i++) {
+            if (i == pv.tn) { if (!same) tout = pack(ps); ps = in; }
+            exec(ps, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
+        }
+        if (__any_sync(kFull, ((tout ^ pack(ps)) & m) != 0)) return false;
     }
     return true;
 }
@@ -1287,6 +1336,7 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t n = min((uint64_t)*n_pairs_ptr, n_cap);
     unsigned long long nstates = 0, probe_rej = 0;
+    TargetProbe tprobe;   // the probe's target outputs, kept across this warp's pairs
     unsigned long long next = 0, lim = 0;   // this warp's batch of tickets
     const unsigned long long tbatch = a.ticket_batch ? a.ticket_batch : kTicketBatch;
     const uint64_t chunk_min = a.chunk_log2 ? (1ull << a.chunk_log2) : kChunk;
@@ -1307,11 +1357,16 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
         src.load(p, s_t[w], s_c[w], pv.tn, pv.cn, pv.dead, lane);
         __syncwarp();
         if (!src.probed(p)) {
-            uint32_t sw = 0;
-            for (int i = 0; i < pv.tn; i++) sw |= c_sweep[pv.t[i] & 0xFFu];
-            for (int i = 0; i < pv.cn; i++) sw |= c_sweep[pv.c[i] & 0xFFu];
+            uint32_t sw_t = 0, sw_c = 0;
+            for (int i = 0; i < pv.tn; i++) sw_t |= c_sweep[pv.t[i] & 0xFFu];
+            for (int i = 0; i < pv.cn; i++) sw_c |= c_sweep[pv.c[i] & 0xFFu];
+            const uint32_t sw = sw_t | sw_c;
             const bool prep = a.sweep == M6502_SWEEP_REFERENCE && __popc(sw) >= 3;
-            if (!probe_domain(pv, sw | LB(L_A) | LB(L_C), prep, pv.dead, p, lane)) {
+            const uint64_t tid = src.target_id(p);
+            const bool ok = (tid != kNoTarget && !prep)
+                                ? probe_cached(pv, sw_t, sw_c, tid, tprobe, lane)
+                                : probe_domain(pv, sw | LB(L_A) | LB(L_C), prep, pv.dead, p, lane);
+            if (!ok) {
                 if (lane == 0) { a.fail[p] = 1u; probe_rej++; }
                 __syncwarp();
                 continue;

@@ -400,6 +400,7 @@ struct StokeSource {
         dead = dead_;
     }
     __device__ bool probed(uint64_t) const { return false; }
+    __device__ uint64_t target_id(uint64_t) const { return kNoTarget; }   // candidates may be empty
 };
 
 // Over the vec_ok entries sorted by key (one CTA, chunks of 1,024): rep[i] =
