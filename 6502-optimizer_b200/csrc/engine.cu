@@ -697,6 +697,35 @@ __device__ __forceinline__ Flow dataflow_s(const PairView& pv, int lane, const u
     return fl;
 }
 
+// The same composition with the target's half kept per warp: pairs of one
+// target (consecutive survivors) compose only their candidate.  The two
+// halves are independent: each starts from the identity.
+struct TargetFlow {
+    uint64_t id = kNoTarget;   // target whose composition is kept (uniform)
+    uint32_t dt = 0;           // this lane's composed dependencies of the target
+    uint32_t wt = 0, st = 0;   // locations the target writes / sweeps (uniform)
+};
+
+__device__ __forceinline__ Flow dataflow_cached(const PairView& pv, int lane, const uint16_t (*dep_tab)[NUM_LOCS],
+                                                uint64_t tid, TargetFlow& tf) {
+    const uint32_t id = (lane < NUM_LOCS) ? (1u << lane) : 0u;
+    if (tid == kNoTarget || tf.id != tid) {   // warp-uniform
+        uint32_t wt = 0, st = 0;
+        tf.dt = compose_s(id, pv.t, pv.tn, lane, wt, st, dep_tab);
+        tf.wt = wt;
+        tf.st = st;
+        tf.id = tid;
+    }
+    Flow fl;
+    uint32_t wc = 0, sw = tf.st;
+    const uint32_t dc = compose_s(id, pv.c, pv.cn, lane, wc, sw, dep_tab);
+    fl.k = __popc(sw);
+    fl.swept = sw | LB(L_A) | LB(L_C);
+    fl.written = tf.wt | wc;
+    fl.cone = (tf.dt | dc) & fl.swept;
+    return fl;
+}
+
 // Lane-distributed groups: lane o (< 13) keeps the cone of output o; the
 // maximal cones are found with shuffles and visited smallest first with warp
 // reductions, so no per-thread arrays (local memory) are needed.
@@ -1337,6 +1366,7 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
     const uint64_t n = min((uint64_t)*n_pairs_ptr, n_cap);
     unsigned long long nstates = 0, probe_rej = 0;
     TargetProbe tprobe;   // the probe's target outputs, kept across this warp's pairs
+    TargetFlow tflow;     // the target's half of the dataflow composition, likewise
     unsigned long long next = 0, lim = 0;   // this warp's batch of tickets
     const unsigned long long tbatch = a.ticket_batch ? a.ticket_batch : kTicketBatch;
     const uint64_t chunk_min = a.chunk_log2 ? (1ull << a.chunk_log2) : kChunk;
@@ -1372,7 +1402,7 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
                 continue;
             }
         }
-        Flow fl = dataflow_s(pv, lane, s_dep);
+        Flow fl = dataflow_cached(pv, lane, s_dep, src.target_id(p), tflow);
         const bool rep = a.sweep == M6502_SWEEP_REFERENCE && fl.k >= 3;
         LaneGroups lg;
         if (a.brute) {   // one group: the whole product space, every output
