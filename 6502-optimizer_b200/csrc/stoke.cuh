@@ -135,16 +135,22 @@ __device__ __forceinline__ int32_t stoke_cost(const uint16_t* seq, int len, uint
 }
 
 // Index drawn from one head of a chain's cumulative distribution (entries
-// [a, b) hold running sums); warp-uniform binary search.
-__device__ __forceinline__ int cdf_sample(const float* cdf, int a, int b, uint64_t& rng) {
+// [a, b) of the chain's row in shared memory hold running sums): the first
+// entry above a uniform point of the head's range (the last one if rounding
+// leaves none).  Warp-collective, two ballots: lane i tests the last entry
+// of block i (blocks of ceil((b - a) / 32) entries), then the lanes of the
+// first block above the point test its entries.
+__device__ __forceinline__ int cdf_sample(const float* cdf, int a, int b, uint64_t& rng, int lane) {
     const float base = a > 0 ? cdf[a - 1] : 0.0f;
     const float r = base + sm_unit(rng) * (cdf[b - 1] - base);
-    int lo = a, hi = b - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (cdf[mid] > r) hi = mid; else lo = mid + 1;
-    }
-    return lo - a;
+    const int n = b - a, bs = (n + 31) >> 5;
+    const int last = min((lane + 1) * bs, n) - 1;
+    const unsigned above = __ballot_sync(kFull, lane * bs < n && cdf[a + last] > r);
+    if (!above) return n - 1;
+    const int blk = __ffs(above) - 1;
+    const int j = blk * bs + lane;
+    const unsigned in = __ballot_sync(kFull, lane < bs && j < n && cdf[a + j] > r);
+    return in ? blk * bs + __ffs(in) - 1 : min((blk + 1) * bs, n) - 1;
 }
 
 constexpr uint32_t kNoRow = 0xFFFFFFFFu;
@@ -204,6 +210,7 @@ __global__ void __launch_bounds__(256) k_stoke_epoch(StokeChain* __restrict__ ch
                                                       StokeCounters* __restrict__ sc) {
     __shared__ uint16_t s_buf[kWarpsPerBlock][2][kMaxSeq];
     __shared__ uint16_t s_best[kWarpsPerBlock][kMaxSeq];
+    __shared__ float s_cdf[kWarpsPerBlock][330];   // the chain's learned distributions, staged once
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint32_t ci = blockIdx.x * kWarpsPerBlock + (uint32_t)w;
     if (ci >= n_chains) return;
@@ -230,7 +237,13 @@ __global__ void __launch_bounds__(256) k_stoke_epoch(StokeChain* __restrict__ ch
     uint32_t accepted = 0, diff = 0;
     bool zero;
     const uint32_t crow = prm.cdf ? prm.row[ci] : kNoRow;
-    const float* cdf = crow != kNoRow ? prm.cdf + (size_t)crow * 330 : nullptr;
+    const float* cdf = nullptr;
+    if (crow != kNoRow) {   // uniform
+        const float* g = prm.cdf + (size_t)crow * 330;
+        for (int i = lane; i < 330; i += 32) s_cdf[w][i] = g[i];
+        __syncwarp();
+        cdf = s_cdf[w];
+    }
     if (status == 0) {   // NewChain (mcmc.go:28-49): start from the target
         if (lane < (int)tlen) { cur[lane] = tg.ins[t0 + lane]; best[lane] = cur[lane]; }
         __syncwarp();
@@ -270,10 +283,10 @@ __global__ void __launch_bounds__(256) k_stoke_epoch(StokeChain* __restrict__ ch
         const bool learned = cdf && (kind == 0 || kind == 3) && sm_unit(rng) < prm.learned_frac;
         if (learned) {   // position, opcode, operand from the model's distributions
             const int lim = kind == 0 ? len : len + 1;
-            pos = cdf_sample(cdf, 0, 16, rng);
+            pos = cdf_sample(cdf, 0, 16, rng, lane);
             if (pos >= lim) pos = (int)sm_below(rng, (uint32_t)lim);
-            const uint32_t op = (uint32_t)cdf_sample(cdf, 16, 74, rng);
-            const uint32_t imm = has_imm(op) ? (uint32_t)cdf_sample(cdf, 74, 330, rng) : 0u;
+            const uint32_t op = (uint32_t)cdf_sample(cdf, 16, 74, rng, lane);
+            const uint32_t imm = has_imm(op) ? (uint32_t)cdf_sample(cdf, 74, 330, rng, lane) : 0u;
             ins = (uint16_t)(op | (imm << 8));
             if (kind == 3) nlen = len + 1;
         }

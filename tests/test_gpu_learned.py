@@ -8,7 +8,8 @@ moves a higher log-likelihood than the uniform proposal; (2) STOKE with the
 mixed proposal is run beside uniform STOKE on the same held-out targets and
 seeds, and every rewrite either finds passes the CPU oracle's QuickCheck and
 MidCheck, and the oracle's ExhaustiveCheck where its domain has at most
-2^25 states; (3) on the held-out targets uniform STOKE does not prove in its
+2^25 states; (3) on the STOKE benchmark's targets (a draw disjoint from the
+training and validation draws) that uniform STOKE does not prove in its
 first epoch (the model is first used in the second, so that epoch is the
 same under both), the median device time to the first proof is lower with
 the mixed proposal.
@@ -51,17 +52,25 @@ def test_learned_proposal_gains_over_uniform(engine):
               cost=_lib.COST_HAMMING, stop_on_proof=True)
     res_u, proofs_u, st_u = engine.stoke(held, **kw)
     res_l, proofs_l, st_l = engine.stoke(held, model=mlp, learned_frac=0.5, **kw)
+    # (3) time-to-proof on hard targets: the STOKE benchmark's draw (512
+    # targets of length 4-8, seed 2, disjoint from the training and
+    # validation draws), 128 chains each, full sweep
+    bench = I.draw_targets(2, 4, 8, 512, reject_pruned=False)
+    kb = dict(chains_per_target=128, steps=200000, steps_per_epoch=2000, first_epoch=64, seed=2,
+              cost=_lib.COST_HAMMING, sweep=_lib.SWEEP_FULL, stop_on_proof=True)
+    bu, _, sbu = engine.stoke(bench, **kb)
+    bl, _, sbl = engine.stoke(bench, model=mlp, learned_frac=0.5, **kb)
     hard_u, hard_l = [], []
-    for ru, rl in zip(res_u, res_l):
+    for ru, rl in zip(bu, bl):
         if ru["first_proof_ms"] >= 0 and ru["first_proof_step"] < 64:
             continue   # proved in the first epoch, which is the same for both
         if ru["first_proof_ms"] < 0 and rl["first_proof_ms"] < 0:
             continue
-        hard_u.append(ru["first_proof_ms"] if ru["first_proof_ms"] >= 0 else st_u["ms_device"])
-        hard_l.append(rl["first_proof_ms"] if rl["first_proof_ms"] >= 0 else st_l["ms_device"])
-    print(f"hard held-out targets: {len(hard_u)}; median ms uniform {np.median(hard_u):.2f}, "
+        hard_u.append(ru["first_proof_ms"] if ru["first_proof_ms"] >= 0 else sbu["ms_device"])
+        hard_l.append(rl["first_proof_ms"] if rl["first_proof_ms"] >= 0 else sbl["ms_device"])
+    print(f"hard targets: {len(hard_u)}; median ms uniform {np.median(hard_u):.2f}, "
           f"learned {np.median(hard_l):.2f}")
-    assert len(hard_u) >= 8
+    assert len(hard_u) >= 10
     assert np.median(hard_l) < np.median(hard_u)
     for res, name in ((res_u, "uniform"), (res_l, "learned")):
         st = sorted(r["first_proof_step"] for r in res if r["first_proof_ms"] >= 0)
