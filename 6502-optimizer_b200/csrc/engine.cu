@@ -418,61 +418,47 @@ __device__ __forceinline__ uint64_t probe_z(uint64_t salt, int i) {
     return z ^ (z >> 31);
 }
 
-// Probe: 64 pseudo-random states of the pair's whole sweep domain (A and
-// carry always swept), all outputs compared.  A mismatch anywhere in the
-// domain decides the pair (not equivalent) without the cone analysis;
-// passing decides nothing.
-__device__ __forceinline__ bool probe_domain(const PairView& pv, uint32_t swept, bool rep, uint32_t dead,
-                                             uint64_t salt, int lane) {
-    const OutMask m = out_mask(cmp_mask(dead));
-    for (int it = 0; it < 2; it++) {   // 32 states at a time: most failing pairs fail in the first
-        const uint64_t z = probe_z(salt, lane + 32 * it);
-        if (__any_sync(kFull, state_diff_in(pv, m, probe_state(swept, rep, z)) != 0)) return false;
-    }
-    return true;
-}
-
-// The probe with the target's outputs kept per warp: consecutive pairs of
-// one target (a warp's ticket batch holds consecutive survivors, and the
-// join appends a target's survivors together) draw the same states, from
-// the target's salt.  The target's outputs on the states of its own domain
-// (A, carry and the registers it reads) are computed once and reused by
-// every candidate that reads no other register: one candidate instruction
-// per state instead of the whole pair.  A candidate that widens the domain
-// runs the target again on the wider states.  False when a state differs.
-struct TargetProbe {
-    uint64_t id = kNoTarget;   // target whose outputs `out` holds (uniform)
-    uint32_t sw = 0;           // its swept locations (uniform)
-    uint64_t out[2];           // this lane's target outputs on states lane, lane + 32
+// Per-warp memory of the target last probed and composed, in shared memory
+// so that nothing of it stays in registers across the pair loop.
+struct TargetCache {
+    uint64_t probe_id;        // target whose probe outputs `out` holds (kNoTarget: none)
+    uint64_t flow_id;         // target whose composition `dt` / wt / st hold
+    uint64_t out[2][32];      // per lane: the target's outputs on probe states lane, lane + 32
+    uint32_t dt[32];          // per lane: the target's composed dependencies
+    uint32_t wt, st;          // locations the target writes / sweeps
 };
 
-__device__ __forceinline__ bool probe_cached(const PairView& pv, uint32_t sw_t, uint32_t sw_c, uint64_t tid,
-                                             TargetProbe& tp, int lane) {
-    const uint64_t salt = tid * 0xD1B54A32D192ED03ull + 0x632BE59BD9B4E019ull;
-    if (tp.id != tid) {   // warp-uniform
-        tp.id = tid;
-        tp.sw = sw_t;
-        for (int r = 0; r < 2; r++) {
-            St ts = probe_state(sw_t | LB(L_A) | LB(L_C), false, probe_z(salt, lane + 32 * r));
-            for (int i = 0; i < pv.tn; i++) exec(ts, pv.t[i]);
-            tp.out[r] = pack(ts);
-        }
-    }
-    const bool same = (sw_c & ~tp.sw) == 0;   // uniform
+// The probe of one pair: 64 pseudo-random states of its whole sweep domain,
+// drawn from the target's salt when the source says which pairs share a
+// target (`tid`), else from the pair's.  The target's outputs on the states
+// are kept in the warp's cache when the pair's domain is the target's own
+// (the candidate reads no other register); a later pair of the same target
+// with the same domain then runs only its candidate.  One exec site.  False
+// when a state differs.
+__device__ __forceinline__ bool probe_pair(const PairView& pv, uint32_t sw_t, uint32_t sw_c, bool rep, uint64_t tid,
+                                           uint64_t p, TargetCache& tc, int lane) {
+    const uint64_t salt = tid != kNoTarget ? tid * 0xD1B54A32D192ED03ull + 0x632BE59BD9B4E019ull : p;
+    const bool same = tid != kNoTarget && (sw_c & ~sw_t) == 0;   // uniform
+    const bool hit = same && tc.probe_id == tid;
+    if (same && !hit) tc.probe_id = kNoTarget;   // being refilled; valid again once both rounds are in
     const uint32_t swu = sw_t | sw_c | LB(L_A) | LB(L_C);
-    const uint64_t m = cmp_mask(pv.dead);
-    const int n = pv.tn + pv.cn;   // pv.cn >= 1 for every source with target ids
+    const OutMask m = out_mask(cmp_mask(pv.dead));
+    const int n = pv.tn + pv.cn;
     for (int r = 0; r < 2; r++) {   // 32 states at a time: most failing pairs fail in the first
-        const St in = probe_state(swu, false, probe_z(salt, lane + 32 * r));
-        uint64_t tout = tp.out[r];
-        St ps = in;
-        // one exec site: the target (when the domain widened), then the candidate
-        for (int i = same ? pv.tn : 0; i < n; i++) {
-            if (i == pv.tn) { if (!same) tout = pack(ps); ps = in; }
+        const St in = probe_state(swu, rep, probe_z(salt, lane + 32 * r));
+        St ps = in, ts = in;
+        if (hit) ts = unpack(tc.out[r][lane]);
+        for (int i = hit ? pv.tn : 0; i < n; i++) {
+            if (i == pv.tn) { ts = ps; ps = in; }
             exec(ps, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
         }
-        if (__any_sync(kFull, ((tout ^ pack(ps)) & m) != 0)) return false;
+        if (pv.cn == 0 && !hit) { ts = ps; ps = in; }
+        if (same && !hit) tc.out[r][lane] = pack(ts);
+        if (__any_sync(kFull, out_diff(ts, ps, m) != 0)) return false;
     }
+    __syncwarp();
+    if (same && !hit && lane == 0) tc.probe_id = tid;
+    __syncwarp();
     return true;
 }
 
@@ -697,32 +683,32 @@ __device__ __forceinline__ Flow dataflow_s(const PairView& pv, int lane, const u
     return fl;
 }
 
-// The same composition with the target's half kept per warp: pairs of one
-// target (consecutive survivors) compose only their candidate.  The two
-// halves are independent: each starts from the identity.
-struct TargetFlow {
-    uint64_t id = kNoTarget;   // target whose composition is kept (uniform)
-    uint32_t dt = 0;           // this lane's composed dependencies of the target
-    uint32_t wt = 0, st = 0;   // locations the target writes / sweeps (uniform)
-};
-
+// The same composition with the target's half kept in the warp's cache:
+// pairs of one target (consecutive survivors) compose only their candidate.
+// The two halves are independent: each starts from the identity.
 __device__ __forceinline__ Flow dataflow_cached(const PairView& pv, int lane, const uint16_t (*dep_tab)[NUM_LOCS],
-                                                uint64_t tid, TargetFlow& tf) {
+                                                uint64_t tid, TargetCache& tc) {
     const uint32_t id = (lane < NUM_LOCS) ? (1u << lane) : 0u;
-    if (tid == kNoTarget || tf.id != tid) {   // warp-uniform
-        uint32_t wt = 0, st = 0;
-        tf.dt = compose_s(id, pv.t, pv.tn, lane, wt, st, dep_tab);
-        tf.wt = wt;
-        tf.st = st;
-        tf.id = tid;
+    uint32_t dt, wt, st;
+    if (tid == kNoTarget || tc.flow_id != tid) {   // warp-uniform
+        wt = 0; st = 0;
+        dt = compose_s(id, pv.t, pv.tn, lane, wt, st, dep_tab);
+        if (tid != kNoTarget) {
+            __syncwarp();
+            tc.dt[lane] = dt;
+            if (lane == 0) { tc.wt = wt; tc.st = st; tc.flow_id = tid; }
+            __syncwarp();
+        }
+    } else {
+        dt = tc.dt[lane]; wt = tc.wt; st = tc.st;
     }
     Flow fl;
-    uint32_t wc = 0, sw = tf.st;
+    uint32_t wc = 0, sw = st;
     const uint32_t dc = compose_s(id, pv.c, pv.cn, lane, wc, sw, dep_tab);
     fl.k = __popc(sw);
     fl.swept = sw | LB(L_A) | LB(L_C);
-    fl.written = tf.wt | wc;
-    fl.cone = (tf.dt | dc) & fl.swept;
+    fl.written = wt | wc;
+    fl.cone = (dt | dc) & fl.swept;
     return fl;
 }
 
@@ -1365,8 +1351,10 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const uint64_t n = min((uint64_t)*n_pairs_ptr, n_cap);
     unsigned long long nstates = 0, probe_rej = 0;
-    TargetProbe tprobe;   // the probe's target outputs, kept across this warp's pairs
-    TargetFlow tflow;     // the target's half of the dataflow composition, likewise
+    __shared__ TargetCache s_tc[kWarpsPerBlock];   // the warp's last target: probe outputs, composition
+    TargetCache& tc = s_tc[threadIdx.x >> 5];
+    if ((threadIdx.x & 31) == 0) { tc.probe_id = kNoTarget; tc.flow_id = kNoTarget; }
+    __syncwarp();
     unsigned long long next = 0, lim = 0;   // this warp's batch of tickets
     const unsigned long long tbatch = a.ticket_batch ? a.ticket_batch : kTicketBatch;
     const uint64_t chunk_min = a.chunk_log2 ? (1ull << a.chunk_log2) : kChunk;
@@ -1390,19 +1378,15 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
             uint32_t sw_t = 0, sw_c = 0;
             for (int i = 0; i < pv.tn; i++) sw_t |= c_sweep[pv.t[i] & 0xFFu];
             for (int i = 0; i < pv.cn; i++) sw_c |= c_sweep[pv.c[i] & 0xFFu];
-            const uint32_t sw = sw_t | sw_c;
+            const uint32_t sw = sw_t | sw_c;   // swept extra registers
             const bool prep = a.sweep == M6502_SWEEP_REFERENCE && __popc(sw) >= 3;
-            const uint64_t tid = src.target_id(p);
-            const bool ok = (tid != kNoTarget && !prep)
-                                ? probe_cached(pv, sw_t, sw_c, tid, tprobe, lane)
-                                : probe_domain(pv, sw | LB(L_A) | LB(L_C), prep, pv.dead, p, lane);
-            if (!ok) {
+            if (!probe_pair(pv, sw_t, sw_c, prep, src.target_id(p), p, tc, lane)) {
                 if (lane == 0) { a.fail[p] = 1u; probe_rej++; }
                 __syncwarp();
                 continue;
             }
         }
-        Flow fl = dataflow_cached(pv, lane, s_dep, src.target_id(p), tflow);
+        Flow fl = dataflow_cached(pv, lane, s_dep, src.target_id(p), tc);
         const bool rep = a.sweep == M6502_SWEEP_REFERENCE && fl.k >= 3;
         LaneGroups lg;
         if (a.brute) {   // one group: the whole product space, every output
