@@ -435,7 +435,7 @@ def stoke_once(eng, targets, args, model=None):
               first_epoch=args.stoke_first_epoch, seed=2, cost=_lib.COST_HAMMING, sweep=_lib.SWEEP_FULL,
               stop_on_proof=True)
     if model is not None:
-        kw.update(model=model, learned_frac=0.5)
+        kw.update(model=model, learned_frac=args.stoke_learned_frac)
     res, proofs, st = eng.stoke(targets, **kw)
     times = sorted(r["first_proof_ms"] for r in res if r["first_proof_ms"] >= 0)
     steps = sorted(r["first_proof_step"] for r in res if r["first_proof_ms"] >= 0)
@@ -568,7 +568,8 @@ def stoke_config(args, learned):
             "chains_per_target": 128, "steps_per_chain": args.stoke_steps,
             "steps_per_epoch": args.stoke_epoch, "first_epoch": args.stoke_first_epoch,
             "cost": "hamming over 32 vectors + bytes + cycles/100", "temperature": "1.0 -> 0.1",
-            "proposal": "mixed 50/50 learned + uniform (model from the second epoch on)" if learned else "uniform",
+            "proposal": (f"mixed {args.stoke_learned_frac:.2f} learned + uniform (model from the second epoch on)"
+                         if learned else "uniform"),
             "sweep": "full", "stop_on_proof": True}
 
 
@@ -794,6 +795,8 @@ def main():
     ap.add_argument("--last-op", type=int, default=2863)
     ap.add_argument("--stoke-steps", type=int, default=1000000, help="steps per chain (STOKE workload)")
     ap.add_argument("--stoke-epoch", type=int, default=2000, help="steps between proof rounds (STOKE workload)")
+    ap.add_argument("--stoke-learned-frac", type=float, default=0.5,
+                    help="share of replace / insert moves the learned proposal draws")
     ap.add_argument("--stoke-first-epoch", type=int, default=64,
                     help="steps of the first STOKE epoch; epochs double up to --stoke-epoch")
     args = ap.parse_args()
