@@ -447,9 +447,9 @@ __device__ __forceinline__ bool probe_pair(const PairView& pv, uint32_t sw_t, ui
     for (int r = 0; r < 2; r++) {   // 32 states at a time: most failing pairs fail in the first
         const St in = probe_state(swu, rep, probe_z(salt, lane + 32 * r));
         St ps = in, ts = in;
-        if (hit) ts = unpack(tc.out[r][lane]);
+        if (hit) ts = unpack(tc.out[r][lane]);   // the target's outputs on this state, kept
         for (int i = hit ? pv.tn : 0; i < n; i++) {
-            if (i == pv.tn) { ts = ps; ps = in; }
+            if (i == pv.tn && !hit) { ts = ps; ps = in; }   // the target is done: the candidate starts
             exec(ps, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
         }
         if (pv.cn == 0 && !hit) { ts = ps; ps = in; }
