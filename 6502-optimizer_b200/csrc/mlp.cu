@@ -306,6 +306,7 @@ struct m6502_mlp {
     __nv_bfloat16 *x0 = nullptr, *h[3] = {}, *dzb = nullptr, *dh[3] = {}, *tr_a = nullptr, *tr_b = nullptr;
     float *z = nullptr, *dx0 = nullptr, *loss = nullptr, *probs = nullptr;
     int* d_err = nullptr;
+    float* ws = nullptr;     // split-K partial tiles of the weight gradients
 };
 
 namespace {
@@ -323,10 +324,13 @@ const int kLayerW[4] = {T_W1, T_W2, T_W3, T_W4};
         }                                                                             \
     } while (0)
 
+constexpr int kMaxSplits = 32;   // split-K workspace: kMaxSplits x kHid x kHid floats
+
 int gemm(m6502_mlp* mlp, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, int M, int N, int K,
-         tcg::Epilogue epi) {
+         tcg::Epilogue epi, int splits = 1) {
     if (K % tcg::kBK != 0 || lda % 8 || ldb % 8) { mlp->err = "gemm shape"; return M6502_E_INVAL; }
-    if (!tcg::launch_gemm(A, lda, B, ldb, M, N, K, epi, mlp->d_err, mlp->stream)) {
+    if (splits > 1 && (size_t)M * N > (size_t)kHid * kHid) splits = 1;
+    if (!tcg::launch_gemm(A, lda, B, ldb, M, N, K, epi, mlp->d_err, mlp->stream, splits, mlp->ws)) {
         mlp->err = "tensor-core GEMM launch failed (tensor map or launch)";
         return M6502_E_CUDA;
     }
@@ -336,6 +340,7 @@ int gemm(m6502_mlp* mlp, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B
 tcg::Epilogue epi_of(int mode, float* of, __nv_bfloat16* ob, const float* bias, const __nv_bfloat16* act, int ldc) {
     tcg::Epilogue e;
     e.mode = mode; e.out_f32 = of; e.out_bf16 = ob; e.bias = bias; e.act = act; e.ldc = ldc;
+    e.split_stride = 0;
     return e;
 }
 
@@ -392,7 +397,8 @@ int backward(m6502_mlp* mlp, const m6502_mlp_example* d_ex, int n, int rows, flo
         int rc = transpose(mlp, dout, rows, nout, mlp->tr_a);
         if (!rc) rc = transpose(mlp, acts[l], rows, nin, mlp->tr_b);
         if (!rc) rc = gemm(mlp, mlp->tr_a, rows, mlp->tr_b, rows, nout, nin, rows,
-                           epi_of(tcg::EPI_F32, G + mlp->off[kLayerW[l]], nullptr, nullptr, nullptr, nin));
+                           epi_of(tcg::EPI_F32, G + mlp->off[kLayerW[l]], nullptr, nullptr, nullptr, nin),
+                           tcg::split_count(nout, nin, rows, kMaxSplits));
         if (rc) return rc;
         // input gradient: dout . W  (B operand = W^T, [nin x nout])
         if (l > 0) {
@@ -481,7 +487,8 @@ int m6502_mlp_create(m6502_ctx* ctx, uint64_t seed, m6502_mlp** out) {
                (mlp->tr_a = dalloc<__nv_bfloat16>((size_t)kMaxBatch * kHid, err)) &&
                (mlp->tr_b = dalloc<__nv_bfloat16>((size_t)kMaxBatch * kHid, err)) &&
                (mlp->probs = dalloc<float>((size_t)kMaxBatch * kHeadEnd, err)) &&
-               (mlp->loss = dalloc<float>(1, err)) && (mlp->d_err = dalloc<int>(1, err));
+               (mlp->loss = dalloc<float>(1, err)) && (mlp->d_err = dalloc<int>(1, err)) &&
+               (mlp->ws = dalloc<float>((size_t)kMaxSplits * kHid * kHid, err));
     for (int l = 0; l < 3 && okk; l++)
         okk = (mlp->h[l] = dalloc<__nv_bfloat16>((size_t)kMaxBatch * kHid, err)) &&
               (mlp->dh[l] = dalloc<__nv_bfloat16>((size_t)kMaxBatch * kHid, err));
@@ -515,7 +522,7 @@ void m6502_mlp_destroy(m6502_mlp* mlp) {
     void* ps[] = {mlp->w, mlp->g, mlp->m, mlp->v, mlp->d_ex, mlp->x0, mlp->z, mlp->dzb, mlp->dx0, mlp->tr_a,
                   mlp->tr_b, mlp->loss, mlp->d_err, mlp->probs, mlp->h[0], mlp->h[1], mlp->h[2], mlp->dh[0], mlp->dh[1],
                   mlp->dh[2], mlp->wb[0], mlp->wb[1], mlp->wb[2], mlp->wb[3], mlp->wt[0], mlp->wt[1],
-                  mlp->wt[2], mlp->wt[3]};
+                  mlp->wt[2], mlp->wt[3], mlp->ws};
     for (void* p : ps) if (p) cudaFree(p);
     delete mlp;
 }
@@ -612,21 +619,40 @@ int m6502_mlp_train(m6502_mlp* mlp, const m6502_mlp_example* ex, uint64_t n, uin
 
 int m6502_gemm_bf16(m6502_ctx* ctx, int M, int N, int K, const void* A, const void* B, float* C) {
     if (!ctx || !A || !B || !C || M <= 0 || N <= 0 || K <= 0 || K % 64) return M6502_E_INVAL;
-    static int* d_err = nullptr;
+    // Per device: the error flag and the split-K workspace (grown on demand).
+    constexpr int kDevs = 64;
+    static int* d_err[kDevs] = {};
+    static float* d_ws[kDevs] = {};
+    static size_t ws_floats[kDevs] = {};
     static std::mutex mu;
     std::lock_guard<std::mutex> lk(mu);
-    if (cudaSetDevice(m6502_ctx_device(ctx)) != cudaSuccess) return M6502_E_CUDA;
+    const int dev = m6502_ctx_device(ctx);
+    if (dev < 0 || dev >= kDevs) return M6502_E_INVAL;
+    if (cudaSetDevice(dev) != cudaSuccess) return M6502_E_CUDA;
     if (cudaFuncSetAttribute(tcg::k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, tcg::kSmemBytes) != cudaSuccess)
         return M6502_E_CUDA;
-    if (!d_err && cudaMalloc(&d_err, sizeof(int)) != cudaSuccess) return M6502_E_NOMEM;
+    if (!d_err[dev] && cudaMalloc(&d_err[dev], sizeof(int)) != cudaSuccess) return M6502_E_NOMEM;
     cudaStream_t st = (cudaStream_t)m6502_stream(ctx);
-    if (cudaMemsetAsync(d_err, 0, sizeof(int), st) != cudaSuccess) return M6502_E_CUDA;
+    const int splits = tcg::split_count(M, N, K, 64);
+    if (splits > 1 && ws_floats[dev] < (size_t)splits * M * N) {
+        if (d_ws[dev]) {
+            if (cudaStreamSynchronize(st) != cudaSuccess) return M6502_E_CUDA;
+            cudaFree(d_ws[dev]);
+            d_ws[dev] = nullptr;
+            ws_floats[dev] = 0;
+        }
+        if (cudaMalloc(&d_ws[dev], (size_t)splits * M * N * sizeof(float)) != cudaSuccess) return M6502_E_NOMEM;
+        ws_floats[dev] = (size_t)splits * M * N;
+    }
+    if (cudaMemsetAsync(d_err[dev], 0, sizeof(int), st) != cudaSuccess) return M6502_E_CUDA;
     tcg::Epilogue e;
     e.mode = tcg::EPI_F32; e.out_f32 = C; e.out_bf16 = nullptr; e.bias = nullptr; e.act = nullptr; e.ldc = N;
-    if (!tcg::launch_gemm((const __nv_bfloat16*)A, K, (const __nv_bfloat16*)B, K, M, N, K, e, d_err, st))
+    e.split_stride = 0;
+    if (!tcg::launch_gemm((const __nv_bfloat16*)A, K, (const __nv_bfloat16*)B, K, M, N, K, e, d_err[dev], st, splits,
+                          d_ws[dev]))
         return M6502_E_CUDA;
     int h = 0;
-    if (cudaMemcpyAsync(&h, d_err, sizeof h, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+    if (cudaMemcpyAsync(&h, d_err[dev], sizeof h, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return M6502_E_CUDA;
     return h ? M6502_E_CUDA : M6502_OK;

@@ -19,6 +19,10 @@
 //     lanes 32w..32w+31 = tile rows) and apply the fused bias / ReLU /
 //     ReLU-gradient / conversion.
 // Rows and columns past M, N are zero-filled by the TMA and not stored.
+// Split K (gridDim.z > 1, EPI_F32 only): CTA z runs K blocks
+// [z * kb_per, (z + 1) * kb_per) and writes its partial tile to slice z of a
+// workspace (epi.split_stride floats apart); k_sum_splits then adds the
+// slices in a fixed order, so the result does not depend on scheduling.
 // Every mbarrier wait is bounded; on expiry the kernel records an error,
 // stops issuing, waits a bounded time for work in flight, frees TMEM and
 // returns.  No cluster multicast is used.
@@ -54,6 +58,7 @@ struct Epilogue {
     const float* bias;
     const __nv_bfloat16* act;   // EPI_RELU_GRAD: the layer's post-ReLU activation
     int ldc;
+    size_t split_stride;        // split K: floats between the partial slices of out_f32
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -112,7 +117,7 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 
 __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB, int M, int N, int K,
-                                                    Epilogue epi, int* __restrict__ err) {
+                                                    int kb_per, Epilogue epi, int* __restrict__ err) {
     extern __shared__ uint8_t smem_raw[];
     __shared__ uint64_t full[kStages], empty[kStages], done;
     __shared__ uint32_t s_tmem;
@@ -120,7 +125,9 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUten
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN;
-    const int nk = K / kBK;
+    const int kb0 = blockIdx.z * kb_per;                 // this CTA's K blocks: [kb0, kb0 + nk)
+    const int nk = min(K / kBK - kb0, kb_per);          // >= 1 by the launcher's choice of kb_per
+    if (gridDim.z > 1) epi.out_f32 += blockIdx.z * epi.split_stride;
 
     if (warp == 0) {   // 256 TMEM columns: one fp32 accumulator column per N
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
@@ -152,8 +159,8 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUten
             if (*(volatile int*)&s_fail) break;
             uint8_t* sa = smem + s * kStageBytes;
             mbar_expect_tx(&full[s], (uint32_t)kStageBytes);
-            tma_load_2d(sa, &tmA, kb * kBK, m0, &full[s]);
-            tma_load_2d(sa + kStageA, &tmB, kb * kBK, n0, &full[s]);
+            tma_load_2d(sa, &tmA, (kb0 + kb) * kBK, m0, &full[s]);
+            tma_load_2d(sa + kStageA, &tmB, (kb0 + kb) * kBK, n0, &full[s]);
             issued = kb + 1;
         }
     } else if (warp == 1 && lane == 0) {
@@ -270,16 +277,58 @@ inline bool make_map(CUtensorMap* map, const void* base, int rows, int K, int ld
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// C[row][col] = sum over the splits of ws[z][row][col], in order z = 0, 1, ...
+__global__ void k_sum_splits(const float* __restrict__ ws, int splits, int M, int N, float* __restrict__ out,
+                             int ldc) {
+    const size_t slice = (size_t)M * N;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < slice; i += (size_t)gridDim.x * blockDim.x) {
+        float acc = 0.0f;
+        for (int z = 0; z < splits; z++) acc += ws[z * slice + i];
+        out[(i / N) * ldc + i % N] = acc;
+    }
+}
+
+// Number of K splits for C[M x N] = A . B^T over K: 1 when the output tiles
+// fill the 148 SMs, else enough splits to fill them, each of at least
+// kStages K blocks, at most `max_splits`.
+inline int split_count(int M, int N, int K, int max_splits) {
+    const int tiles = ((N + kBN - 1) / kBN) * ((M + kBM - 1) / kBM), nk = K / kBK;
+    if (tiles >= 74 || nk < 2 * kStages) return 1;
+    int s = (148 + tiles - 1) / tiles;
+    s = s < nk / kStages ? s : nk / kStages;
+    s = s < max_splits ? s : max_splits;
+    if (s <= 1) return 1;
+    const int per = (nk + s - 1) / s;   // every split gets at least one K block
+    return (nk + per - 1) / per;
+}
+
 // C = A . B^T with the fused epilogue, on `stream`.  K must be a multiple of
 // kBK; lda and ldb multiples of 8; A and B 16-byte aligned.  Returns false if
 // the shapes or the tensor maps are not usable (nothing is launched).
+// With splits > 1 (EPI_F32 only) `ws` holds splits x M x N floats of
+// partial tiles, summed into epi.out_f32 by k_sum_splits.
 inline bool launch_gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, int M, int N, int K,
-                        const Epilogue& epi, int* err, cudaStream_t stream) {
+                        const Epilogue& epi, int* err, cudaStream_t stream, int splits = 1, float* ws = nullptr) {
     if (M <= 0 || N <= 0 || K <= 0 || K % kBK) return false;
+    if (splits > 1 && (epi.mode != EPI_F32 || !ws)) return false;
     CUtensorMap ma, mb;
     if (!make_map(&ma, A, M, K, lda, kBM) || !make_map(&mb, B, N, K, ldb, kBN)) return false;
-    dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM);
-    k_gemm<<<grid, kThreads, kSmemBytes, stream>>>(ma, mb, M, N, K, epi, err);
+    const int nk = K / kBK;
+    const int per = (nk + splits - 1) / splits;
+    splits = (nk + per - 1) / per;
+    dim3 grid((N + kBN - 1) / kBN, (M + kBM - 1) / kBM, splits);
+    Epilogue e = epi;
+    if (splits > 1) {
+        e.out_f32 = ws;
+        e.ldc = N;
+        e.split_stride = (size_t)M * N;
+    }
+    k_gemm<<<grid, kThreads, kSmemBytes, stream>>>(ma, mb, M, N, K, per, e, err);
+    if (splits > 1) {
+        const size_t slice = (size_t)M * N;
+        const int blocks = (int)((slice + 255) / 256 < 1184 ? (slice + 255) / 256 : 1184);
+        k_sum_splits<<<blocks, 256, 0, stream>>>(ws, splits, M, N, epi.out_f32, epi.ldc);
+    }
     return cudaGetLastError() == cudaSuccess;
 }
 

@@ -575,35 +575,19 @@ def stoke_config(args, learned):
 
 def run_gemm(args):
     """The learned proposal's dense-layer kernel (tcgen05 bf16 GEMM, fp32
-    accumulate in TMEM) on a square problem, against the measured cuBLAS bf16
-    peak of this pool (MEASURED_PEAKS.json, burst figure)."""
+    accumulate in TMEM) against the measured cuBLAS bf16 peak of this pool
+    (MEASURED_PEAKS.json, burst figure): a square problem (--gemm-n), then
+    the proposal network's own layer shapes at its largest batch (65,536
+    chain rows: 448 -> 512, 512 -> 512, 512 -> 384, and the weight gradient
+    512 x 512 over K = 65,536 rows).  One JSON line per shape."""
     import torch
     import m6502
     from m6502.mlp import gemm_bf16
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    n = args.gemm_n
-    eng = m6502.Engine(device=local)
-    stream = torch.cuda.ExternalStream(eng.stream, device=local)
-    g = torch.Generator(device=f"cuda:{local}").manual_seed(0)
-    a = torch.randn(n, n, device=f"cuda:{local}", generator=g).to(torch.bfloat16)
-    b = torch.randn(n, n, device=f"cuda:{local}", generator=g).to(torch.bfloat16)
-    for _ in range(max(args.warmup, 3)):
-        c = gemm_bf16(eng, a, b)
-    torch.cuda.synchronize()
-    ref = a[:256].float() @ b.float().T
-    err = float((c[:256] - ref).abs().max() / ref.abs().max())
-    clocks = ClockSampler(local)
-    clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        gemm_bf16(eng, a, b)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    tflops = 2.0 * n ** 3 / (ms / 1e3) / 1e12
+    shapes = [(args.gemm_n, args.gemm_n, args.gemm_n)]
+    if args.gemm_shapes:
+        shapes += [tuple(int(v) for v in s.split("x")) for s in args.gemm_shapes.split(",")]
     peaks = {}
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -611,15 +595,43 @@ def run_gemm(args):
     except OSError:
         pass
     peak = peaks.get("bf16_tflops", 1590.0)
-    line = {"metric": "bf16 GEMM TFLOP/s (tcgen05, TMA, 128x256 tiles)", "value": tflops, "unit": "TFLOP/s",
-            "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": max(args.warmup, 3),
-            "ms_per_step": ms, "dtype": "bf16", "data": "synthetic (seeded normal)",
-            "config": {"workload": f"gemm-{n}", "M": n, "N": n, "K": n},
-            "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
-                         "frac": tflops / peak, "peak_source": "measured" if peaks else "fallback"},
-            "max_rel_err_vs_fp32": err,
-            "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}}
-    print(json.dumps(line), flush=True)
+    eng = m6502.Engine(device=local)
+    stream = torch.cuda.ExternalStream(eng.stream, device=local)
+    g = torch.Generator(device=f"cuda:{local}").manual_seed(0)
+    for (M, N, K) in shapes:
+        a = torch.randn(M, K, device=f"cuda:{local}", generator=g).to(torch.bfloat16)
+        b = torch.randn(N, K, device=f"cuda:{local}", generator=g).to(torch.bfloat16)
+        for _ in range(max(args.warmup, 3)):
+            c = gemm_bf16(eng, a, b)
+        torch.cuda.synchronize()
+        ref = a[:256].float() @ b.float().T
+        err = float((c[:256] - ref).abs().max() / ref.abs().max())
+        # short problems: repeat so that the timed region spans ~100 ms
+        flop = 2.0 * M * N * K
+        reps = max(args.steps, int(min(2000, max(1, 1e14 / flop))))
+        clocks = ClockSampler(local)
+        clocks.start()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            gemm_bf16(eng, a, b)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        ms = e0.elapsed_time(e1) / reps
+        tflops = flop / (ms / 1e3) / 1e12
+        square = M == N == K
+        line = {"metric": "bf16 GEMM TFLOP/s (tcgen05, TMA, 128x256 tiles)", "value": tflops, "unit": "TFLOP/s",
+                "higher_is_better": True, "n_gpus": 1, "steps": reps, "warmup": max(args.warmup, 3),
+                "ms_per_step": ms, "dtype": "bf16", "data": "synthetic (seeded normal)",
+                "config": {"workload": f"gemm-{M}" if square else f"gemm-mlp-{M}x{N}x{K}", "M": M, "N": N, "K": K,
+                           "output": "fp32, written to HBM (the MLP's layers fuse bias/ReLU instead)"},
+                "roofline": {"bound": "tensor", "achieved": tflops, "peak": peak, "unit": "TFLOP/s",
+                             "frac": tflops / peak, "peak_source": "measured" if peaks else "fallback"},
+                "max_rel_err_vs_fp32": err,
+                "clocks": {"sm_mhz": clk["sm_mhz"], "sm_max_mhz": clk["sm_max_mhz"], "reasons": clk["reasons"]}}
+        print(json.dumps(line), flush=True)
+        del a, b, c
     eng.close()
 
 
@@ -789,6 +801,8 @@ def main():
                          "tuning (force), or the built-in defaults")
     ap.add_argument("--workload", choices=["len2", "len3", "stoke", "stoke-learned", "gemm"], default="len2")
     ap.add_argument("--gemm-n", type=int, default=8192, help="GEMM workload: M = N = K")
+    ap.add_argument("--gemm-shapes", default="65536x512x448,65536x512x512,65536x384x512,512x512x65536",
+                    help="GEMM workload: further MxNxK shapes after the square one (empty: none)")
     ap.add_argument("--first-op", type=int, default=0,
                     help="length-2 workload: first instructions [first-op, last-op) of the CUDA-order table "
                          "(a subset, for small profiler captures)")

@@ -12,11 +12,13 @@ pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 320), (300, 200, 128), (1024, 512, 512),
-                                   (512, 320, 4096)])
+                                   (512, 320, 4096), (128, 256, 2368), (512, 512, 65536)])
 def test_tcgen05_gemm_matches_torch_fp32(engine, M, N, K):
     """C = A . B^T with bf16 operands: products are exact in fp32, so the only
     difference from the fp32 reference is summation order (tolerance 1e-4 of
-    the row scale)."""
+    the row scale).  The last three shapes split K across CTAs (37 K blocks
+    in 8 uneven splits; 1,024 in 19); the partial tiles are summed in a fixed
+    order, so a second call is bit-identical."""
     import torch
     g = torch.Generator(device="cuda").manual_seed(M * 7 + N * 13 + K)
     a = torch.randn((M, K), generator=g, device="cuda").to(torch.bfloat16)
