@@ -469,7 +469,7 @@ int m6502_mlp_create(m6502_ctx* ctx, uint64_t seed, m6502_mlp** out) {
     mlp->device = m6502_ctx_device(ctx);
     mlp->stream = (cudaStream_t)m6502_stream(ctx);
     if (cudaSetDevice(mlp->device) != cudaSuccess) { delete mlp; return M6502_E_CUDA; }
-    if (cudaFuncSetAttribute(tcg::k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, tcg::kSmemBytes) != cudaSuccess) {
+    if (!tcg::prepare_gemm()) {
         delete mlp;
         return M6502_E_CUDA;
     }
@@ -617,21 +617,25 @@ int m6502_mlp_train(m6502_mlp* mlp, const m6502_mlp_example* ex, uint64_t n, uin
     return check_err(mlp);
 }
 
-int m6502_gemm_bf16(m6502_ctx* ctx, int M, int N, int K, const void* A, const void* B, float* C) {
-    if (!ctx || !A || !B || !C || M <= 0 || N <= 0 || K <= 0 || K % 64) return M6502_E_INVAL;
-    // Per device: the error flag and the split-K workspace (grown on demand).
+int m6502_gemm_bf16_timed(m6502_ctx* ctx, int M, int N, int K, const void* A, const void* B, float* C, int reps,
+                          float* ms_per_launch) {
+    if (!ctx || !A || !B || !C || M <= 0 || N <= 0 || K <= 0 || K % 64 || reps < 1) return M6502_E_INVAL;
+    // Per device: the error flag, the split-K workspace (grown on demand)
+    // and two timing events.
     constexpr int kDevs = 64;
     static int* d_err[kDevs] = {};
     static float* d_ws[kDevs] = {};
     static size_t ws_floats[kDevs] = {};
+    static cudaEvent_t ev[kDevs][2] = {};
     static std::mutex mu;
     std::lock_guard<std::mutex> lk(mu);
     const int dev = m6502_ctx_device(ctx);
     if (dev < 0 || dev >= kDevs) return M6502_E_INVAL;
     if (cudaSetDevice(dev) != cudaSuccess) return M6502_E_CUDA;
-    if (cudaFuncSetAttribute(tcg::k_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize, tcg::kSmemBytes) != cudaSuccess)
-        return M6502_E_CUDA;
+    if (!tcg::prepare_gemm()) return M6502_E_CUDA;
     if (!d_err[dev] && cudaMalloc(&d_err[dev], sizeof(int)) != cudaSuccess) return M6502_E_NOMEM;
+    if (!ev[dev][0] && (cudaEventCreate(&ev[dev][0]) != cudaSuccess || cudaEventCreate(&ev[dev][1]) != cudaSuccess))
+        return M6502_E_CUDA;
     cudaStream_t st = (cudaStream_t)m6502_stream(ctx);
     const int splits = tcg::split_count(M, N, K, 64);
     if (splits > 1 && ws_floats[dev] < (size_t)splits * M * N) {
@@ -648,14 +652,26 @@ int m6502_gemm_bf16(m6502_ctx* ctx, int M, int N, int K, const void* A, const vo
     tcg::Epilogue e;
     e.mode = tcg::EPI_F32; e.out_f32 = C; e.out_bf16 = nullptr; e.bias = nullptr; e.act = nullptr; e.ldc = N;
     e.split_stride = 0;
-    if (!tcg::launch_gemm((const __nv_bfloat16*)A, K, (const __nv_bfloat16*)B, K, M, N, K, e, d_err[dev], st, splits,
-                          d_ws[dev]))
-        return M6502_E_CUDA;
+    if (ms_per_launch && cudaEventRecord(ev[dev][0], st) != cudaSuccess) return M6502_E_CUDA;
+    for (int r = 0; r < reps; r++)
+        if (!tcg::launch_gemm((const __nv_bfloat16*)A, K, (const __nv_bfloat16*)B, K, M, N, K, e, d_err[dev], st,
+                              splits, d_ws[dev]))
+            return M6502_E_CUDA;
+    if (ms_per_launch && cudaEventRecord(ev[dev][1], st) != cudaSuccess) return M6502_E_CUDA;
     int h = 0;
     if (cudaMemcpyAsync(&h, d_err[dev], sizeof h, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess)
         return M6502_E_CUDA;
+    if (ms_per_launch) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, ev[dev][0], ev[dev][1]) != cudaSuccess) return M6502_E_CUDA;
+        *ms_per_launch = ms / (float)reps;
+    }
     return h ? M6502_E_CUDA : M6502_OK;
+}
+
+int m6502_gemm_bf16(m6502_ctx* ctx, int M, int N, int K, const void* A, const void* B, float* C) {
+    return m6502_gemm_bf16_timed(ctx, M, N, K, A, B, C, 1, nullptr);
 }
 
 }  // extern "C"

@@ -5,7 +5,10 @@
 //
 // One CTA of 128 threads computes a 128 x 256 tile; the fp32 accumulator
 // (256 columns) lives in tensor memory.  The K loop runs through a ring of
-// kStages shared-memory stages (A 16 KB + B 32 KB each):
+// STAGES shared-memory stages (A 16 KB + B 32 KB each): 4 with one CTA per
+// SM, or 2 with two CTAs per SM (the 512 TMEM columns hold both
+// accumulators) when a CTA's K range is at most 8 blocks, so that one CTA's
+// epilogue overlaps the other's loads and MMAs:
 //   - lane 0 of warp 0 (producer) waits until a stage is free (its `empty`
 //     mbarrier), arms its `full` mbarrier with the stage's byte count and
 //     issues two TMA tile loads (cp.async.bulk.tensor, 128-byte swizzle)
@@ -16,8 +19,9 @@
 //     core has read it;
 //   - after the last K block a commit on `done` releases the epilogue: all
 //     four warps read the accumulator with tcgen05.ld (warp w owns TMEM
-//     lanes 32w..32w+31 = tile rows) and apply the fused bias / ReLU /
-//     ReLU-gradient / conversion.
+//     lanes 32w..32w+31 = tile rows), transpose each 32 x 32 slab through
+//     shared memory so that stores run along rows, and apply the fused
+//     bias / ReLU / ReLU-gradient / conversion.
 // Rows and columns past M, N are zero-filled by the TMA and not stored.
 // Split K (gridDim.z > 1, EPI_F32 only): CTA z runs K blocks
 // [z * kb_per, (z + 1) * kb_per) and writes its partial tile to slice z of a
@@ -35,12 +39,14 @@
 namespace tcg {
 
 constexpr int kBM = 128, kBN = 256, kBK = 64;
-constexpr int kStages = 4;
+constexpr int kStages = 4;          // deep ring: one CTA per SM (K of more than 8 blocks)
+constexpr int kStagesShallow = 2;   // two CTAs per SM: one's epilogue overlaps the other's K loop
 constexpr int kThreads = 128;
 constexpr int kStageA = kBM * kBK * 2;                  // 16 KB
 constexpr int kStageB = kBN * kBK * 2;                  // 32 KB
 constexpr int kStageBytes = kStageA + kStageB;          // 48 KB
-constexpr int kSmemBytes = kStages * kStageBytes + 1024;   // + slack to align to 1,024 bytes
+constexpr int smem_bytes(int stages) { return stages * kStageBytes + 1024; }   // + slack to align to 1,024 bytes
+constexpr int kEpiPitch = 33;       // epilogue staging: 32 x 32 fp32 per warp, one float of padding per row
 constexpr uint32_t kWaitLimit = 1u << 26;               // bounded mbarrier polling
 
 // Epilogue modes.
@@ -115,11 +121,12 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
+template <int STAGES>
 __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUtensorMap tmA,
                                                     const __grid_constant__ CUtensorMap tmB, int M, int N, int K,
                                                     int kb_per, Epilogue epi, int* __restrict__ err) {
     extern __shared__ uint8_t smem_raw[];
-    __shared__ uint64_t full[kStages], empty[kStages], done;
+    __shared__ uint64_t full[STAGES], empty[STAGES], done;
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -135,7 +142,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUten
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; s++) {
+        for (int s = 0; s < STAGES; s++) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
@@ -154,7 +161,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUten
     if (warp == 0 && lane == 0) {
         // producer: stage s of round r is free once the MMAs of round r-1 committed on empty[s]
         for (int kb = 0; kb < nk; kb++) {
-            const int s = kb % kStages, r = kb / kStages;
+            const int s = kb % STAGES, r = kb / STAGES;
             if (r > 0 && !mbar_wait(&empty[s], (uint32_t)((r - 1) & 1))) { atomicExch(&s_fail, 1); break; }
             if (*(volatile int*)&s_fail) break;
             uint8_t* sa = smem + s * kStageBytes;
@@ -167,7 +174,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUten
         // MMA issuer
         const uint32_t idesc = idesc_bf16(kBM, kBN);
         for (int kb = 0; kb < nk; kb++) {
-            const int s = kb % kStages, r = kb / kStages;
+            const int s = kb % STAGES, r = kb / STAGES;
             if (!mbar_wait(&full[s], (uint32_t)(r & 1)) || *(volatile int*)&s_fail) {
                 atomicExch(&s_fail, 1);
                 break;
@@ -202,15 +209,24 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUten
         // memory: the producer waits (bounded) for the last phase it armed on
         // each stage before the CTA releases its memory.
         if (warp == 0 && lane == 0)
-            for (int kb = max(0, issued - kStages); kb < issued; kb++)
-                mbar_wait(&full[kb % kStages], (uint32_t)((kb / kStages) & 1));
+            for (int kb = max(0, issued - STAGES); kb < issued; kb++)
+                mbar_wait(&full[kb % STAGES], (uint32_t)((kb / STAGES) & 1));
     } else {
-        // Epilogue: row = m0 + 32 * warp + lane; 16 columns per tcgen05.ld.
-        const int row = m0 + 32 * warp + lane;
+        // Epilogue.  Warp w owns tile rows 32w..32w+31 (its TMEM lanes).  Each
+        // 32-column slab is read from TMEM with lane = row, transposed through
+        // shared memory (the operand stages are free once `done` fired: every
+        // load was consumed by an MMA that has completed) and written with
+        // lane = column, so one store instruction covers one contiguous run of
+        // a row (128 B of fp32, 64 B of bf16) instead of 32 rows.  The padded
+        // pitch keeps both the row writes and the column reads free of bank
+        // conflicts.
+        float* stage = reinterpret_cast<float*>(smem) + warp * (32 * kEpiPitch);
+        const int r0 = m0 + 32 * warp;
+        const bool has_bias = epi.mode == EPI_BIAS_F32 || epi.mode == EPI_BIAS_RELU;
 #pragma unroll 1
-        for (int c0 = 0; c0 < kBN; c0 += 16) {
+        for (int c0 = 0; c0 < kBN; c0 += 32) {
             if (n0 + c0 >= N) break;   // warp-uniform
-            uint32_t v[16];
+            uint32_t v[32];
             const uint32_t taddr = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0;
             asm volatile(
                 "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
@@ -218,18 +234,28 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUten
                   "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
                   "=r"(v[15])
                 : "r"(taddr));
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+                : "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]),
+                  "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]),
+                  "=r"(v[30]), "=r"(v[31])
+                : "r"(taddr + 16u));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (row < M) {
 #pragma unroll
-                for (int j = 0; j < 16; j++) {
-                    const int col = n0 + c0 + j;
-                    if (col >= N) continue;
-                    float x = __uint_as_float(v[j]);
-                    const size_t o = (size_t)row * epi.ldc + col;
+            for (int j = 0; j < 32; j++) stage[lane * kEpiPitch + j] = __uint_as_float(v[j]);
+            __syncwarp();
+            const int col = n0 + c0 + lane;
+            if (col < N) {
+                const float bias = has_bias ? epi.bias[col] : 0.0f;
+                const int rows = min(32, M - r0);
+#pragma unroll 4
+                for (int r = 0; r < rows; r++) {
+                    const float x = stage[r * kEpiPitch + lane];
+                    const size_t o = (size_t)(r0 + r) * epi.ldc + col;
                     switch (epi.mode) {
                     case EPI_F32: epi.out_f32[o] = x; break;
-                    case EPI_BIAS_F32: epi.out_f32[o] = x + epi.bias[col]; break;
-                    case EPI_BIAS_RELU: epi.out_bf16[o] = __float2bfloat16(fmaxf(x + epi.bias[col], 0.0f)); break;
+                    case EPI_BIAS_F32: epi.out_f32[o] = x + bias; break;
+                    case EPI_BIAS_RELU: epi.out_bf16[o] = __float2bfloat16(fmaxf(x + bias, 0.0f)); break;
                     case EPI_RELU_GRAD:
                         epi.out_bf16[o] = __float2bfloat16(__bfloat162float(epi.act[o]) > 0.0f ? x : 0.0f);
                         break;
@@ -237,6 +263,7 @@ __global__ void __launch_bounds__(kThreads) k_gemm(const __grid_constant__ CUten
                     }
                 }
             }
+            __syncwarp();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -288,6 +315,19 @@ __global__ void k_sum_splits(const float* __restrict__ ws, int splits, int M, in
     }
 }
 
+// Raises the dynamic shared-memory limit of both kernel variants on the
+// current device; call once per device before the first launch_gemm.
+// The two-stage variant also asks for the largest shared-memory carveout:
+// with the default the driver sizes the carveout for one of its CTAs.
+inline bool prepare_gemm() {
+    return cudaFuncSetAttribute(k_gemm<kStages>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem_bytes(kStages)) == cudaSuccess &&
+           cudaFuncSetAttribute(k_gemm<kStagesShallow>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem_bytes(kStagesShallow)) == cudaSuccess &&
+           cudaFuncSetAttribute(k_gemm<kStagesShallow>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared) == cudaSuccess;
+}
+
 // Number of K splits for C[M x N] = A . B^T over K: 1 when the output tiles
 // fill the 148 SMs, else enough splits to fill them, each of at least
 // kStages K blocks, at most `max_splits`.
@@ -323,7 +363,10 @@ inline bool launch_gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B,
         e.ldc = N;
         e.split_stride = (size_t)M * N;
     }
-    k_gemm<<<grid, kThreads, kSmemBytes, stream>>>(ma, mb, M, N, K, per, e, err);
+    if (per <= 8)   // a short K range: two CTAs per SM
+        k_gemm<kStagesShallow><<<grid, kThreads, smem_bytes(kStagesShallow), stream>>>(ma, mb, M, N, K, per, e, err);
+    else
+        k_gemm<kStages><<<grid, kThreads, smem_bytes(kStages), stream>>>(ma, mb, M, N, K, per, e, err);
     if (splits > 1) {
         const size_t slice = (size_t)M * N;
         const int blocks = (int)((slice + 255) / 256 < 1184 ? (slice + 255) / 256 : 1184);

@@ -151,7 +151,7 @@ SYMBOLS = (
     "m6502_seq_bytes", "m6502_seq_cycles", "m6502_op_deps", "m6502_format_jsonl",
     "m6502_exhaustive_static", "m6502_stoke_run", "m6502_mlp_param_count", "m6502_mlp_create",
     "m6502_mlp_destroy", "m6502_mlp_last_error", "m6502_mlp_params", "m6502_mlp_predict", "m6502_mlp_gradients",
-    "m6502_mlp_train", "m6502_gemm_bf16", "m6502_tune_get", "m6502_tune_set", "m6502_autotune",
+    "m6502_mlp_train", "m6502_gemm_bf16", "m6502_gemm_bf16_timed", "m6502_tune_get", "m6502_tune_set", "m6502_autotune",
 )
 
 
@@ -212,6 +212,8 @@ def lib():
         L.m6502_mlp_train.argtypes = [vp, P(MlpExample), ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint32,
                                       ctypes.c_float, ctypes.c_uint64, vp]
         L.m6502_gemm_bf16.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
+        L.m6502_gemm_bf16_timed.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int,
+                                            P(ctypes.c_float)]
         L.m6502_exhaustive_static.argtypes = [ctypes.c_uint64, vp, vp, vp, vp, ctypes.c_uint8, ctypes.c_uint32,
                                               vp, vp]
         L.m6502_tune_get.argtypes = [vp, P(Tune)]

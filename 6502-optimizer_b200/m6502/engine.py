@@ -6,6 +6,7 @@ FlagDiff / Fingerprint / ShouldPrune keep the Go signatures and run on a
 shared default engine; the batch methods take many pairs at once.
 """
 import ctypes
+import sys
 import threading
 
 import numpy as np
@@ -37,6 +38,7 @@ class Engine:
         if rc != _lib.M6502_OK:
             raise M6502Error(rc, "m6502_create failed (no CUDA device?)")
         self._lock = threading.Lock()
+        self.device = device
 
     def close(self):
         if self._ctx:
@@ -56,6 +58,18 @@ class Engine:
     @property
     def stream(self):
         return self._L.m6502_stream(self._ctx)
+
+    def order_after_torch(self):
+        """Device inputs written by torch: the engine's stream is a
+        non-blocking stream, so it does not wait for torch's kernels by
+        itself.  Makes it wait for torch's current stream on this device
+        (an event, no host synchronisation).  Nothing to do when torch has
+        not initialised CUDA in this process."""
+        torch = sys.modules.get("torch")
+        if torch is None or not torch.cuda.is_initialized():
+            return
+        es = torch.cuda.ExternalStream(self.stream, device=self.device)
+        es.wait_stream(torch.cuda.current_stream(self.device))
 
     # ---- scheduling knobs (m6502_tune) ----
     @property
@@ -207,6 +221,7 @@ class Engine:
             tptr, n, tlen = device_ptr
             flags = _lib.TARGETS_ON_DEVICE
             keep = None
+            self.order_after_torch()
         else:
             keep = np.ascontiguousarray(np.asarray(targets, dtype=np.uint16))
             if keep.ndim != 2:

@@ -86,8 +86,27 @@ def gemm_bf16(engine, a, b):
     M, K = a.shape
     N = b.shape[0]
     c = torch.empty((M, N), dtype=torch.float32, device=a.device)
+    engine.order_after_torch()   # a, b (and c's memory) come from torch's stream
     rc = _lib.lib().m6502_gemm_bf16(engine._ctx, M, N, K, ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(b.data_ptr()),
                                     ctypes.c_void_p(c.data_ptr()))
     if rc != _lib.M6502_OK:
         raise M6502Error(rc, "m6502_gemm_bf16 failed")
     return c
+
+
+def gemm_bf16_timed(engine, a, b, reps):
+    """The same GEMM launched `reps` times back to back on the engine's
+    stream; returns (C of the last launch, mean device ms per launch from
+    CUDA events on that stream)."""
+    import torch
+    M, K = a.shape
+    N = b.shape[0]
+    c = torch.empty((M, N), dtype=torch.float32, device=a.device)
+    ms = ctypes.c_float(0.0)
+    engine.order_after_torch()
+    rc = _lib.lib().m6502_gemm_bf16_timed(engine._ctx, M, N, K, ctypes.c_void_p(a.data_ptr()),
+                                          ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(c.data_ptr()), int(reps),
+                                          ctypes.byref(ms))
+    if rc != _lib.M6502_OK:
+        raise M6502Error(rc, "m6502_gemm_bf16_timed failed")
+    return c, float(ms.value)

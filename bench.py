@@ -582,7 +582,7 @@ def run_gemm(args):
     512 x 512 over K = 65,536 rows).  One JSON line per shape."""
     import torch
     import m6502
-    from m6502.mlp import gemm_bf16
+    from m6502.mlp import gemm_bf16, gemm_bf16_timed
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
     shapes = [(args.gemm_n, args.gemm_n, args.gemm_n)]
@@ -596,7 +596,6 @@ def run_gemm(args):
         pass
     peak = peaks.get("bf16_tflops", 1590.0)
     eng = m6502.Engine(device=local)
-    stream = torch.cuda.ExternalStream(eng.stream, device=local)
     g = torch.Generator(device=f"cuda:{local}").manual_seed(0)
     for (M, N, K) in shapes:
         a = torch.randn(M, K, device=f"cuda:{local}", generator=g).to(torch.bfloat16)
@@ -611,14 +610,9 @@ def run_gemm(args):
         reps = max(args.steps, int(min(2000, max(1, 1e14 / flop))))
         clocks = ClockSampler(local)
         clocks.start()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            gemm_bf16(eng, a, b)
-        e1.record(stream)
-        torch.cuda.synchronize()
+        # back-to-back launches on the engine's stream, timed there by CUDA events
+        _, ms = gemm_bf16_timed(eng, a, b, reps)
         clk = clocks.stop()
-        ms = e0.elapsed_time(e1) / reps
         tflops = flop / (ms / 1e3) / 1e12
         square = M == N == K
         line = {"metric": "bf16 GEMM TFLOP/s (tcgen05, TMA, 128x256 tiles)", "value": tflops, "unit": "TFLOP/s",

@@ -405,6 +405,13 @@ int m6502_mlp_train(m6502_mlp *mlp, const m6502_mlp_example *ex, uint64_t n, uin
  * row-major DEVICE pointers, K a multiple of 64.  (The MLP's GEMM, exposed
  * for testing.) */
 int m6502_gemm_bf16(m6502_ctx *ctx, int M, int N, int K, const void *A, const void *B, float *C);
+/* The same GEMM launched `reps` times back to back on the context's stream
+ * with no host synchronisation between launches; *ms_per_launch (may be
+ * NULL) gets the mean device time per launch from CUDA events recorded on
+ * that stream around the launches.  C holds the result of the last launch.
+ * (For benchmarking the kernel alone.) */
+int m6502_gemm_bf16_timed(m6502_ctx *ctx, int M, int N, int K, const void *A, const void *B, float *C, int reps,
+                          float *ms_per_launch);
 
 /* ---- host helpers (no GPU needed) ---- */
 /* The 2863 instructions in CUDA order (cuda/6502_search_v2.cu:741-752) or Go

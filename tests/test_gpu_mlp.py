@@ -6,19 +6,23 @@ import pytest
 
 import mlp_ref
 from m6502 import inst as I
-from m6502.mlp import MLP, gemm_bf16
+from m6502.mlp import MLP, gemm_bf16, gemm_bf16_timed
 
 pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("M,N,K", [(128, 128, 64), (256, 384, 320), (300, 200, 128), (1024, 512, 512),
-                                   (512, 320, 4096), (128, 256, 2368), (512, 512, 65536)])
+                                   (512, 320, 4096), (128, 256, 2368), (512, 512, 65536), (4096, 1024, 1024),
+                                   (65536, 512, 448), (1000, 384, 512)])
 def test_tcgen05_gemm_matches_torch_fp32(engine, M, N, K):
     """C = A . B^T with bf16 operands: products are exact in fp32, so the only
     difference from the fp32 reference is summation order (tolerance 1e-4 of
     the row scale).  The last three shapes split K across CTAs (37 K blocks
     in 8 uneven splits; 1,024 in 19); the partial tiles are summed in a fixed
-    order, so a second call is bit-identical."""
+    order, so a second call is bit-identical.  K ranges of at most 8 blocks
+    run the two-stage kernel (two CTAs per SM), longer ones the four-stage
+    kernel ((4096, 1024, 1024) and the 65,536-deep split); (65536, 512, 448)
+    is the proposal network's first layer at its largest batch."""
     import torch
     g = torch.Generator(device="cuda").manual_seed(M * 7 + N * 13 + K)
     a = torch.randn((M, K), generator=g, device="cuda").to(torch.bfloat16)
@@ -29,6 +33,20 @@ def test_tcgen05_gemm_matches_torch_fp32(engine, M, N, K):
     assert err <= 1e-4 * ref.abs().max().item() + 1e-3, err
     # second call on the same inputs: identical result (no stale accumulator)
     assert torch.equal(gemm_bf16(engine, a, b), c)
+
+
+@pytest.mark.parametrize("M,N,K", [(65536, 512, 512), (4096, 1024, 1024)])
+def test_tcgen05_gemm_timed_launches_match(engine, M, N, K):
+    """Back-to-back launches without host synchronisation (the benchmark's
+    entry point) give the single call's result bit for bit."""
+    import torch
+    g = torch.Generator(device="cuda").manual_seed(M + N + K)
+    a = torch.randn((M, K), generator=g, device="cuda").to(torch.bfloat16)
+    b = torch.randn((N, K), generator=g, device="cuda").to(torch.bfloat16)
+    c1 = gemm_bf16(engine, a, b)
+    c5, ms = gemm_bf16_timed(engine, a, b, 5)
+    assert torch.equal(c1, c5)
+    assert ms > 0
 
 
 def _examples(n, seed):
