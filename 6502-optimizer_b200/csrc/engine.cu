@@ -421,44 +421,48 @@ __device__ __forceinline__ uint64_t probe_z(uint64_t salt, int i) {
 // Per-warp memory of the target last probed and composed, in shared memory
 // so that nothing of it stays in registers across the pair loop.
 struct TargetCache {
-    uint64_t probe_id;        // target whose probe outputs `out` holds (kNoTarget: none)
+    uint64_t probe_id[2];     // per probe round: target whose states `in` / `out` hold (kNoTarget: none)
     uint64_t flow_id;         // target whose composition `dt` / wt / st hold
-    uint64_t out[2][32];      // per lane: the target's outputs on probe states lane, lane + 32
+    uint64_t in[2][32];       // per lane: probe input states lane, lane + 32 (packed)
+    uint64_t out[2][32];      // per lane: the target's outputs on them (packed)
     uint32_t dt[32];          // per lane: the target's composed dependencies
     uint32_t wt, st;          // locations the target writes / sweeps
 };
 
 // The probe of one pair: 64 pseudo-random states of its whole sweep domain,
 // drawn from the target's salt when the source says which pairs share a
-// target (`tid`), else from the pair's.  The target's outputs on the states
-// are kept in the warp's cache when the pair's domain is the target's own
-// (the candidate reads no other register); a later pair of the same target
-// with the same domain then runs only its candidate.  One exec site.  False
-// when a state differs.
+// target (`tid`), else from the pair's.  When the pair's domain is the
+// target's own (the candidate reads no other register) each round's input
+// states and the target's outputs on them are kept in the warp's cache, per
+// round; a later pair of the same target then unpacks its inputs and runs
+// only its candidate.  Outputs are compared packed under the compare mask.
+// One exec site.  False when a state differs.
 __device__ __forceinline__ bool probe_pair(const PairView& pv, uint32_t sw_t, uint32_t sw_c, bool rep, uint64_t tid,
                                            uint64_t p, TargetCache& tc, int lane) {
     const uint64_t salt = tid != kNoTarget ? tid * 0xD1B54A32D192ED03ull + 0x632BE59BD9B4E019ull : p;
     const bool same = tid != kNoTarget && (sw_c & ~sw_t) == 0;   // uniform
-    const bool hit = same && tc.probe_id == tid;
-    if (same && !hit) tc.probe_id = kNoTarget;   // being refilled; valid again once both rounds are in
     const uint32_t swu = sw_t | sw_c | LB(L_A) | LB(L_C);
-    const OutMask m = out_mask(cmp_mask(pv.dead));
+    const uint64_t m64 = cmp_mask(pv.dead);
     const int n = pv.tn + pv.cn;
     for (int r = 0; r < 2; r++) {   // 32 states at a time: most failing pairs fail in the first
-        const St in = probe_state(swu, rep, probe_z(salt, lane + 32 * r));
+        const bool hit = same && tc.probe_id[r] == tid;   // uniform
+        const St in = hit ? unpack(tc.in[r][lane]) : probe_state(swu, rep, probe_z(salt, lane + 32 * r));
         St ps = in, ts = in;
-        if (hit) ts = unpack(tc.out[r][lane]);   // the target's outputs on this state, kept
         for (int i = hit ? pv.tn : 0; i < n; i++) {
             if (i == pv.tn && !hit) { ts = ps; ps = in; }   // the target is done: the candidate starts
             exec(ps, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
         }
         if (pv.cn == 0 && !hit) { ts = ps; ps = in; }
-        if (same && !hit) tc.out[r][lane] = pack(ts);
-        if (__any_sync(kFull, out_diff(ts, ps, m) != 0)) return false;
+        const uint64_t tp = hit ? tc.out[r][lane] : pack(ts);
+        if (same && !hit) {   // every lane read probe_id[r] above, before this sync
+            tc.in[r][lane] = pack(in);
+            tc.out[r][lane] = tp;
+            __syncwarp();
+            if (lane == 0) tc.probe_id[r] = tid;
+            __syncwarp();
+        }
+        if (__any_sync(kFull, ((pack(ps) ^ tp) & m64) != 0)) return false;
     }
-    __syncwarp();
-    if (same && !hit && lane == 0) tc.probe_id = tid;
-    __syncwarp();
     return true;
 }
 
@@ -1353,7 +1357,7 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
     unsigned long long nstates = 0, probe_rej = 0;
     __shared__ TargetCache s_tc[kWarpsPerBlock];   // the warp's last target: probe outputs, composition
     TargetCache& tc = s_tc[threadIdx.x >> 5];
-    if ((threadIdx.x & 31) == 0) { tc.probe_id = kNoTarget; tc.flow_id = kNoTarget; }
+    if ((threadIdx.x & 31) == 0) { tc.probe_id[0] = tc.probe_id[1] = kNoTarget; tc.flow_id = kNoTarget; }
     __syncwarp();
     unsigned long long next = 0, lim = 0;   // this warp's batch of tickets
     const unsigned long long tbatch = a.ticket_batch ? a.ticket_batch : kTicketBatch;
