@@ -419,51 +419,76 @@ __device__ __forceinline__ uint64_t probe_z(uint64_t salt, int i) {
 }
 
 // Per-warp memory of the target last probed and composed, in shared memory
-// so that nothing of it stays in registers across the pair loop.
+// so that nothing of it stays in registers across the pair loop.  The probe
+// states are stored field-major (field f of lane l at [f][l]): one
+// conflict-free 32-bit access per field.
 struct TargetCache {
-    uint64_t probe_id[2];     // per probe round: target whose states `in` / `out` hold (kNoTarget: none)
+    uint64_t probe_id;        // target whose probe states `in4` / `out4` hold (kNoTarget: none)
     uint64_t flow_id;         // target whose composition `dt` / wt / st hold
-    uint64_t in[2][32];       // per lane: probe input states lane, lane + 32 (packed)
-    uint64_t out[2][32];      // per lane: the target's outputs on them (packed)
+    uint32_t in4[8][32];      // per lane: four probe input states packed one per byte
+    uint32_t out4[8][32];     // per lane: the target's outputs on them, packed the same way
     uint32_t dt[32];          // per lane: the target's composed dependencies
     uint32_t wt, st;          // locations the target writes / sweeps
 };
 
-// The probe of one pair: 64 pseudo-random states of its whole sweep domain,
-// drawn from the target's salt when the source says which pairs share a
-// target (`tid`), else from the pair's.  When the pair's domain is the
-// target's own (the candidate reads no other register) each round's input
-// states and the target's outputs on them are kept in the warp's cache, per
-// round; a later pair of the same target then unpacks its inputs and runs
-// only its candidate.  Outputs are compared packed under the compare mask.
-// One exec site.  False when a state differs.
+__device__ __forceinline__ St st_load(const uint32_t (*a)[32], int lane) {
+    St s;
+    s.a = a[0][lane]; s.x = a[1][lane]; s.y = a[2][lane]; s.p = a[3][lane];
+    s.s = a[4][lane]; s.m = a[5][lane]; s.s0 = a[6][lane]; s.s1 = a[7][lane];
+    return s;
+}
+__device__ __forceinline__ void st_store(uint32_t (*a)[32], int lane, const St& s) {
+    a[0][lane] = s.a; a[1][lane] = s.x; a[2][lane] = s.y; a[3][lane] = s.p;
+    a[4][lane] = s.s; a[5][lane] = s.m; a[6][lane] = s.s0; a[7][lane] = s.s1;
+}
+
+// Probe states lane + 32 k, k = 0..3, packed one per byte (state k in byte
+// k of every field; see exec_x4).
+__device__ __forceinline__ St probe_state_x4(uint32_t swept, bool rep, uint64_t salt, int lane) {
+    St o{0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const St s = probe_state(swept, rep, probe_z(salt, lane + 32 * k));
+        const int sh = 8 * k;
+        o.a |= s.a << sh; o.x |= s.x << sh; o.y |= s.y << sh; o.p |= s.p << sh;
+        o.s |= s.s << sh; o.m |= s.m << sh; o.s0 |= s.s0 << sh; o.s1 |= s.s1 << sh;
+    }
+    return o;
+}
+
+// The probe of one pair: 128 pseudo-random states of its whole sweep domain,
+// four per lane packed one per byte (one exec_x4 dispatch per instruction
+// for four states), drawn from the target's salt when the source says which
+// pairs share a target (`tid`), else from the pair's.  When the pair's
+// domain is the target's own (the candidate reads no other register) the
+// packed input states and the target's outputs on them are kept in the
+// warp's cache; a later pair of the same target then loads its inputs and
+// runs only its candidate.  One exec site.  False when a state differs.
 __device__ __forceinline__ bool probe_pair(const PairView& pv, uint32_t sw_t, uint32_t sw_c, bool rep, uint64_t tid,
                                            uint64_t p, TargetCache& tc, int lane) {
     const uint64_t salt = tid != kNoTarget ? tid * 0xD1B54A32D192ED03ull + 0x632BE59BD9B4E019ull : p;
     const bool same = tid != kNoTarget && (sw_c & ~sw_t) == 0;   // uniform
+    const bool hit = same && tc.probe_id == tid;                  // uniform
     const uint32_t swu = sw_t | sw_c | LB(L_A) | LB(L_C);
-    const uint64_t m64 = cmp_mask(pv.dead);
     const int n = pv.tn + pv.cn;
-    for (int r = 0; r < 2; r++) {   // 32 states at a time: most failing pairs fail in the first
-        const bool hit = same && tc.probe_id[r] == tid;   // uniform
-        const St in = hit ? unpack(tc.in[r][lane]) : probe_state(swu, rep, probe_z(salt, lane + 32 * r));
-        St ps = in, ts = in;
-        for (int i = hit ? pv.tn : 0; i < n; i++) {
-            if (i == pv.tn && !hit) { ts = ps; ps = in; }   // the target is done: the candidate starts
-            exec(ps, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
-        }
-        if (pv.cn == 0 && !hit) { ts = ps; ps = in; }
-        const uint64_t tp = hit ? tc.out[r][lane] : pack(ts);
-        if (same && !hit) {   // every lane read probe_id[r] above, before this sync
-            tc.in[r][lane] = pack(in);
-            tc.out[r][lane] = tp;
-            __syncwarp();
-            if (lane == 0) tc.probe_id[r] = tid;
-            __syncwarp();
-        }
-        if (__any_sync(kFull, ((pack(ps) ^ tp) & m64) != 0)) return false;
+    const St in = hit ? st_load(tc.in4, lane) : probe_state_x4(swu, rep, salt, lane);
+    St ps = in, ts = in;
+    for (int i = hit ? pv.tn : 0; i < n; i++) {
+        if (i == pv.tn && !hit) { ts = ps; ps = in; }   // the target is done: the candidate starts
+        exec_x4(ps, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
     }
-    return true;
+    if (pv.cn == 0 && !hit) { ts = ps; ps = in; }
+    if (hit) ts = st_load(tc.out4, lane);
+    if (same && !hit) {   // every lane read probe_id above, before this sync
+        st_store(tc.in4, lane, in);
+        st_store(tc.out4, lane, ts);
+        __syncwarp();
+        if (lane == 0) tc.probe_id = tid;
+        __syncwarp();
+    }
+    OutMask m = out_mask(cmp_mask(pv.dead));
+    m.a *= kB1; m.x *= kB1; m.y *= kB1; m.p *= kB1; m.s *= kB1; m.m *= kB1; m.s0 *= kB1; m.s1 *= kB1;
+    return !__any_sync(kFull, out_diff(ts, ps, m) != 0);
 }
 
 // Four consecutive states s..s+3 (s a multiple of 4) packed one per byte
@@ -1357,7 +1382,7 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
     unsigned long long nstates = 0, probe_rej = 0;
     __shared__ TargetCache s_tc[kWarpsPerBlock];   // the warp's last target: probe outputs, composition
     TargetCache& tc = s_tc[threadIdx.x >> 5];
-    if ((threadIdx.x & 31) == 0) { tc.probe_id[0] = tc.probe_id[1] = kNoTarget; tc.flow_id = kNoTarget; }
+    if ((threadIdx.x & 31) == 0) { tc.probe_id = kNoTarget; tc.flow_id = kNoTarget; }
     __syncwarp();
     unsigned long long next = 0, lim = 0;   // this warp's batch of tickets
     const unsigned long long tbatch = a.ticket_batch ? a.ticket_batch : kTicketBatch;

@@ -30,6 +30,7 @@ import sys
 import tempfile
 import time
 
+PROBE_STATES = 128   # random domain states k_exhaustive tries on every pair before its cone sweeps
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "6502-optimizer_b200"))
 
@@ -308,7 +309,7 @@ def run_engine(args):
         exh_ms = avg("ms_exhaustive") + avg("ms_exh_items")
         qc_ms = avg("ms_qc")
         exh_achieved = s0["exh_algo_ops"] / (exh_ms / 1e3) if exh_ms > 0 else 0.0
-        exh_exec = ((s0["exh_states"] + 64 * s0["exh_checked"]) * (10 * 3 + 3) / (exh_ms / 1e3)
+        exh_exec = ((s0["exh_states"] + PROBE_STATES * s0["exh_checked"]) * (10 * 3 + 3) / (exh_ms / 1e3)
                     if exh_ms > 0 else 0.0)
         qc_algo = 13 * s0["pairs"] + 13 * (7 + 24) * s0["qc_hits"]
         qc_achieved = qc_algo / (qc_ms / 1e3) if qc_ms > 0 else 0.0
@@ -324,9 +325,9 @@ def run_engine(args):
             kernels, ktime = ("k_qc_join",), qc_ms
         else:
             # states the two exhaustive kernels evaluated (cone sweeps, work items and
-            # the 64-state random probes) at the convention's 10 ops per executed
+            # the 128-state random probes) at the convention's 10 ops per executed
             # instruction + 3 per compare
-            achieved, alg = exh_exec, ("states evaluated (cone sweeps + items + 64-state probes) x "
+            achieved, alg = exh_exec, ("states evaluated (cone sweeps + items + 128-state probes) x "
                                        "(10 ops/instruction x 3 instructions + 3)")
             kernels, ktime = exh_kernels, exh_ms
         traffic = sum(figs[k]["traffic"] for k in kernels if k in figs) if all(k in figs for k in kernels) else None
