@@ -442,17 +442,36 @@ __device__ __forceinline__ void st_store(uint32_t (*a)[32], int lane, const St& 
     a[4][lane] = s.s; a[5][lane] = s.m; a[6][lane] = s.s0; a[7][lane] = s.s1;
 }
 
-// Probe states lane + 32 k, k = 0..3, packed one per byte (state k in byte
-// k of every field; see exec_x4).
+// 128 random states of a pair's sweep domain, four per lane packed one per
+// byte (state k in byte k of every field; see exec_x4).  Under the full
+// sweep every packed field of a swept register is 32 random bits (four
+// independent uniform bytes), the carry one random bit per byte, and the
+// other fields hold the sweep's fixed values (S = 0xFD, the rest 0, the
+// other flags clear): four splitmix64 words per lane.  Under the reduced
+// sweep each byte of an extra register is a representative value
+// (c_rep[byte & 31]), drawn state by state through probe_state.
 __device__ __forceinline__ St probe_state_x4(uint32_t swept, bool rep, uint64_t salt, int lane) {
     St o{0, 0, 0, 0, 0, 0, 0, 0};
+    if (rep) {
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const St s = probe_state(swept, rep, probe_z(salt, lane + 32 * k));
-        const int sh = 8 * k;
-        o.a |= s.a << sh; o.x |= s.x << sh; o.y |= s.y << sh; o.p |= s.p << sh;
-        o.s |= s.s << sh; o.m |= s.m << sh; o.s0 |= s.s0 << sh; o.s1 |= s.s1 << sh;
+        for (int k = 0; k < 4; k++) {
+            const St s = probe_state(swept, true, probe_z(salt, lane + 32 * k));
+            const int sh = 8 * k;
+            o.a |= s.a << sh; o.x |= s.x << sh; o.y |= s.y << sh; o.p |= s.p << sh;
+            o.s |= s.s << sh; o.m |= s.m << sh; o.s0 |= s.s0 << sh; o.s1 |= s.s1 << sh;
+        }
+        return o;
     }
+    const uint64_t z0 = probe_z(salt, lane), z1 = probe_z(salt, lane + 32), z2 = probe_z(salt, lane + 64),
+                   z3 = probe_z(salt, lane + 96);
+    o.a = (uint32_t)z0;
+    o.x = (swept & LB(L_X)) ? (uint32_t)(z0 >> 32) : 0u;
+    o.y = (swept & LB(L_Y)) ? (uint32_t)z1 : 0u;
+    o.s = (swept & LB(L_S)) ? (uint32_t)(z1 >> 32) : 0xFDu * kB1;
+    o.m = (swept & LB(L_M)) ? (uint32_t)z2 : 0u;
+    o.s0 = (swept & LB(L_S0)) ? (uint32_t)(z2 >> 32) : 0u;
+    o.s1 = (swept & LB(L_S1)) ? (uint32_t)z3 : 0u;
+    o.p = (uint32_t)(z3 >> 32) & kB1;
     return o;
 }
 
