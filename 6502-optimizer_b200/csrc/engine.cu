@@ -96,11 +96,19 @@ __constant__ uint64_t c_vec[32];             // packed test vectors
 __constant__ uint16_t c_dep[NUM_OPS][NUM_LOCS];
 __constant__ uint16_t c_wr[NUM_OPS];          // written locations per opcode
 __constant__ uint16_t c_sweep[NUM_OPS];       // swept locations implied by opReads
+__constant__ uint32_t c_x4d[NUM_OPS];         // packed-executor descriptors (x4_desc)
 __constant__ uint16_t c_tab[kNumInsns];       // instructions, CUDA order
 __constant__ uint16_t c_gotab[kNumInsns];     // instructions, Go order
 __constant__ uint32_t c_gorank[kNumInsns];    // Go-order rank of CUDA index i
 __constant__ uint16_t c_goidx[kNumInsns];     // CUDA index of Go rank r
 __constant__ uint32_t c_rep[32];
+
+// Packed-executor descriptor of an instruction (an opcode outside the table
+// runs as NOP, as exec leaves the state unchanged for it).
+__device__ __forceinline__ uint32_t desc_x4(uint32_t insn) {
+    const uint32_t op = insn & 0xFFu;
+    return op < NUM_OPS ? c_x4d[op] : (uint32_t)X4_NOP;
+}
 
 // ---------------------------------------------------------------------------
 // Host tables
@@ -494,7 +502,8 @@ __device__ __forceinline__ bool probe_pair(const PairView& pv, uint32_t sw_t, ui
     St ps = in, ts = in;
     for (int i = hit ? pv.tn : 0; i < n; i++) {
         if (i == pv.tn && !hit) { ts = ps; ps = in; }   // the target is done: the candidate starts
-        exec_x4(ps, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
+        const uint32_t insn = i < pv.tn ? pv.t[i] : pv.c[i - pv.tn];
+        exec_x4d(ps, insn, desc_x4(insn));
     }
     if (pv.cn == 0 && !hit) { ts = ps; ps = in; }
     if (hit) ts = st_load(tc.out4, lane);
@@ -536,12 +545,20 @@ __device__ __forceinline__ St decode_x4(const Fields& f, uint64_t s) {
     return o;
 }
 
+// DESC: run the instructions through their descriptors (exec_x4d, a
+// 12-way class switch) instead of the per-opcode switch (exec_x4).  The
+// descriptors pay off where the warps of an SM hop between different pairs
+// (fewer branch targets to fetch); long sweeps of one pair prefer the
+// specialised cases.
+template <bool DESC>
 __device__ __forceinline__ uint32_t state_diff_x4(const PairView& pv, const Fields& f, const OutMask& m4, uint64_t s) {
     St c = decode_x4(f, s), t = c;
     const int n = pv.tn + pv.cn;
     for (int i = 0; i < n; i++) {
         if (i == pv.tn) { t = c; c = decode_x4(f, s); }
-        exec_x4(c, i < pv.tn ? pv.t[i] : pv.c[i - pv.tn]);
+        const uint32_t insn = i < pv.tn ? pv.t[i] : pv.c[i - pv.tn];
+        if (DESC) exec_x4d(c, insn, desc_x4(insn));
+        else exec_x4(c, insn);
     }
     if (pv.cn == 0) { t = c; c = decode_x4(f, s); }
     return out_diff(t, c, m4);
@@ -555,7 +572,7 @@ __device__ __forceinline__ uint32_t state_diff_x4(const PairView& pv, const Fiel
 // (exec_x4: one dispatch, byte-parallel arithmetic); 2: two states per lane
 // and dispatch; 1: one.  The packed path needs 4-aligned ranges and a
 // lowest field of at least 2 bits, and falls back to one state per lane.
-template <int PER_LANE>
+template <int PER_LANE, bool DESC = false>
 __device__ __forceinline__ bool sweep_states(const PairView& pv, const Fields& f, uint64_t om, uint64_t s0,
                                              uint64_t s1, const volatile uint32_t* stop, unsigned long long* nstates,
                                              int lane) {
@@ -572,7 +589,7 @@ __device__ __forceinline__ bool sweep_states(const PairView& pv, const Fields& f
         uint32_t d = 0;
         if (PER_LANE == 4) {
             const uint64_t s4 = b + 4 * (uint64_t)lane;
-            d = s4 < s1 ? state_diff_x4(pv, f, m, s4) : 0u;
+            d = s4 < s1 ? state_diff_x4<DESC>(pv, f, m, s4) : 0u;
         } else if (PER_LANE == 2) {
             const uint64_t sb = sa + 32;   // past the end: evaluate a state in range again
             d = sa < s1 ? state_diff2(pv, f, m, sa, sb < s1 ? sb : sa) : 0u;
@@ -1466,7 +1483,7 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
             Fields f = make_fields(cone, fl.swept, rep);
             const uint64_t total = 1ull << bits;
             const uint64_t end = total <= kSmallSweep ? total : kProbe;
-            ok = sweep_states<4>(pv, f, mask, 0, end, nullptr, &nstates, lane);
+            ok = sweep_states<4, true>(pv, f, mask, 0, end, nullptr, &nstates, lane);
             if (ok && end < total) big |= 1u << o;
         }
         if (ok && big) {
@@ -2086,6 +2103,9 @@ int init_ctx(m6502_ctx* ctx) {
     CK(cudaMemcpyToSymbol(c_dep, dep, sizeof dep));
     CK(cudaMemcpyToSymbol(c_wr, wr, sizeof wr));
     CK(cudaMemcpyToSymbol(c_sweep, sw, sizeof sw));
+    uint32_t x4[NUM_OPS];
+    for (uint32_t op = 0; op < NUM_OPS; op++) x4[op] = x4_desc(op);
+    CK(cudaMemcpyToSymbol(c_x4d, x4, sizeof x4));
     CK(cudaMemcpyToSymbol(c_tab, tab, sizeof tab));
     CK(cudaMemcpyToSymbol(c_gotab, gotab, sizeof gotab));
     CK(cudaMemcpyToSymbol(c_gorank, gorank, sizeof gorank));
@@ -3299,12 +3319,14 @@ int static_setup(int dev, StaticDevice** out) {
             wr[op] = (uint16_t)op_deps(op, dep[op]);
             sw[op] = (uint16_t)sweep_locs_of_reads(op_reads(op));
         }
-        uint32_t rep[32];
+        uint32_t rep[32], x4[NUM_OPS];
         for (int i = 0; i < 32; i++) rep[i] = kRepValues[i];
+        for (uint32_t op = 0; op < NUM_OPS; op++) x4[op] = x4_desc(op);
         if (cudaMemcpyToSymbol(c_vec, vec, sizeof vec) != cudaSuccess ||
             cudaMemcpyToSymbol(c_dep, dep, sizeof dep) != cudaSuccess ||
             cudaMemcpyToSymbol(c_wr, wr, sizeof wr) != cudaSuccess ||
             cudaMemcpyToSymbol(c_sweep, sw, sizeof sw) != cudaSuccess ||
+            cudaMemcpyToSymbol(c_x4d, x4, sizeof x4) != cudaSuccess ||
             cudaMemcpyToSymbol(c_rep, rep, sizeof rep) != cudaSuccess)
             return M6502_E_CUDA;
         void* ptr = nullptr;

@@ -321,6 +321,160 @@ M6502_HD void exec_x4(St& s, uint32_t insn) {
     }
 }
 
+// ---- Four states per register through per-opcode descriptors ----
+//
+// exec_x4d runs an instruction from a small descriptor instead of one case
+// per opcode: the 58 opcodes fall into 12 classes (bits 0-3), parameterised
+// by a source (bits 4-6) and a destination / register operand (bits 7-9)
+// among A, X, Y, S, M and the immediate, a sub-operation (bits 10-11), and
+// for the flag instructions the P bits to clear (16-23) and set (24-31).
+// A warp runs the same instruction on every lane, so the class switch has
+// 12 targets instead of 58 and the register selects are uniform.  Results
+// equal exec_x4's (tests/x4_check.cpp checks every instruction).
+enum : uint32_t {
+    X4_NOP, X4_MOVE_NZ, X4_MOVE, X4_INCDEC, X4_SHIFT, X4_FLAG, X4_ADDSUB, X4_LOGIC, X4_CMP, X4_PUSH, X4_PLA, X4_PLP,
+    X4_BIT
+};
+enum : uint32_t { X4R_A = 0, X4R_X = 1, X4R_Y = 2, X4R_S = 3, X4R_M = 4, X4R_IMM = 7 };
+
+M6502_HD constexpr uint32_t x4d(uint32_t cls, uint32_t src = 0, uint32_t dst = 0, uint32_t sub = 0,
+                                uint32_t clr = 0, uint32_t set = 0) {
+    return cls | (src << 4) | (dst << 7) | (sub << 10) | (clr << 16) | (set << 24);
+}
+
+// The descriptor of an opcode (semantics of pkg/cpu/exec.go:8-189).
+M6502_HD uint32_t x4_desc(uint32_t op) {
+    switch (op) {
+    case TAX: return x4d(X4_MOVE_NZ, X4R_A, X4R_X);
+    case TAY: return x4d(X4_MOVE_NZ, X4R_A, X4R_Y);
+    case TXA: return x4d(X4_MOVE_NZ, X4R_X, X4R_A);
+    case TYA: return x4d(X4_MOVE_NZ, X4R_Y, X4R_A);
+    case TSX: return x4d(X4_MOVE_NZ, X4R_S, X4R_X);
+    case TXS: return x4d(X4_MOVE, X4R_X, X4R_S);
+    case INX: return x4d(X4_INCDEC, 0, X4R_X, 0);
+    case INY: return x4d(X4_INCDEC, 0, X4R_Y, 0);
+    case DEX: return x4d(X4_INCDEC, 0, X4R_X, 1);
+    case DEY: return x4d(X4_INCDEC, 0, X4R_Y, 1);
+    case ASL_A: return x4d(X4_SHIFT, 0, X4R_A, 0);
+    case LSR_A: return x4d(X4_SHIFT, 0, X4R_A, 1);
+    case ROL_A: return x4d(X4_SHIFT, 0, X4R_A, 2);
+    case ROR_A: return x4d(X4_SHIFT, 0, X4R_A, 3);
+    case CLC: return x4d(X4_FLAG, 0, 0, 0, kFlagC, 0);
+    case SEC: return x4d(X4_FLAG, 0, 0, 0, 0, kFlagC);
+    case CLD: return x4d(X4_FLAG, 0, 0, 0, kFlagD, 0);
+    case SED: return x4d(X4_FLAG, 0, 0, 0, 0, kFlagD);
+    case CLI: return x4d(X4_FLAG, 0, 0, 0, kFlagI, 0);
+    case SEI: return x4d(X4_FLAG, 0, 0, 0, 0, kFlagI);
+    case CLV: return x4d(X4_FLAG, 0, 0, 0, kFlagV, 0);
+    case PHA: return x4d(X4_PUSH, 0, 0, 0);
+    case PHP: return x4d(X4_PUSH, 0, 0, 1);
+    case PLA: return x4d(X4_PLA);
+    case PLP: return x4d(X4_PLP);
+    case LDA_IMM: return x4d(X4_MOVE_NZ, X4R_IMM, X4R_A);
+    case LDX_IMM: return x4d(X4_MOVE_NZ, X4R_IMM, X4R_X);
+    case LDY_IMM: return x4d(X4_MOVE_NZ, X4R_IMM, X4R_Y);
+    case ADC_IMM: return x4d(X4_ADDSUB, X4R_IMM, 0, 0);
+    case SBC_IMM: return x4d(X4_ADDSUB, X4R_IMM, 0, 1);
+    case AND_IMM: return x4d(X4_LOGIC, X4R_IMM, 0, 0);
+    case ORA_IMM: return x4d(X4_LOGIC, X4R_IMM, 0, 1);
+    case EOR_IMM: return x4d(X4_LOGIC, X4R_IMM, 0, 2);
+    case CMP_IMM: return x4d(X4_CMP, X4R_IMM, X4R_A);
+    case CPX_IMM: return x4d(X4_CMP, X4R_IMM, X4R_X);
+    case CPY_IMM: return x4d(X4_CMP, X4R_IMM, X4R_Y);
+    case LDA_M: return x4d(X4_MOVE_NZ, X4R_M, X4R_A);
+    case LDX_M: return x4d(X4_MOVE_NZ, X4R_M, X4R_X);
+    case LDY_M: return x4d(X4_MOVE_NZ, X4R_M, X4R_Y);
+    case STA_M: return x4d(X4_MOVE, X4R_A, X4R_M);
+    case STX_M: return x4d(X4_MOVE, X4R_X, X4R_M);
+    case STY_M: return x4d(X4_MOVE, X4R_Y, X4R_M);
+    case ADC_M: return x4d(X4_ADDSUB, X4R_M, 0, 0);
+    case SBC_M: return x4d(X4_ADDSUB, X4R_M, 0, 1);
+    case AND_M: return x4d(X4_LOGIC, X4R_M, 0, 0);
+    case ORA_M: return x4d(X4_LOGIC, X4R_M, 0, 1);
+    case EOR_M: return x4d(X4_LOGIC, X4R_M, 0, 2);
+    case CMP_M: return x4d(X4_CMP, X4R_M, X4R_A);
+    case CPX_M: return x4d(X4_CMP, X4R_M, X4R_X);
+    case CPY_M: return x4d(X4_CMP, X4R_M, X4R_Y);
+    case INC_M: return x4d(X4_INCDEC, 0, X4R_M, 0);
+    case DEC_M: return x4d(X4_INCDEC, 0, X4R_M, 1);
+    case ASL_M: return x4d(X4_SHIFT, 0, X4R_M, 0);
+    case LSR_M: return x4d(X4_SHIFT, 0, X4R_M, 1);
+    case ROL_M: return x4d(X4_SHIFT, 0, X4R_M, 2);
+    case ROR_M: return x4d(X4_SHIFT, 0, X4R_M, 3);
+    case BIT_M: return x4d(X4_BIT);
+    default: return x4d(X4_NOP);
+    }
+}
+
+// Register operand `r` (X4R_*) of a packed state; X4R_IMM gives immw.
+M6502_HD uint32_t x4_reg(const St& s, uint32_t r, uint32_t immw) {
+    uint32_t v = immw;
+    v = r == X4R_A ? s.a : v;
+    v = r == X4R_X ? s.x : v;
+    v = r == X4R_Y ? s.y : v;
+    v = r == X4R_S ? s.s : v;
+    v = r == X4R_M ? s.m : v;
+    return v;
+}
+M6502_HD void x4_set_reg(St& s, uint32_t r, uint32_t v) {
+    s.a = r == X4R_A ? v : s.a;
+    s.x = r == X4R_X ? v : s.x;
+    s.y = r == X4R_Y ? v : s.y;
+    s.s = r == X4R_S ? v : s.s;
+    s.m = r == X4R_M ? v : s.m;
+}
+
+// One instruction (insn = op | imm << 8, descriptor d = x4_desc(op)) on the
+// four states packed in s.
+M6502_HD void exec_x4d(St& s, uint32_t insn, uint32_t d) {
+    const uint32_t immw = (insn >> 8) * kB1;
+    const uint32_t src = (d >> 4) & 7u, dst = (d >> 7) & 7u, sub = (d >> 10) & 3u;
+    switch (d & 15u) {
+    case X4_MOVE_NZ: {
+        const uint32_t v = x4_reg(s, src, immw);
+        x4_set_reg(s, dst, v);
+        x4_set_nz(s, v);
+    } break;
+    case X4_MOVE: x4_set_reg(s, dst, x4_reg(s, src, immw)); break;
+    case X4_INCDEC: {
+        const uint32_t v0 = x4_reg(s, dst, 0u);
+        const uint32_t v = sub ? x4_dec(v0) : x4_inc(v0);
+        x4_set_reg(s, dst, v);
+        x4_set_nz(s, v);
+    } break;
+    case X4_SHIFT: {   // sub: 0 ASL, 1 LSR, 2 ROL, 3 ROR
+        const uint32_t v = x4_reg(s, dst, 0u), cin = s.p & kB1;
+        const bool left = (sub & 1u) == 0, rot = sub >= 2;
+        uint32_t r = left ? (v & kL7) << 1 : (v >> 1) & kL7;
+        if (rot) r |= left ? cin : cin << 7;
+        const uint32_t c = left ? (v >> 7) & kB1 : v & kB1;
+        s.p = (s.p & (0x7Cu * kB1)) | x4_nzf(r) | c;
+        x4_set_reg(s, dst, r);
+    } break;
+    case X4_FLAG: s.p = (s.p & ~(((d >> 16) & 0xFFu) * kB1)) | (((d >> 24) & 0xFFu) * kB1); break;
+    case X4_ADDSUB: {   // sub 1: SBC, a + ~m + c
+        const uint32_t m = x4_reg(s, src, immw) ^ (sub ? 0xFFFFFFFFu : 0u);
+        uint32_t co;
+        const uint32_t r = x4_add(s.a, m, s.p & kB1, co);
+        const uint32_t v = (s.a ^ r) & (m ^ r) & kH;
+        s.p = (s.p & (0x3Cu * kB1)) | x4_nzf(r) | co | (v >> 1);
+        s.a = r;
+    } break;
+    case X4_LOGIC: {   // sub: 0 AND, 1 ORA, 2 EOR
+        const uint32_t m = x4_reg(s, src, immw);
+        const uint32_t r = sub == 0 ? (s.a & m) : sub == 1 ? (s.a | m) : (s.a ^ m);
+        s.a = r;
+        x4_set_nz(s, r);
+    } break;
+    case X4_CMP: x4_cmp(s, x4_reg(s, dst, 0u), x4_reg(s, src, immw)); break;
+    case X4_PUSH: x4_push(s, sub ? (s.p | ((kFlagB | kFlagU) * kB1)) : s.a); break;
+    case X4_PLA: s.a = x4_pull(s); x4_set_nz(s, s.a); break;
+    case X4_PLP: s.p = x4_pull(s); break;
+    case X4_BIT: s.p = (s.p & (0x3Du * kB1)) | (s.m & (0xC0u * kB1)) | (x4_zero(s.a & s.m) >> 6); break;
+    default: break;
+    }
+}
+
 M6502_HD uint64_t pack(const St& s) {
     return (uint64_t)(s.a | (s.x << 8) | (s.y << 16) | (s.p << 24)) |
            ((uint64_t)(s.s | (s.m << 8) | (s.s0 << 16) | (s.s1 << 24)) << 32);

@@ -1,6 +1,6 @@
-// Checks the four-states-per-register executor (exec_x4) against four
-// scalar exec calls for every instruction of the table on seeded random
-// states.  Built and run by tests/test_abi_host.py::test_swar_exec_matches_scalar.
+// Checks the four-states-per-register executors (exec_x4, and exec_x4d
+// driven by the per-opcode descriptors of x4_desc) against four scalar exec
+// calls for every instruction of the table on seeded random states.  Built and run by tests/test_abi_host.py::test_swar_exec_matches_scalar.
 #include <cstdio>
 #include <cstdint>
 
@@ -22,7 +22,7 @@ int main() {
         for (uint32_t imm = 0; imm < (has_imm(op) ? 256u : 1u); imm++) {
             const uint32_t insn = op | (imm << 8);
             for (int trial = 0; trial < 64; trial++) {
-                St one[4], packed{};
+                St one[4], packed{}, packed_d{};
                 for (int k = 0; k < 4; k++) {
                     one[k] = {next8(), next8(), next8(), next8(), next8(), next8(), next8(), next8()};
                     if (trial < 8) one[k].a = (trial * 4 + k) & 1 ? 0u : 0x80u;   // zero / sign edge cases
@@ -30,13 +30,17 @@ int main() {
                     uint32_t* g = &packed.a;
                     for (int i = 0; i < 8; i++) g[i] |= f[i] << (8 * k);
                 }
+                packed_d = packed;
                 exec_x4(packed, insn);
+                exec_x4d(packed_d, insn, x4_desc(op));
                 for (int k = 0; k < 4; k++) {
                     exec(one[k], insn);
                     const uint32_t* f = &one[k].a;
                     const uint32_t* g = &packed.a;
+                    const uint32_t* gd = &packed_d.a;
                     for (int i = 0; i < 8; i++) {
-                        if (((g[i] >> (8 * k)) & 0xFFu) != (f[i] & 0xFFu)) {
+                        if (((g[i] >> (8 * k)) & 0xFFu) != (f[i] & 0xFFu) ||
+                            ((gd[i] >> (8 * k)) & 0xFFu) != (f[i] & 0xFFu)) {
                             if (bad < 10) std::printf("mismatch op %u imm %u state %d field %d\n", op, imm, k, i);
                             bad++;
                         }
