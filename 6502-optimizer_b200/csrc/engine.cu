@@ -1438,20 +1438,22 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
         PairView pv;
         pv.t = s_t[w]; pv.c = s_c[w];
         src.load(p, s_t[w], s_c[w], pv.tn, pv.cn, pv.dead, lane);
+        const uint64_t tid = src.target_id(p);
+        const bool probed = src.probed(p);
         __syncwarp();
-        if (!src.probed(p)) {
+        if (!probed) {
             uint32_t sw_t = 0, sw_c = 0;
             for (int i = 0; i < pv.tn; i++) sw_t |= c_sweep[pv.t[i] & 0xFFu];
             for (int i = 0; i < pv.cn; i++) sw_c |= c_sweep[pv.c[i] & 0xFFu];
             const uint32_t sw = sw_t | sw_c;   // swept extra registers
             const bool prep = a.sweep == M6502_SWEEP_REFERENCE && __popc(sw) >= 3;
-            if (!probe_pair(pv, sw_t, sw_c, prep, src.target_id(p), p, tc, lane)) {
+            if (!probe_pair(pv, sw_t, sw_c, prep, tid, p, tc, lane)) {
                 if (lane == 0) { a.fail[p] = 1u; probe_rej++; }
                 __syncwarp();
                 continue;
             }
         }
-        Flow fl = dataflow_cached(pv, lane, s_dep, src.target_id(p), tc);
+        Flow fl = dataflow_cached(pv, lane, s_dep, tid, tc);
         const bool rep = a.sweep == M6502_SWEEP_REFERENCE && fl.k >= 3;
         LaneGroups lg;
         if (a.brute) {   // one group: the whole product space, every output
