@@ -158,18 +158,20 @@ constexpr uint32_t kNoRow = 0xFFFFFFFFu;
 // The model's input for every chain still searching: target, current
 // candidate and its vector mismatch mask (a chain about to (re)start uses
 // the target itself).  Chains of proved targets under stop_on_proof get no
-// row; the others get consecutive rows (row[ci]), so the forward pass runs
-// over the live chains only.
+// row, nor do the chains that keep the uniform proposal (the first
+// `uniform8` of every 8 chains of a target); the others get consecutive
+// rows (row[ci]), so the forward pass runs over the live model-driven
+// chains only.
 __global__ void k_stoke_examples(const StokeChain* __restrict__ chains, uint32_t n_chains, uint32_t cpt,
                                  StokeTargets tg, const uint32_t* __restrict__ proven, uint32_t stop_on_proof,
-                                 m6502_mlp_example* __restrict__ ex, uint32_t* __restrict__ row,
+                                 uint32_t uniform8, m6502_mlp_example* __restrict__ ex, uint32_t* __restrict__ row,
                                  StokeCounters* __restrict__ sc) {
     const int lane = threadIdx.x & 31;
     for (uint32_t ci = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5); ci < n_chains;
          ci += gridDim.x * kWarpsPerBlock) {
         const StokeChain& ch = chains[ci];
         const uint32_t t = ci / cpt, t0 = tg.off[t], tlen = tg.off[t + 1] - t0;
-        if (ch.status == 2 || (stop_on_proof && proven[t])) {
+        if (ch.status == 2 || (stop_on_proof && proven[t]) || ((ci % cpt) & 7u) < uniform8) {
             if (lane == 0) row[ci] = kNoRow;
             continue;
         }
@@ -659,7 +661,8 @@ int m6502_stoke_run(m6502_ctx* ctx, const m6502_stoke_cfg* cfg, const uint16_t* 
         if (use_model) {   // refresh the learned proposal of the chains still searching
             k_stoke_examples<<<(n_chains + kWarpsPerBlock - 1) / kWarpsPerBlock, 256, 0, ctx->stream>>>(
                 (const StokeChain*)ctx->st_chains.p, n_chains, cpt, tg, (const uint32_t*)ctx->st_proven.p,
-                cfg->stop_on_proof, (m6502_mlp_example*)ctx->st_mex.p, (uint32_t*)ctx->st_row.p, sc);
+                cfg->stop_on_proof, std::min<uint32_t>(cfg->uniform_chains, 8u), (m6502_mlp_example*)ctx->st_mex.p,
+                (uint32_t*)ctx->st_row.p, sc);
             CKL("k_stoke_examples");
             unsigned long long rows = 0;
             CK(cudaMemcpyAsync(&rows, &sc->ex_rows, sizeof rows, cudaMemcpyDeviceToHost, ctx->stream));

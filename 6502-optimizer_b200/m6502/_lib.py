@@ -79,7 +79,8 @@ class StokeCfg(ctypes.Structure):
                 ("steps", ctypes.c_uint64), ("seed", ctypes.c_uint64), ("decay", ctypes.c_double),
                 ("t_start", ctypes.c_double), ("t_end", ctypes.c_double), ("cost", ctypes.c_uint32),
                 ("max_len", ctypes.c_uint32), ("sweep", ctypes.c_uint32), ("stop_on_proof", ctypes.c_uint32),
-                ("proposal", ctypes.c_uint32), ("dead_flags", ctypes.c_uint8), ("reserved", ctypes.c_uint8 * 3),
+                ("proposal", ctypes.c_uint32), ("dead_flags", ctypes.c_uint8), ("uniform_chains", ctypes.c_uint8),
+                ("reserved", ctypes.c_uint8 * 2),
                 ("learned_frac", ctypes.c_float), ("first_epoch", ctypes.c_uint32), ("model", ctypes.c_void_p),
                 ("trajectories", ctypes.c_void_p), ("traj_cap", ctypes.c_uint64),
                 ("traj_count", ctypes.POINTER(ctypes.c_uint64))]

@@ -264,7 +264,7 @@ class Engine:
     def stoke(self, targets, chains_per_target=128, steps=1_000_000, steps_per_epoch=1000, seed=0,
               cost=_lib.COST_REF, decay=0.9999, t_start=1.0, t_end=0.1, max_len=0, dead_flags=0,
               sweep=_lib.SWEEP_REFERENCE, stop_on_proof=False, cap=1 << 18, model=None, learned_frac=0.5,
-              trajectories=None, first_epoch=0):
+              trajectories=None, first_epoch=0, uniform_chains=0):
         """Batched STOKE over targets (list of sequences).  Returns (results,
         proofs, stats): results[i] is a dict per target (first_proof_ms < 0 when
         unproven, best rewrite), proofs every proof found, in order."""
@@ -276,6 +276,7 @@ class Engine:
         cfg.first_epoch = first_epoch
         if model is not None:
             cfg.proposal, cfg.model, cfg.learned_frac = _lib.PROPOSAL_MIXED, model.handle, learned_frac
+            cfg.uniform_chains = uniform_chains
         if trajectories is not None:   # (ctypes array of MlpExample, capacity, c_uint64 count)
             buf, tcap, tcount = trajectories
             cfg.trajectories = ctypes.cast(buf, ctypes.c_void_p)

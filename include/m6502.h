@@ -308,7 +308,10 @@ typedef struct m6502_stoke_cfg {
     uint32_t stop_on_proof;     /* stop a target's chains at its first proof */
     uint32_t proposal;          /* M6502_PROPOSAL_* */
     uint8_t dead_flags;         /* stoke --dead-flags */
-    uint8_t reserved[3];
+    uint8_t uniform_chains;     /* PROPOSAL_MIXED: of every 8 chains of a target, how many keep the
+                                   uniform proposal (0..8; a portfolio: a target is proved by
+                                   whichever chains get there first); 0 = every chain mixed */
+    uint8_t reserved[2];
     float learned_frac;         /* PROPOSAL_MIXED: share of replace / insert moves from the model */
     uint32_t first_epoch;       /* steps of the first epoch; each next epoch doubles, up to
                                    steps_per_epoch (finer time-to-proof early on); 0 = steps_per_epoch */
