@@ -11,8 +11,10 @@ MidCheck, and the oracle's ExhaustiveCheck where its domain has at most
 2^25 states; (3) on the STOKE benchmark's targets (a draw disjoint from the
 training and validation draws) that uniform STOKE does not prove in its
 first epoch (the model is first used in the second, so that epoch is the
-same under both), the median device time to the first proof is lower with
-the mixed proposal.
+same under both), the median device time to the first proof is at most
+half of uniform's with the benchmark's portfolio (4 of every 8 chains of a
+target uniform, the others mixed), and the portfolio proves at least as
+many of the 512 targets.
 """
 import numpy as np
 import pytest
@@ -54,12 +56,13 @@ def test_learned_proposal_gains_over_uniform(engine):
     res_l, proofs_l, st_l = engine.stoke(held, model=mlp, learned_frac=0.5, **kw)
     # (3) time-to-proof on hard targets: the STOKE benchmark's draw (512
     # targets of length 4-8, seed 2, disjoint from the training and
-    # validation draws), 128 chains each, full sweep
+    # validation draws), 128 chains each, full sweep, and the benchmark's
+    # portfolio (4 of every 8 chains of a target uniform, the others mixed)
     bench = I.draw_targets(2, 4, 8, 512, reject_pruned=False)
     kb = dict(chains_per_target=128, steps=200000, steps_per_epoch=2000, first_epoch=64, seed=2,
               cost=_lib.COST_HAMMING, sweep=_lib.SWEEP_FULL, stop_on_proof=True)
     bu, _, sbu = engine.stoke(bench, **kb)
-    bl, _, sbl = engine.stoke(bench, model=mlp, learned_frac=0.5, **kb)
+    bl, _, sbl = engine.stoke(bench, model=mlp, learned_frac=0.5, uniform_chains=4, **kb)
     hard_u, hard_l = [], []
     for ru, rl in zip(bu, bl):
         if ru["first_proof_ms"] >= 0 and ru["first_proof_step"] < 64:
@@ -71,7 +74,9 @@ def test_learned_proposal_gains_over_uniform(engine):
     print(f"hard targets: {len(hard_u)}; median ms uniform {np.median(hard_u):.2f}, "
           f"learned {np.median(hard_l):.2f}")
     assert len(hard_u) >= 10
-    assert np.median(hard_l) < np.median(hard_u)
+    # at least twice as fast at the median, and no target lost on the whole draw
+    assert np.median(hard_l) <= 0.5 * np.median(hard_u)
+    assert sum(r["first_proof_ms"] >= 0 for r in bl) >= sum(r["first_proof_ms"] >= 0 for r in bu)
     for res, name in ((res_u, "uniform"), (res_l, "learned")):
         st = sorted(r["first_proof_step"] for r in res if r["first_proof_ms"] >= 0)
         ms = sorted(r["first_proof_ms"] for r in res if r["first_proof_ms"] >= 0)
