@@ -227,6 +227,7 @@ struct Counters {
     unsigned long long surv1, items1;      // phase-1 survivors and work items (length-2 phase runs after)
     unsigned long long surv_need, items_need;   // largest survivor / work-item counts seen, for the
                                                 // overflow check after the pass
+    unsigned long long probe_ticket, probe_pass;   // k_probe_pairs: claimed pairs, pairs it passed on
 };
 
 struct Item {   // one chunk of a large cone sweep
@@ -830,6 +831,8 @@ struct ExhArgs {
     uint32_t defer_bits;         // > 0: pairs with a cone above 2^defer_bits states get fail = 4 (deferred)
     uint32_t ticket_batch;       // pairs a warp claims per ticket atomic (0 = kTicketBatch)
     uint32_t chunk_log2;         // states per work item, at least (0 = kChunk)
+    const uint32_t* order;       // non-null: ticket q sweeps pair order[q] (the pairs k_probe_pairs
+                                 // passed on, already probed); null: ticket q is pair q
 };
 
 // ---------------------------------------------------------------------------
@@ -1433,13 +1436,14 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
             lim = next + tbatch;
             if (lane == 0 && next < n) ahead = atomicAdd(&a.cnt->exh_ticket, tbatch);
         }
-        const unsigned long long p = next++;
-        if (p >= n) break;
+        const unsigned long long q = next++;
+        if (q >= n) break;
+        const unsigned long long p = a.order ? (unsigned long long)a.order[q] : q;
         PairView pv;
         pv.t = s_t[w]; pv.c = s_c[w];
         src.load(p, s_t[w], s_c[w], pv.tn, pv.cn, pv.dead, lane);
         const uint64_t tid = src.target_id(p);
-        const bool probed = src.probed(p);
+        const bool probed = a.order != nullptr || src.probed(p);
         __syncwarp();
         if (!probed) {
             uint32_t sw_t = 0, sw_c = 0;
@@ -1515,6 +1519,69 @@ __global__ void __launch_bounds__(256, MINB) k_exhaustive(Src src, const unsigne
         __syncwarp();
     }
     if (lane == 0 && nstates) atomicAdd(&a.cnt->states, nstates);
+    if (lane == 0 && probe_rej) atomicAdd(&a.cnt->probe_rejects, probe_rej);
+}
+
+// The random-state probe of every pair on its own, ahead of k_exhaustive:
+// a lean persistent kernel (many resident warps) runs probe_pair on each
+// surviving pair, marks the pairs it rejects (fail = 1) and appends the
+// others to `order`, 32 at a time per warp so that the passed pairs of one
+// target stay together; k_exhaustive then sweeps only those.  Pairs the
+// join already probed are passed on unprobed.
+template <class Src>
+__global__ void __launch_bounds__(256) k_probe_pairs(Src src, const unsigned long long* n_pairs_ptr, uint64_t n_cap,
+                                                     ExhArgs a, uint32_t* __restrict__ order) {
+    __shared__ uint16_t s_t[kWarpsPerBlock][kMaxSeq], s_c[kWarpsPerBlock][kMaxSeq];
+    __shared__ TargetCache s_tc[kWarpsPerBlock];
+    __shared__ uint32_t s_pass[kWarpsPerBlock][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    TargetCache& tc = s_tc[w];
+    if (lane == 0) { tc.probe_id = kNoTarget; tc.flow_id = kNoTarget; }
+    __syncwarp();
+    const uint64_t n = min((uint64_t)*n_pairs_ptr, n_cap);
+    const unsigned long long tbatch = a.ticket_batch ? a.ticket_batch : kTicketBatch;
+    unsigned long long next = 0, lim = 0, ahead = 0, probe_rej = 0;
+    int npass = 0;   // passed pairs staged in s_pass[w] (uniform)
+    auto flush = [&]() {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(&a.cnt->probe_pass, (unsigned long long)npass);
+        base = __shfl_sync(kFull, base, 0);
+        if (lane < npass && base + lane < n_cap) order[base + lane] = s_pass[w][lane];
+        __syncwarp();
+        npass = 0;
+    };
+    if (lane == 0) ahead = atomicAdd(&a.cnt->probe_ticket, tbatch);
+    for (;;) {
+        if (next >= lim) {
+            next = __shfl_sync(kFull, ahead, 0);
+            lim = next + tbatch;
+            if (lane == 0 && next < n) ahead = atomicAdd(&a.cnt->probe_ticket, tbatch);
+        }
+        const unsigned long long p = next++;
+        if (p >= n) break;
+        bool pass = true;
+        if (!src.probed(p)) {
+            PairView pv;
+            pv.t = s_t[w]; pv.c = s_c[w];
+            src.load(p, s_t[w], s_c[w], pv.tn, pv.cn, pv.dead, lane);
+            const uint64_t tid = src.target_id(p);
+            __syncwarp();
+            uint32_t sw_t = 0, sw_c = 0;
+            for (int i = 0; i < pv.tn; i++) sw_t |= c_sweep[pv.t[i] & 0xFFu];
+            for (int i = 0; i < pv.cn; i++) sw_c |= c_sweep[pv.c[i] & 0xFFu];
+            const bool prep = a.sweep == M6502_SWEEP_REFERENCE && __popc(sw_t | sw_c) >= 3;
+            pass = probe_pair(pv, sw_t, sw_c, prep, tid, p, tc, lane);
+            __syncwarp();
+        }
+        if (!pass) {
+            if (lane == 0) { a.fail[p] = 1u; probe_rej++; }
+        } else {
+            if (lane == 0) s_pass[w][npass] = (uint32_t)p;
+            __syncwarp();
+            if (++npass == 32) flush();
+        }
+    }
+    if (npass) flush();
     if (lane == 0 && probe_rej) atomicAdd(&a.cnt->probe_rejects, probe_rej);
 }
 
@@ -1968,7 +2035,7 @@ struct m6502_ctx {
     std::string err;
     std::mutex mu;
     int sms = 148;
-    int exh_blocks = 0, exh_item_blocks = 0, qc_blocks = 0, fp_blocks = 0;
+    int exh_blocks = 0, exh_item_blocks = 0, qc_blocks = 0, fp_blocks = 0, probe_blocks = 0;
     int exh_occ[5] = {};       // resident blocks per SM of k_exhaustive<SurvSource, MINB>, by MINB
     m6502_tune tune{4, 4, 11, 1, {0, 0, 0, 0}};   // scheduling knobs (m6502_tune_set / m6502_autotune)
     uint64_t pass_targets = 1ull << 21;
@@ -1982,6 +2049,7 @@ struct m6502_ctx {
     std::vector<uint8_t> h_cmeta;
     DevBuf go_keys, go_keys2, go_ord, go_round, go_sort_tmp;   // Go-order verification rounds
     DevBuf jitems;                                             // chunks of long length-2 equal ranges
+    DevBuf order;                                              // k_probe_pairs: the pairs it passed on
     DevBuf join_keys[256], join_idx[256];
     struct Cand2Table {            // sorted (key, index) of all length-2 sequences for one mask
         uint32_t dead = 0xFFFFFFFFu;
@@ -2038,9 +2106,17 @@ int ensure(m6502_ctx* ctx, DevBuf& b, size_t bytes) {
 // The exhaustive kernel over survivors with the context's knobs: ticket
 // batch and work-item size in the arguments, the register-cap variant and
 // its persistent grid (SMs x resident blocks).
-int launch_exh(m6502_ctx* ctx, const SurvSource& src, const unsigned long long* n_ptr, uint64_t cap, ExhArgs ea) {
+int launch_exh(m6502_ctx* ctx, const SurvSource& src, const unsigned long long* n_ptr, uint64_t cap, ExhArgs ea,
+               bool split = false) {
     ea.ticket_batch = ctx->tune.ticket_batch;
     ea.chunk_log2 = ctx->tune.chunk_log2;
+    if (split) {   // the probe first, in its own kernel; k_exhaustive then sweeps the pairs it passed on
+        k_probe_pairs<SurvSource><<<ctx->probe_blocks, 256, 0, ctx->stream>>>(src, n_ptr, cap, ea,
+                                                                               (uint32_t*)ctx->order.p);
+        CKL("k_probe_pairs");
+        ea.order = (const uint32_t*)ctx->order.p;
+        n_ptr = &ea.cnt->probe_pass;
+    }
     const int minb = (int)ctx->tune.exh_minb;
     const unsigned grid = (unsigned)(ctx->sms * ctx->exh_occ[minb >= 2 && minb <= 4 ? minb : 4]);
     if (minb == 2)
@@ -2124,6 +2200,8 @@ int init_ctx(m6502_ctx* ctx) {
     ctx->exh_occ[3] = std::max(occ, 1);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_exhaustive<SurvSource, 2>, 256, 0));
     ctx->exh_occ[2] = std::max(occ, 1);
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_probe_pairs<SurvSource>, 256, 0));
+    ctx->probe_blocks = ctx->sms * std::max(occ, 1);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_exh_items<SurvSource>, 256, 0));
     ctx->exh_item_blocks = ctx->sms * std::max(occ, 1);
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_qc1<false>, 256, 0));
@@ -2257,6 +2335,7 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
         // below can be recorded as one CUDA graph and replayed.
         TRY(ensure(ctx, ctx->surv, scap * sizeof(Surv)));
         TRY(ensure(ctx, ctx->fail, scap * sizeof(uint32_t)));
+        TRY(ensure(ctx, ctx->order, scap * sizeof(uint32_t)));
         TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
         TRY(ensure(ctx, ctx->rules, rcap * sizeof(m6502_rule)));
         if (go) TRY(ensure(ctx, ctx->best, 2 * nt * sizeof(uint32_t)));
@@ -2364,7 +2443,7 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             return M6502_OK;
         };
         if (go) CK(cudaMemsetAsync(ctx->best.p, 0xFF, 2 * nt * sizeof(uint32_t), ctx->stream));
-        if (exh && !rounds) TRY(launch_exh(ctx, src, &cnt->surv, scap, ea));
+        if (exh && !rounds) TRY(launch_exh(ctx, src, &cnt->surv, scap, ea, true));
         if (rounds) TRY(go_rounds(kNumInsns));   // a target has at most 2,863 length-1 candidates
         CK(rec(ctx->sev[3]));
         if (exh && !rounds) TRY(launch_items(ctx, src, ea));
@@ -2416,7 +2495,7 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             }
             CKL("k_qc_join2");
             CK(rec(ctx->sev2[1]));
-            if (exh && !rounds) TRY(launch_exh(ctx, src, &cnt->surv, scap, ea));
+            if (exh && !rounds) TRY(launch_exh(ctx, src, &cnt->surv, scap, ea, true));
             if (rounds) TRY(go_rounds((uint64_t)kNumInsns * kNumInsns));
             CK(rec(ctx->sev2[2]));
             if (exh && !rounds) TRY(launch_items(ctx, src, ea));
@@ -2442,6 +2521,7 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
                 (uint64_t)(uintptr_t)d_targets, nt, tlen, (uint64_t)(uintptr_t)d_ids, cfg.semantics, cfg.sweep,
                 cfg.exh_mode, stages, cfg.flags, dead, cfg.max_cand_len, scap, icap, rcap, jcap,
                 (uint64_t)(uintptr_t)ctx->surv.p, (uint64_t)(uintptr_t)ctx->fail.p, (uint64_t)(uintptr_t)ctx->items.p,
+                (uint64_t)(uintptr_t)ctx->order.p,
                 (uint64_t)(uintptr_t)ctx->rules.p, (uint64_t)(uintptr_t)ctx->cnt.p, (uint64_t)(uintptr_t)ctx->best.p,
                 (uint64_t)(uintptr_t)ctx->tfp.p, (uint64_t)(uintptr_t)ctx->tmeta.p,
                 (uint64_t)(uintptr_t)ctx->go_keys.p, (uint64_t)(uintptr_t)ctx->go_keys2.p,
@@ -2575,6 +2655,7 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
     for (int attempt = 0; attempt < 6; attempt++) {
         TRY(ensure(ctx, ctx->surv, scap * sizeof(Surv)));
         TRY(ensure(ctx, ctx->fail, scap * sizeof(uint32_t)));
+        TRY(ensure(ctx, ctx->order, scap * sizeof(uint32_t)));
         TRY(ensure(ctx, ctx->items, icap * sizeof(Item)));
         TRY(ensure(ctx, ctx->rules, rcap * sizeof(m6502_rule)));
         // All passes, queued with no host round trip, recorded once as a CUDA
@@ -2615,7 +2696,7 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
                 SurvSource src{(const Surv*)ctx->surv.p, d_t, tlen, dead, 0};
                 ExhArgs ea{(uint32_t*)ctx->fail.p, (Item*)ctx->items.p, icap, cnt, cfg.sweep,
                            cfg.exh_mode == M6502_EXH_BRUTE};
-                if (exh) TRY(launch_exh(ctx, src, &cnt->surv, scap, ea));
+                if (exh) TRY(launch_exh(ctx, src, &cnt->surv, scap, ea, true));
                 CK(rec(ev[3]));
                 if (exh) TRY(launch_items(ctx, src, ea));
                 CK(rec(ev[4]));
@@ -2635,7 +2716,7 @@ int search_async(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* ta
             const std::vector<uint64_t> key = {
                 (uint64_t)(uintptr_t)targets, n, tlen, cfg.semantics, cfg.sweep, cfg.exh_mode, stages,
                 cfg.flags, dead, scap, icap, rcap, P, (uint64_t)(uintptr_t)ctx->surv.p,
-                (uint64_t)(uintptr_t)ctx->fail.p, (uint64_t)(uintptr_t)ctx->items.p,
+                (uint64_t)(uintptr_t)ctx->fail.p, (uint64_t)(uintptr_t)ctx->items.p, (uint64_t)(uintptr_t)ctx->order.p,
                 (uint64_t)(uintptr_t)ctx->rules.p, (uint64_t)(uintptr_t)ctx->cnt_slots.p,
                 (uint64_t)(uintptr_t)ctx->tfp.p, (uint64_t)(uintptr_t)ctx->tmeta.p,
                 (uint64_t)(uintptr_t)ctx->join_keys[dead].p, ctx->tune.exh_minb, ctx->tune.ticket_batch,
@@ -2926,7 +3007,7 @@ void m6502_destroy(m6502_ctx* ctx) {
                       &ctx->st_vlist, &ctx->st_vpos, &ctx->st_sort_tmp, &ctx->c2_keys_in, &ctx->c2_idx_in,
                       &ctx->c2_sort_tmp, &ctx->go_keys, &ctx->go_keys2, &ctx->go_ord, &ctx->go_round,
                       &ctx->go_sort_tmp, &ctx->jitems, &ctx->cnt_slots, &ctx->st_vphase, &ctx->st_pphase,
-                      &ctx->tall, &ctx->opflag};
+                      &ctx->tall, &ctx->opflag, &ctx->order};
     for (DevBuf* b : bufs) if (b->p) cudaFree(b->p);
     for (cudaEvent_t e : ctx->sev) if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : ctx->sev2) if (e) cudaEventDestroy(e);
