@@ -332,14 +332,15 @@ def run_engine(args):
         dominant = max(("k_exhaustive", avg("ms_exhaustive")), ("k_exh_items", avg("ms_exh_items")),
                        ("k_qc_join", qc_ms), key=lambda kv: kv[1])[0]
         figs, figs_source = load_profile_figures()
-        exh_kernels = ("k_exhaustive", "k_exh_items")
+        # the exhaustive stage's events bracket the probe kernel and k_exhaustive
+        exh_kernels = ("k_probe_pairs", "k_exhaustive", "k_exh_items")
         if dominant == "k_qc_join":
             achieved, alg = qc_achieved, "13 ops/pair + 31x13 ops per QC hit (QC+MidCheck)"
             kernels, ktime = ("k_qc_join",), qc_ms
         else:
-            # states the two exhaustive kernels evaluated (cone sweeps, work items and
-            # the 128-state random probes) at the convention's 10 ops per executed
-            # instruction + 3 per compare
+            # states the exhaustive stage's kernels evaluated (cone sweeps, work items
+            # and the 128-state random probes) at the convention's 10 ops per
+            # executed instruction + 3 per compare
             achieved, alg = exh_exec, ("states evaluated (cone sweeps + items + 128-state probes) x "
                                        "(10 ops/instruction x 3 instructions + 3)")
             kernels, ktime = exh_kernels, exh_ms
