@@ -13,11 +13,14 @@
 //                   target, then a tile of 64 targets x all 2,863
 //                   candidates per CTA with one masked 64-bit compare per
 //                   pair; the same survivors as the join.
-//   k_exhaustive    persistent; a warp takes one surviving pair from a
-//                   device ticket, derives the pair's swept input space
-//                   (reference rule) and the input cone of every output
-//                   location, and sweeps each maximal cone; large cones are
-//                   probed in-warp and the rest is split into work items.
+//   k_probe_pairs   persistent, lean; 128 random states of every surviving
+//                   pair's sweep domain (four per lane, packed); rejects are
+//                   marked, the rest listed for k_exhaustive.
+//   k_exhaustive    persistent; a warp takes one listed pair from a device
+//                   ticket, derives the pair's swept input space (reference
+//                   rule) and the input cone of every output location, and
+//                   sweeps each maximal cone; large cones are probed in-warp
+//                   and the rest is split into work items.
 //   k_exh_items     persistent; warps drain the work-item queue; a failing
 //                   item raises the pair's fail flag, which the others poll.
 //   k_emit_*        passing pairs -> rules (CUDA semantics: all of them; Go
