@@ -2478,8 +2478,9 @@ int run_pass(m6502_ctx* ctx, const m6502_search_cfg& cfg, const uint16_t* d_targ
             // phase are checked once, after the pass.
             k_mark_phase<<<1, 1, 0, ctx->stream>>>(cnt);
             CKL("k_mark_phase");
-            // survivor, exhaustive-ticket and work-item counters restart for this phase
+            // survivor, exhaustive-ticket, work-item and probe counters restart for this phase
             CK(cudaMemsetAsync(&cnt->surv, 0, 4 * sizeof(unsigned long long), ctx->stream));
+            CK(cudaMemsetAsync(&cnt->probe_ticket, 0, 2 * sizeof(unsigned long long), ctx->stream));
             CK(rec(ctx->sev2[0]));
             const uint32_t jgrid2 =
                 (uint32_t)std::min<uint64_t>((uint64_t)ctx->sms * 8, (nt + kWarpsPerBlock - 1) / kWarpsPerBlock);
