@@ -214,6 +214,34 @@ def test_draw_targets_matches_oracle_draw():
     assert len({len(s) for s in var}) == 5
 
 
+def test_ctypes_layouts_match_the_header(tmp_path):
+    """Every ctypes structure of the Python mirror has the C header's size and
+    the same offset and size for every field (tests/abi_layout.c prints the
+    C side with offsetof / sizeof)."""
+    import subprocess
+    exe = str(tmp_path / "abi_layout")
+    subprocess.run(["gcc", "-O0", "-std=c11", "-I", os.path.join(ROOT, "include"), "-o", exe,
+                    os.path.join(ROOT, "tests", "abi_layout.c")], check=True)
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=60, check=True).stdout
+    mirror = {"m6502_opts": _lib.Opts, "m6502_rule": _lib.Rule, "m6502_search_cfg": _lib.SearchCfg,
+              "m6502_stats": _lib.Stats, "m6502_tune": _lib.Tune, "m6502_stoke_cfg": _lib.StokeCfg,
+              "m6502_stoke_proof": _lib.StokeProof, "m6502_stoke_result": _lib.StokeResult,
+              "m6502_stoke_stats": _lib.StokeStats, "m6502_mlp_example": _lib.MlpExample}
+    seen = {name: set() for name in mirror}
+    for line in out.splitlines():
+        parts = line.split()
+        cls = mirror[parts[0]]
+        if parts[1] == "SIZEOF":
+            assert ctypes.sizeof(cls) == int(parts[2]), line
+            continue
+        field, off, size = parts[1], int(parts[2]), int(parts[3])
+        f = getattr(cls, field)
+        assert (f.offset, f.size) == (off, size), (line, f.offset, f.size)
+        seen[parts[0]].add(field)
+    for name, cls in mirror.items():   # no ctypes field the C side does not have
+        assert {n for n, _ in cls._fields_} == seen[name], name
+
+
 def test_swar_exec_matches_scalar(tmp_path):
     """exec_x4 (four machine states per 32-bit register, one dispatch) gives
     the same result as four scalar exec calls for every instruction."""
